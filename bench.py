@@ -1,0 +1,304 @@
+"""Benchmark of the B200 cavity step (MLUPS and fraction of the HBM roofline).
+
+Workload (default): the 128x512 differentially heated cavity at Ra = 1e8
+(Pr 0.71, Cs 0.10, TRT Lambda = 3/16, Guo forcing, theta = 0 + U(+-1e-4)),
+populations stored in FP16 shifted by w_i with FP32 arithmetic.  One bench
+"step" is a chunk of CHUNK lattice time steps of that cavity; the L2 is
+flushed between timed chunks (the 5 MB cavity state itself is L2-resident
+inside a chunk: that is the workload).
+
+value   node updates per second (MLUPS) with the state resident on the GPU,
+        CUDA events on the solver's stream around each chunk;
+e2e     the same metric through the public C ABI with host buffers: every
+        chunk restarts from host fields (cav_init_from_fields), runs CHUNK
+        steps and reads the fields back (cav_get_fields);
+roofline  algorithmic bytes of the fused step kernel (80 B per node update
+        for 16-bit storage: 18 populations x 2 B read + written, plus the
+        FP32 Guo force read + written) / its average launch time, against the
+        measured HBM copy bandwidth;
+cpu_baseline  the FP64 oracle (a restatement of the reference's Rust solver)
+        timed on the host cores with row-band threading, bounded sample.
+
+``--impl reference`` times that CPU implementation alone (rank 0).
+Multi-GPU (torchrun): independent replicas, one cavity per GPU ("weak").
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX, NY, RA = 128, 512, 1e8
+PHYS = dict(pr=0.71, cs=0.10, pr_t=0.9, utarget=0.02, seed=42)
+CHUNK = 2000
+BYTES_PER_NODE = {"f64": 304, "f32": 152, "f16": 80, "bf16": 80}
+PRECISION = "f16"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(precision):
+    """DRAM bytes per launch of the fused kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "k_fused_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as fh:
+        d = json.load(fh)
+    v = d.get(precision)
+    return None if v is None else float(v["dram_bytes_per_launch_full"])
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.proc = None
+        self.index = index
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 6:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[2:]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(seconds=12.0, jobs=None):
+    """FP64 oracle on the host cores, bounded sample of the same cavity."""
+    import oracle
+
+    jobs = jobs or (os.cpu_count() or 1)
+    s = oracle.OracleSolver(NX, NY, RA, PHYS["pr"], PHYS["cs"], PHYS["pr_t"], PHYS["utarget"],
+                            PHYS["seed"], jobs, init_mode=oracle.INIT_ZERO, noise_amp=1e-4)
+    s.step(5)  # warm-up
+    n, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        s.step(20)
+        n += 20
+    dt = time.perf_counter() - t0
+    mlups = NX * NY * n / dt / 1e6
+    return {"value": mlups, "unit": "MLUPS", "cores": jobs, "kind": "port",
+            "sample": f"{NX}x{NY} Ra=1e8 FP64 oracle, {n} lattice steps in {dt:.1f} s "
+                      f"({jobs} row-band threads)"}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "gloo" if args.impl == "reference" else "nccl"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local, dist
+
+
+def run_reference(args, world, rank, dist):
+    if rank != 0:
+        return 0
+    base = cpu_baseline(seconds=max(5.0, min(30.0, 2.0 * args.steps)))
+    line = {
+        "impl": "reference", "metric": "MLUPS", "value": base["value"], "unit": "MLUPS",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": f"dhc {NX}x{NY} Ra=1e8 (oracle FP64, CPU)"},
+        "cpu_baseline": base,
+        "e2e": {"value": base["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default=PRECISION, choices=list(BYTES_PER_NODE))
+    ap.add_argument("--chunk", type=int, default=CHUNK)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local, dist = dist_setup(args)
+    if args.impl == "reference":
+        rc = run_reference(args, world, rank, dist)
+        if dist:
+            dist.destroy_process_group()
+        return rc
+
+    import torch
+
+    from cfd_cavity_b200 import CavitySolver
+    from cfd_cavity_b200 import _lib as L
+
+    dev = local
+    torch.cuda.set_device(dev)
+    prec = args.precision
+    s = CavitySolver(NX, NY, RA, PHYS["pr"], PHYS["cs"], PHYS["pr_t"], PHYS["utarget"],
+                     PHYS["seed"], precision=prec, init_mode=L.CAV_INIT_ZERO, noise_amp=1e-4,
+                     device=dev)
+    stream = torch.cuda.ExternalStream(s.stream_handle(), device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    nodes = NX * NY
+    # get past the spin-up ramps once: the timed chunks are steady-state steps
+    s.step(s.info()["spin_up_steps"] + 64)
+    for _ in range(args.warmup):
+        s.step(args.chunk)
+    s.sync()
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
+
+    # ---- device-resident timing -------------------------------------------------
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    launches0 = s.launch_count()
+    clocks = Clocks(dev)
+    barrier()
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(i & 0xFF)  # write > L2 between chunks (outside the events)
+            ev[i][0].record(stream)
+        s.step(args.chunk)
+        with torch.cuda.stream(stream):
+            ev[i][1].record(stream)
+    barrier()
+    clk = clocks.stop()
+    launches = s.launch_count() - launches0
+    ms = [a.elapsed_time(b) for a, b in ev]
+    t_total = sum(ms) / 1e3
+    t_max = t_total
+    if dist:
+        tt = torch.tensor([t_total], device=f"cuda:{dev}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    updates = nodes * args.chunk * args.steps * world
+    value = updates / t_max / 1e6
+    kernel_us = t_total / (args.chunk * args.steps) * 1e6  # per fused launch
+    bpn = BYTES_PER_NODE[prec]
+    achieved = bpn * nodes / (kernel_us * 1e-6) / 1e9
+    peak, peak_kind = measured_peaks()
+
+    # ---- end to end through the C ABI, host buffers ------------------------------
+    n = nodes
+    host = {k: torch.empty(n, dtype=torch.float64, pin_memory=True) for k in ("rho", "ux", "uy", "t")}
+    f0 = s.fields()
+    for k, src in (("rho", "rho"), ("ux", "ux"), ("uy", "uy"), ("t", "temperature")):
+        host[k].copy_(torch.from_numpy(f0[src]))
+    outs = {k: torch.empty(n, dtype=torch.float64, pin_memory=True) for k in ("rho", "ux", "uy", "t")}
+    ptr = {k: ctypes.cast(v.data_ptr(), L._dp) for k, v in host.items()}
+    optr = {k: ctypes.cast(v.data_ptr(), L._dp) for k, v in outs.items()}
+    lib = L.load()
+    e2e_steps = max(2, min(args.steps, 5))
+
+    def e2e_once():
+        L.check(lib.cav_init_from_fields(s._h, ptr["rho"], ptr["ux"], ptr["uy"], ptr["t"]), s._h)
+        L.check(lib.cav_step(s._h, args.chunk), s._h)
+        L.check(lib.cav_get_fields(s._h, optr["rho"], optr["ux"], optr["uy"], optr["t"], None, None), s._h)
+
+    e2e_once()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_once()
+    barrier()
+    te = time.perf_counter() - t0
+    if dist:
+        tt = torch.tensor([te], device=f"cuda:{dev}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te = float(tt.item())
+    e2e_value = nodes * args.chunk * e2e_steps * world / te / 1e6
+
+    line = None
+    if rank == 0:
+        base = None
+        if not args.no_cpu_baseline and world == 1:
+            base = cpu_baseline()
+        line = {
+            "metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"dhc {NX}x{NY} Ra=1e8 uniform D2Q9 TRT+Smagorinsky+Guo, "
+                                   f"{prec} shifted population storage, FP32 arithmetic",
+                       "storage": prec, "nx": NX, "ny": NY, "ra": RA,
+                       "lattice_steps_per_bench_step": args.chunk,
+                       "l2": "flushed (256 MB write) between timed chunks, outside the events; "
+                             "the cavity state (5 MB) is L2-resident within a chunk",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": profile_traffic(prec),
+                         "kernel": "k_fused", "algorithmic_bytes_per_node": bpn,
+                         "avg_launch_us": kernel_us},
+            "cpu_baseline": base,
+            "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": 4 * 8 * n,
+                    "d2h_bytes_per_step": 4 * 8 * n,
+                    "note": "restart from host fields + CHUNK steps + read fields, per bench step"},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,10 @@
+"""B200-native lattice-Boltzmann step of the 2D differentially heated cavity.
+
+Drop-in for the step of bbrangeo/cfd_cavity (``uniform::solver::CavitySolver``,
+``src/uniform/solver.rs``): CUDA kernels for sm_100a behind the C ABI of
+``include/cavity.h``; this package is its Python host mirror.
+"""
+from ._lib import CavError, load  # noqa: F401
+from .solver import DELTA_T, T_COLD, T_HOT, CavitySolver, TimeAverager  # noqa: F401
+
+__all__ = ["CavitySolver", "TimeAverager", "CavError", "load", "T_HOT", "T_COLD", "DELTA_T"]

@@ -1,0 +1,121 @@
+"""ctypes binding of ``libcavity_b200.so`` (the C ABI of ``include/cavity.h``).
+
+Loading fails loudly when the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libcavity_b200.so")
+
+CAV_OK = 0
+CAV_ERR_ARG = 1
+CAV_ERR_TAU = 2
+CAV_ERR_DIVERGED = 3
+CAV_ERR_MAXU = 4
+CAV_ERR_TIMEOUT = 5
+CAV_ERR_CUDA = 6
+CAV_ERR_STATE = 7
+CAV_ERR_NOMEM = 8
+
+CAV_PREC_F64, CAV_PREC_F32, CAV_PREC_F16, CAV_PREC_BF16 = 0, 1, 2, 3
+PRECISIONS = {"f64": CAV_PREC_F64, "f32": CAV_PREC_F32, "f16": CAV_PREC_F16, "bf16": CAV_PREC_BF16}
+CAV_INIT_LINEAR, CAV_INIT_ZERO = 0, 1
+(CAV_PHASE_COLLIDE, CAV_PHASE_STREAM, CAV_PHASE_BOUNCE_BACK, CAV_PHASE_THERMAL_BC,
+ CAV_PHASE_MACRO, CAV_PHASE_NOSLIP, CAV_PHASE_FUSED_IDENTITY) = range(7)
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class CavParams(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int32), ("ny", ctypes.c_int32),
+        ("ra", ctypes.c_double), ("pr", ctypes.c_double), ("cs", ctypes.c_double),
+        ("pr_t", ctypes.c_double), ("utarget", ctypes.c_double),
+        ("seed", ctypes.c_uint64), ("jobs", ctypes.c_int32),
+        ("alpha_mult", ctypes.c_double), ("nu_start_mult", ctypes.c_double),
+        ("has_nu_override", ctypes.c_int32), ("nu_override", ctypes.c_double),
+        ("init_mode", ctypes.c_int32), ("noise_amp", ctypes.c_double),
+        ("geq_order", ctypes.c_int32),
+        ("t_hot_profile", _dp),
+        ("t_cold", ctypes.c_double),
+        ("precision", ctypes.c_int32), ("device", ctypes.c_int32),
+    ]
+
+
+class CavInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in
+                ("nu", "alpha", "alpha_phys", "beta_eff", "lz", "lx", "tau", "tau_t")] + [
+        ("time_step", ctypes.c_int64), ("spin_up_steps", ctypes.c_int64),
+        ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("pitch", ctypes.c_int32),
+        ("precision", ctypes.c_int32)]
+
+
+class CavDiag(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in
+                ("nusselt_hot", "nusselt_cold", "nusselt_hot_wall_link", "total_mass",
+                 "total_f_mass", "max_u", "max_uy", "nu_t_max", "y_plus_hot",
+                 "nusselt_volume")] + [("finite", ctypes.c_int32)]
+
+
+class CavError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load(path: str | None = None):
+    """Loads the library (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(f"CUDA library not built: {p} (run cfd_cavity_b200/build.py)")
+    L = ctypes.CDLL(p)
+    vp, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+    pp = ctypes.POINTER(CavParams)
+    sig = {
+        "cav_version": (ctypes.c_char_p, []),
+        "cav_default_params": (i32, [pp]),
+        "cav_create": (i32, [pp, ctypes.POINTER(vp)]),
+        "cav_destroy": (i32, [vp]),
+        "cav_last_error": (ctypes.c_char_p, [vp]),
+        "cav_init_from_fields": (i32, [vp, _dp, _dp, _dp, _dp]),
+        "cav_step": (i32, [vp, i64]),
+        "cav_get_fields": (i32, [vp, _dp, _dp, _dp, _dp, _dp, _dp]),
+        "cav_set_fields": (i32, [vp, _dp, _dp, _dp, _dp, _dp]),
+        "cav_get_populations": (i32, [vp, _dp, _dp]),
+        "cav_set_populations": (i32, [vp, _dp, _dp]),
+        "cav_get_info": (i32, [vp, ctypes.POINTER(CavInfo)]),
+        "cav_set_time_step": (i32, [vp, i64]),
+        "cav_diag": (i32, [vp, ctypes.POINTER(CavDiag)]),
+        "cav_check_guards": (i32, [vp, ctypes.c_double]),
+        "cav_debug_phase": (i32, [vp, i32, i64]),
+        "cav_sample": (i32, [vp]),
+        "cav_reset_means": (i32, [vp]),
+        "cav_get_means": (i32, [vp, _dp, _dp, _dp, _dp, _dp, ctypes.POINTER(i64)]),
+        "cav_nusselt_from_mean": (i32, [vp, i32, _dp]),
+        "cav_nu_accumulate": (i32, [vp, i32]),
+        "cav_nu_accumulated": (i32, [vp, _dp, _dp, ctypes.POINTER(i64)]),
+        "cav_sync": (i32, [vp]),
+        "cav_get_stream": (i32, [vp, ctypes.POINTER(vp)]),
+        "cav_launch_count": (i32, [vp, ctypes.POINTER(i64)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def check(rc: int, h=None):
+    if rc != CAV_OK:
+        msg = load().cav_last_error(h)
+        raise CavError(rc, msg.decode() if msg else "")

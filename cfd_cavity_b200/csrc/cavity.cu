@@ -1,0 +1,294 @@
+// cavity.cu -- the C ABI declared in include/cavity.h (host code only).
+//
+// Every entry point maps one CavitySolver method or field access of the
+// reference (cited in include/cavity.h) onto a cav::Solver object; errors
+// become status codes and a per-handle message instead of panics.
+#include "solver.cuh"
+
+using namespace cav;
+
+namespace {
+thread_local std::string g_create_error;
+}  // namespace
+
+struct cav_handle {
+    std::unique_ptr<Solver> s;
+};
+
+namespace {
+
+int fail(cav_handle* h, int code, const std::string& msg) {
+    if (h && h->s) h->s->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+template <class F>
+int guarded(cav_handle* h, F&& fn) {
+    if (!h || !h->s) return fail(nullptr, CAV_ERR_ARG, "null handle");
+    try {
+        cudaSetDevice(h->s->p.device);
+        fn(*h->s);
+        return CAV_OK;
+    } catch (const CudaError& e) {
+        return fail(h, CAV_ERR_CUDA, std::string(e.where) + ": " + cudaGetErrorString(e.e));
+    } catch (const ArgError& e) {
+        return fail(h, e.code, e.msg);
+    } catch (const std::bad_alloc&) {
+        return fail(h, CAV_ERR_NOMEM, "host allocation failed");
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cav_version(void) { return "cfd_cavity_b200 0.1 (sm_100a)"; }
+
+int cav_default_params(cav_params* p) {
+    if (!p) return CAV_ERR_ARG;
+    std::memset(p, 0, sizeof(*p));
+    p->nx = 64;
+    p->ny = 256;
+    p->ra = 1.0e6;
+    p->pr = 0.71;
+    p->cs = 0.10;
+    p->pr_t = 0.9;
+    p->utarget = 0.02;
+    p->seed = 42;
+    p->jobs = 1;
+    p->alpha_mult = 1.0;
+    p->nu_start_mult = 1.0;
+    p->has_nu_override = 0;
+    p->nu_override = 0.0;
+    p->init_mode = CAV_INIT_LINEAR;
+    p->noise_amp = 1.0e-3;
+    p->geq_order = 2;
+    p->t_hot_profile = nullptr;
+    p->t_cold = -0.5;
+    p->precision = CAV_PREC_F64;
+    p->device = 0;
+    return CAV_OK;
+}
+
+int cav_create(const cav_params* pp, cav_handle** out) {
+    if (!pp || !out) return fail(nullptr, CAV_ERR_ARG, "null argument");
+    *out = nullptr;
+    const cav_params& p = *pp;
+    if (p.nx < 4 || p.ny < 4 || p.nx > 65536 || p.ny > 65536)
+        return fail(nullptr, CAV_ERR_ARG, "nx and ny must be in [4, 65536]");
+    if (p.precision < CAV_PREC_F64 || p.precision > CAV_PREC_BF16)
+        return fail(nullptr, CAV_ERR_ARG, "unknown precision");
+    if (p.geq_order != 1 && p.geq_order != 2) return fail(nullptr, CAV_ERR_ARG, "geq_order must be 1 or 2");
+    if (p.init_mode != CAV_INIT_LINEAR && p.init_mode != CAV_INIT_ZERO)
+        return fail(nullptr, CAV_ERR_ARG, "unknown init_mode");
+    std::unique_ptr<Solver> s;
+    try {
+        Units U = derive_units(p);
+        s.reset(make_solver(p.precision));
+        s->p = p;
+        s->p.t_hot_profile = nullptr;
+        s->U = U;
+        s->spin_up = std::min<int64_t>(std::max<int64_t>(p.ny / 10, 200), 2000);
+        s->nu_start_mult = std::fmax(p.nu_start_mult, 1.0);
+        s->t_hot.assign(p.ny, 0.5);
+        if (p.t_hot_profile)
+            for (int i = 0; i < p.ny; ++i) s->t_hot[i] = p.t_hot_profile[i];
+        s->pitch = (p.nx + 31) / 32 * 32;
+        CK(cudaSetDevice(p.device));
+        s->alloc();
+        // Initial temperature, src/uniform/solver.rs:159-176 (row-major RNG order).
+        std::vector<double> t0(size_t(p.nx) * p.ny);
+        Rng rng(p.seed);
+        for (int iy = 0; iy < p.ny; ++iy)
+            for (int ix = 0; ix < p.nx; ++ix) {
+                double xf = double(ix) / double(p.nx - 1);
+                double t_lin = 0.5 + (-0.5 - 0.5) * xf;
+                double pert = p.noise_amp * (2.0 * rng.next_f64() - 1.0);
+                t0[size_t(iy) * p.nx + ix] = (p.init_mode == CAV_INIT_LINEAR) ? t_lin + pert : pert;
+            }
+        s->init_default(t0);
+    } catch (const CudaError& e) {
+        return fail(nullptr, e.e == cudaErrorMemoryAllocation ? CAV_ERR_NOMEM : CAV_ERR_CUDA,
+                    std::string(e.where) + ": " + cudaGetErrorString(e.e));
+    } catch (const ArgError& e) {
+        return fail(nullptr, e.code, e.msg);
+    } catch (const std::bad_alloc&) {
+        return fail(nullptr, CAV_ERR_NOMEM, "host allocation failed");
+    }
+    cav_handle* h = new cav_handle;
+    h->s = std::move(s);
+    *out = h;
+    return CAV_OK;
+}
+
+int cav_destroy(cav_handle* h) {
+    if (!h) return CAV_ERR_ARG;
+    if (h->s) cudaSetDevice(h->s->p.device);
+    delete h;
+    return CAV_OK;
+}
+
+const char* cav_last_error(const cav_handle* h) {
+    if (h && h->s) return h->s->err.c_str();
+    return g_create_error.c_str();
+}
+
+int cav_init_from_fields(cav_handle* h, const double* rho, const double* ux, const double* uy, const double* t) {
+    if (!rho || !ux || !uy || !t) return fail(h, CAV_ERR_ARG, "init_from_fields: null field");
+    return guarded(h, [&](Solver& s) { s.init_from_fields(rho, ux, uy, t); });
+}
+
+int cav_step(cav_handle* h, int64_t n) {
+    if (n < 0) return fail(h, CAV_ERR_ARG, "negative step count");
+    return guarded(h, [&](Solver& s) { s.step(n); });
+}
+
+int cav_get_fields(cav_handle* h, double* rho, double* ux, double* uy, double* t, double* nu_t, double* fy) {
+    return guarded(h, [&](Solver& s) { s.get_fields(rho, ux, uy, t, nu_t, fy); });
+}
+
+int cav_set_fields(cav_handle* h, const double* rho, const double* ux, const double* uy, const double* t,
+                   const double* fy) {
+    return guarded(h, [&](Solver& s) { s.set_fields(rho, ux, uy, t, fy); });
+}
+
+int cav_get_populations(cav_handle* h, double* f, double* g) {
+    return guarded(h, [&](Solver& s) { s.get_pops(f, g); });
+}
+
+int cav_set_populations(cav_handle* h, const double* f, const double* g) {
+    return guarded(h, [&](Solver& s) { s.set_pops(f, g); });
+}
+
+int cav_get_info(cav_handle* h, cav_info* o) {
+    if (!o) return fail(h, CAV_ERR_ARG, "null output");
+    return guarded(h, [&](Solver& s) {
+        o->nu = s.U.nu;
+        o->alpha = s.U.alpha;
+        o->alpha_phys = s.U.alpha_phys;
+        o->beta_eff = s.U.beta_eff;
+        o->lz = s.U.lz;
+        o->lx = s.U.lx;
+        o->tau = s.U.tau;
+        o->tau_t = s.U.tau_t;
+        o->time_step = s.time_step;
+        o->spin_up_steps = s.spin_up;
+        o->nx = s.p.nx;
+        o->ny = s.p.ny;
+        o->pitch = s.pitch;
+        o->precision = s.p.precision;
+    });
+}
+
+int cav_set_time_step(cav_handle* h, int64_t t) {
+    if (t < 0) return fail(h, CAV_ERR_ARG, "negative time step");
+    return guarded(h, [&](Solver& s) { s.time_step = t; });
+}
+
+int cav_diag(cav_handle* h, cav_diag_out* o) {
+    if (!o) return fail(h, CAV_ERR_ARG, "null output");
+    return guarded(h, [&](Solver& s) {
+        double v[11];
+        s.diag(v);
+        o->nusselt_hot = v[0];
+        o->nusselt_cold = v[1];
+        o->nusselt_hot_wall_link = v[2];
+        o->total_mass = v[3];
+        o->total_f_mass = v[4];
+        o->max_u = v[5];
+        o->max_uy = v[6];
+        o->nu_t_max = v[7];
+        o->y_plus_hot = v[8];
+        o->nusselt_volume = v[9];
+        o->finite = v[10] == 0.0 ? 1 : 0;
+    });
+}
+
+int cav_check_guards(cav_handle* h, double max_u_abort) {
+    cav_diag_out d;
+    int rc = cav_diag(h, &d);
+    if (rc != CAV_OK) return rc;
+    if (d.max_u > max_u_abort) {
+        char buf[160];
+        std::snprintf(buf, sizeof buf, "max_u = %.5f above the %.2f guard", d.max_u, max_u_abort);
+        return fail(h, CAV_ERR_MAXU, buf);
+    }
+    if (!d.finite) return fail(h, CAV_ERR_DIVERGED, "non-finite field (diverged)");
+    return CAV_OK;
+}
+
+int cav_debug_phase(cav_handle* h, int32_t phase, int64_t step_arg) {
+    return guarded(h, [&](Solver& s) { s.debug_phase(phase, step_arg); });
+}
+
+int cav_sample(cav_handle* h) {
+    return guarded(h, [&](Solver& s) { s.sample(); });
+}
+
+int cav_reset_means(cav_handle* h) {
+    return guarded(h, [&](Solver& s) { s.reset_means(); });
+}
+
+int cav_get_means(cav_handle* h, double* ux, double* uy, double* t, double* nu_t, double* uu, int64_t* n) {
+    return guarded(h, [&](Solver& s) {
+        int64_t c = s.get_means(ux, uy, t, nu_t, uu);
+        if (n) *n = c;
+    });
+}
+
+int cav_nusselt_from_mean(cav_handle* h, int32_t hot, double* out) {
+    if (!out) return fail(h, CAV_ERR_ARG, "null output");
+    return guarded(h, [&](Solver& s) {
+        const int nx = s.p.nx, ny = s.p.ny;
+        std::vector<double> t(size_t(nx) * ny);
+        s.get_means(nullptr, nullptr, t.data(), nullptr, nullptr);
+        double sum = 0.0;
+        for (int iy = 0; iy < ny; ++iy) {
+            const double* r = t.data() + size_t(iy) * nx;
+            double grad = hot ? r[1] - r[2] : r[nx - 3] - r[nx - 2];
+            sum += std::fabs(grad);
+        }
+        *out = (sum / double(ny)) * s.U.lz / 1.0;
+    });
+}
+
+int cav_nu_accumulate(cav_handle* h, int32_t enable) {
+    return guarded(h, [&](Solver& s) { s.nu_accumulate(enable != 0); });
+}
+
+int cav_nu_accumulated(cav_handle* h, double* hot, double* cold, int64_t* n) {
+    return guarded(h, [&](Solver& s) { s.nu_accumulated(hot, cold, n); });
+}
+
+int cav_sync(cav_handle* h) {
+    return guarded(h, [&](Solver& s) { s.sync(); });
+}
+
+int cav_get_stream(cav_handle* h, void** stream) {
+    if (!stream) return fail(h, CAV_ERR_ARG, "null output");
+    return guarded(h, [&](Solver& s) { *stream = (void*)s.stream; });
+}
+
+int cav_launch_count(cav_handle* h, int64_t* n) {
+    if (!n) return fail(h, CAV_ERR_ARG, "null output");
+    return guarded(h, [&](Solver& s) { *n = s.launches; });
+}
+
+}  // extern "C"
+
+namespace cav {
+Solver* make_solver_f64();
+Solver* make_solver_f32();
+Solver* make_solver_f16();
+Solver* make_solver_bf16();
+
+Solver* make_solver(int precision) {
+    switch (precision) {
+        case CAV_PREC_F64: return make_solver_f64();
+        case CAV_PREC_F32: return make_solver_f32();
+        case CAV_PREC_F16: return make_solver_f16();
+        default: return make_solver_bf16();
+    }
+}
+}  // namespace cav

@@ -1,0 +1,406 @@
+// kernels.cuh -- device kernels of the uniform cavity step.
+//
+// Two representations of one state (see cavity.cu):
+//   REF  the reference's own: post-stream f, g plus rho, u, T fields
+//        (what CavitySolver holds between step() calls, src/uniform/solver.rs:35-104);
+//   PC   post-collision f*, g* of the last collide (the form the fused
+//        kernel streams from).
+// k_fused advances PC -> PC by one reference step in one pass: pull-stream
+// with bounce-back for f, thermal boundary conditions for g, macroscopic
+// update with the Guo half-force correction, no-slip, then the collision of
+// the next step.  This is the reference order collide -> stream -> BC ->
+// macroscopic -> no-slip (solver.rs:279-293) rotated by one phase.
+#pragma once
+
+#include "lattice.cuh"
+
+namespace cav {
+
+template <class St>
+__device__ __forceinline__ typename Fmt<St>::A ldp(const St* __restrict__ buf, const Geom& G, int q, int iy,
+                                                  int ix) {
+    return Fmt<St>::load(buf[(long long)q * G.plane + (long long)iy * G.pitch + ix]);
+}
+template <class St>
+__device__ __forceinline__ void stp(St* __restrict__ buf, const Geom& G, int q, int iy, int ix,
+                                    typename Fmt<St>::A v) {
+    buf[(long long)q * G.plane + (long long)iy * G.pitch + ix] = Fmt<St>::store(v);
+}
+
+// Pull-stream of one node from a PC buffer (stream, solver.rs:838-913) fused
+// with the thermal boundary conditions (solver.rs:951-988):
+//  f_i(x) = f*_i(x - c_i) in the domain, else f*_opp(i)(x) (bounce-back);
+//  g on x = 0 / x = nx-1 is geq(T_wall, 0, 0); rows y = 0 / ny-1 take the
+//  post-stream g of rows 1 / ny-2 (corners: the vertical wall value of that
+//  row, as the vertical loop runs first).  Every other g source is inside
+//  the domain, so the reference's "keep g at out-of-domain sources" value
+//  is always overwritten and never needed here.
+template <class St>
+__device__ __forceinline__ void pull_node(const St* __restrict__ src, const Geom& G, int ix, int iy,
+                                          const StepScalars<typename Fmt<St>::A>& c,
+                                          typename Fmt<St>::A (&f)[Q], typename Fmt<St>::A (&g)[Q]) {
+    using A = typename Fmt<St>::A;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const int sx = ix - CX(i), sy = iy - CY(i);
+        if (sx >= 0 && sx < G.nx && sy >= 0 && sy < G.ny)
+            f[i] = ldp(src, G, i, sy, sx);
+        else
+            f[i] = ldp(src, G, OPP(i), iy, ix);
+    }
+    const int gy = iy == 0 ? 1 : (iy == G.ny - 1 ? G.ny - 2 : iy);
+    if (ix == 0) {
+        const A tw = c.t_hot[gy];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) g[i] = geq_rest<A>(i, tw, c.geq_order);
+    } else if (ix == G.nx - 1) {
+#pragma unroll
+        for (int i = 0; i < Q; ++i) g[i] = geq_rest<A>(i, c.t_cold, c.geq_order);
+    } else {
+#pragma unroll
+        for (int i = 0; i < Q; ++i) g[i] = ldp(src, G, Q + i, gy - CY(i), ix - CX(i));
+    }
+}
+
+// Temperature of node (ix, iy) of the streamed state, gathered from a PC
+// buffer (used for the per-step Nusselt accumulation).
+template <class St>
+__device__ __forceinline__ typename Fmt<St>::A gather_t(const St* __restrict__ src, const Geom& G, int ix, int iy,
+                                                       const StepScalars<typename Fmt<St>::A>& c) {
+    using A = typename Fmt<St>::A;
+    const int gy = iy == 0 ? 1 : (iy == G.ny - 1 ? G.ny - 2 : iy);
+    A g[Q];
+    if (ix == 0) {
+#pragma unroll
+        for (int i = 0; i < Q; ++i) g[i] = geq_rest<A>(i, c.t_hot[gy], c.geq_order);
+    } else if (ix == G.nx - 1) {
+#pragma unroll
+        for (int i = 0; i < Q; ++i) g[i] = geq_rest<A>(i, c.t_cold, c.geq_order);
+    } else {
+#pragma unroll
+        for (int i = 0; i < Q; ++i) g[i] = ldp(src, G, Q + i, gy - CY(i), ix - CX(i));
+    }
+    A t = g[0];
+#pragma unroll
+    for (int j = 1; j < Q; ++j) t = t + g[j];
+    return t;
+}
+
+__device__ __forceinline__ bool is_wall(const Geom& G, int ix, int iy) {
+    return ix == 0 || ix == G.nx - 1 || iy == 0 || iy == G.ny - 1;
+}
+
+// One full reference step, PC(src) -> PC(dst).
+//  WRITE_NUT   store nu_t of this collision (only the last step of a call
+//              needs it: the reference reads nu_t after step()).
+//  ACC_NU      add |T(1)-T(2)| and |T(nx-2)-T(nx-3)| of the streamed state
+//              to the per-row FP64 accumulators (nusselt_hot/cold, post.rs:68-111).
+//  NO_COLLIDE  identity collision: checks the streaming / bounce-back /
+//              boundary index maps bit for bit.
+template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE>
+__global__ void __launch_bounds__(256) k_fused(const St* __restrict__ src, St* __restrict__ dst,
+                                               typename Fmt<St>::A* __restrict__ fy,
+                                               typename Fmt<St>::A* __restrict__ nut, double* __restrict__ acc_hot,
+                                               double* __restrict__ acc_cold, Geom G,
+                                               StepScalars<typename Fmt<St>::A> c) {
+    using A = typename Fmt<St>::A;
+    constexpr bool SH = Fmt<St>::SHIFT;
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= G.nx || iy >= G.ny) return;
+    const long long k = (long long)iy * G.pitch + ix;
+    A f[Q], g[Q];
+    pull_node<St>(src, G, ix, iy, c, f, g);
+    const bool wall = is_wall(G, ix, iy);
+    Macro<A, SH> m = macro_node<A, SH>(f, g, fy[k], wall);
+    if (ACC_NU) {
+        if (ix == 1) {
+            A t2 = gather_t<St>(src, G, 2, iy, c);
+            acc_hot[iy] += fabs(double(m.t) - double(t2));
+        }
+        if (ix == G.nx - 2) {
+            A t0 = gather_t<St>(src, G, G.nx - 3, iy, c);
+            acc_cold[iy] += fabs(double(m.t) - double(t0));
+        }
+    }
+    A fyv, nutv;
+    if (!NO_COLLIDE) {
+        collide_node<A, SH>(f, g, m, c, fyv, nutv);
+        fy[k] = fyv;
+        if (WRITE_NUT) nut[k] = nutv;
+    }
+#pragma unroll
+    for (int i = 0; i < Q; ++i) stp(dst, G, i, iy, ix, f[i]);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) stp(dst, G, Q + i, iy, ix, g[i]);
+}
+
+// collide(step) on a REF state (populations + fields), writing PC to dst.
+// This is the reference's first phase of step() when the state comes from
+// new()/init_from_fields() or from the debug phases.
+template <class St>
+__global__ void __launch_bounds__(256) k_collide_ref(const St* __restrict__ src, St* __restrict__ dst,
+                                                     const typename Fmt<St>::A* __restrict__ rho,
+                                                     const typename Fmt<St>::A* __restrict__ ux,
+                                                     const typename Fmt<St>::A* __restrict__ uy,
+                                                     const typename Fmt<St>::A* __restrict__ tt,
+                                                     typename Fmt<St>::A* __restrict__ fy,
+                                                     typename Fmt<St>::A* __restrict__ nut, Geom G,
+                                                     StepScalars<typename Fmt<St>::A> c) {
+    using A = typename Fmt<St>::A;
+    constexpr bool SH = Fmt<St>::SHIFT;
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= G.nx || iy >= G.ny) return;
+    const long long k = (long long)iy * G.pitch + ix;
+    A f[Q], g[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        f[i] = ldp(src, G, i, iy, ix);
+        g[i] = ldp(src, G, Q + i, iy, ix);
+    }
+    Macro<A, SH> m;
+    m.rho = rho[k];
+    m.drho = m.rho - A(1.0);
+    m.ux = ux[k];
+    m.uy = uy[k];
+    m.t = tt[k];
+    A fyv, nutv;
+    collide_node<A, SH>(f, g, m, c, fyv, nutv);
+    fy[k] = fyv;
+    nut[k] = nutv;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) stp(dst, G, i, iy, ix, f[i]);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) stp(dst, G, Q + i, iy, ix, g[i]);
+}
+
+// PC(src) -> REF(dst): stream + thermal BC + macroscopic + no-slip, without
+// the next collision.  Produces the reference's observable state.
+template <class St>
+__global__ void __launch_bounds__(256) k_materialize(const St* __restrict__ src, St* __restrict__ dst,
+                                                     const typename Fmt<St>::A* __restrict__ fy,
+                                                     typename Fmt<St>::A* __restrict__ rho,
+                                                     typename Fmt<St>::A* __restrict__ ux,
+                                                     typename Fmt<St>::A* __restrict__ uy,
+                                                     typename Fmt<St>::A* __restrict__ tt, Geom G,
+                                                     StepScalars<typename Fmt<St>::A> c) {
+    using A = typename Fmt<St>::A;
+    constexpr bool SH = Fmt<St>::SHIFT;
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= G.nx || iy >= G.ny) return;
+    const long long k = (long long)iy * G.pitch + ix;
+    A f[Q], g[Q];
+    pull_node<St>(src, G, ix, iy, c, f, g);
+    Macro<A, SH> m = macro_node<A, SH>(f, g, fy[k], is_wall(G, ix, iy));
+    rho[k] = m.rho;
+    ux[k] = m.ux;
+    uy[k] = m.uy;
+    tt[k] = m.t;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) stp(dst, G, i, iy, ix, f[i]);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) stp(dst, G, Q + i, iy, ix, g[i]);
+}
+
+// Nusselt accumulation of the streamed state of a PC buffer (one thread per row).
+template <class St>
+__global__ void k_acc_nu_pc(const St* __restrict__ src, double* __restrict__ acc_hot, double* __restrict__ acc_cold,
+                            Geom G, StepScalars<typename Fmt<St>::A> c) {
+    const int iy = blockIdx.x * blockDim.x + threadIdx.x;
+    if (iy >= G.ny) return;
+    double t1 = gather_t<St>(src, G, 1, iy, c), t2 = gather_t<St>(src, G, 2, iy, c);
+    double tc2 = gather_t<St>(src, G, G.nx - 2, iy, c), tc3 = gather_t<St>(src, G, G.nx - 3, iy, c);
+    acc_hot[iy] += fabs(t1 - t2);
+    acc_cold[iy] += fabs(tc2 - tc3);
+}
+
+// Same on a REF state (temperature field).
+template <class A>
+__global__ void k_acc_nu_ref(const A* __restrict__ tt, double* __restrict__ acc_hot, double* __restrict__ acc_cold,
+                             Geom G) {
+    const int iy = blockIdx.x * blockDim.x + threadIdx.x;
+    if (iy >= G.ny) return;
+    const long long r = (long long)iy * G.pitch;
+    acc_hot[iy] += fabs(double(tt[r + 1]) - double(tt[r + 2]));
+    acc_cold[iy] += fabs(double(tt[r + G.nx - 2]) - double(tt[r + G.nx - 3]));
+}
+
+// ---------------------------------------------------------------------------
+// Debug phases on a REF state (the pub(crate) methods of the reference,
+// called one at a time by src/uniform/tests.rs:154-169).
+// ---------------------------------------------------------------------------
+// collide(step), src/uniform/solver.rs:421-540, in place.
+template <class St>
+__global__ void k_dbg_collide(St* __restrict__ pop, const typename Fmt<St>::A* __restrict__ rho,
+                              const typename Fmt<St>::A* __restrict__ ux, const typename Fmt<St>::A* __restrict__ uy,
+                              const typename Fmt<St>::A* __restrict__ tt, typename Fmt<St>::A* __restrict__ fy,
+                              typename Fmt<St>::A* __restrict__ nut, Geom G, StepScalars<typename Fmt<St>::A> c) {
+    using A = typename Fmt<St>::A;
+    constexpr bool SH = Fmt<St>::SHIFT;
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= G.nx || iy >= G.ny) return;
+    const long long k = (long long)iy * G.pitch + ix;
+    A f[Q], g[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        f[i] = ldp(pop, G, i, iy, ix);
+        g[i] = ldp(pop, G, Q + i, iy, ix);
+    }
+    Macro<A, SH> m;
+    m.rho = rho[k];
+    m.drho = m.rho - A(1.0);
+    m.ux = ux[k];
+    m.uy = uy[k];
+    m.t = tt[k];
+    A fyv, nutv;
+    collide_node<A, SH>(f, g, m, c, fyv, nutv);
+    fy[k] = fyv;
+    nut[k] = nutv;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        stp(pop, G, i, iy, ix, f[i]);
+        stp(pop, G, Q + i, iy, ix, g[i]);
+    }
+}
+
+// stream(), src/uniform/solver.rs:838-913: pull, bounce-back for f, g kept
+// at out-of-domain sources.
+template <class St>
+__global__ void k_dbg_stream(const St* __restrict__ src, St* __restrict__ dst, Geom G) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= G.nx || iy >= G.ny) return;
+    const long long k = (long long)iy * G.pitch + ix;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const int sx = ix - CX(i), sy = iy - CY(i);
+        if (sx >= 0 && sx < G.nx && sy >= 0 && sy < G.ny) {
+            const long long s = (long long)sy * G.pitch + sx;
+            dst[i * G.plane + k] = src[i * G.plane + s];
+            dst[(Q + i) * G.plane + k] = src[(Q + i) * G.plane + s];
+        } else {
+            dst[i * G.plane + k] = src[OPP(i) * G.plane + k];
+            dst[(Q + i) * G.plane + k] = src[(Q + i) * G.plane + k];
+        }
+    }
+}
+
+// apply_bounce_back / swap_opposite, src/uniform/solver.rs:920-946: on every
+// wall node swap f_i and f_opp(i) for i = 1..4 (corners are visited twice).
+template <class St>
+__global__ void k_dbg_bounce_back(St* __restrict__ pop, Geom G) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= G.nx || iy >= G.ny) return;
+    int visits = (ix == 0 || ix == G.nx - 1 ? 1 : 0) + (iy == 0 || iy == G.ny - 1 ? 1 : 0);
+    if (visits % 2 == 0) return;  // not a wall node, or a corner swapped twice
+    const long long k = (long long)iy * G.pitch + ix;
+#pragma unroll
+    for (int i = 1; i < 5; ++i) {
+        St a = pop[i * G.plane + k];
+        pop[i * G.plane + k] = pop[OPP(i) * G.plane + k];
+        pop[OPP(i) * G.plane + k] = a;
+    }
+}
+
+// apply_thermal_boundary_conditions, src/uniform/solver.rs:951-988, vertical walls.
+template <class St>
+__global__ void k_dbg_thermal_v(St* __restrict__ pop, Geom G, StepScalars<typename Fmt<St>::A> c) {
+    using A = typename Fmt<St>::A;
+    const int iy = blockIdx.x * blockDim.x + threadIdx.x;
+    if (iy >= G.ny) return;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        stp(pop, G, Q + i, iy, 0, geq_rest<A>(i, c.t_hot[iy], c.geq_order));
+        stp(pop, G, Q + i, iy, G.nx - 1, geq_rest<A>(i, c.t_cold, c.geq_order));
+    }
+}
+// ... then the horizontal walls copy rows 1 and ny-2.
+template <class St>
+__global__ void k_dbg_thermal_h(St* __restrict__ pop, Geom G) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ix >= G.nx) return;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const long long p = (long long)(Q + i) * G.plane;
+        pop[p + ix] = pop[p + G.pitch + ix];
+        pop[p + (long long)(G.ny - 1) * G.pitch + ix] = pop[p + (long long)(G.ny - 2) * G.pitch + ix];
+    }
+}
+
+// update_macroscopic, src/uniform/solver.rs:298-367 (no wall override).
+template <class St>
+__global__ void k_dbg_macro(const St* __restrict__ pop, const typename Fmt<St>::A* __restrict__ fy,
+                            typename Fmt<St>::A* __restrict__ rho, typename Fmt<St>::A* __restrict__ ux,
+                            typename Fmt<St>::A* __restrict__ uy, typename Fmt<St>::A* __restrict__ tt, Geom G) {
+    using A = typename Fmt<St>::A;
+    constexpr bool SH = Fmt<St>::SHIFT;
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= G.nx || iy >= G.ny) return;
+    const long long k = (long long)iy * G.pitch + ix;
+    A f[Q], g[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        f[i] = ldp(pop, G, i, iy, ix);
+        g[i] = ldp(pop, G, Q + i, iy, ix);
+    }
+    Macro<A, SH> m = macro_node<A, SH>(f, g, fy[k], false);
+    rho[k] = m.rho;
+    ux[k] = m.ux;
+    uy[k] = m.uy;
+    tt[k] = m.t;
+}
+
+// enforce_wall_velocity, src/uniform/solver.rs:992-1009.
+template <class A>
+__global__ void k_dbg_noslip(A* __restrict__ ux, A* __restrict__ uy, Geom G) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= G.nx || iy >= G.ny) return;
+    if (!is_wall(G, ix, iy)) return;
+    const long long k = (long long)iy * G.pitch + ix;
+    ux[k] = A(0.0);
+    uy[k] = A(0.0);
+}
+
+// ---------------------------------------------------------------------------
+// Population format conversion (ABI arrays are FP64 AoS [k][9]).
+// ---------------------------------------------------------------------------
+template <class St>
+__global__ void k_pops_to_aos(const St* __restrict__ pop, double* __restrict__ f, double* __restrict__ g, Geom G) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= G.nx || iy >= G.ny) return;
+    const long long k = (long long)iy * G.nx + ix;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        double fv = double(ldp(pop, G, i, iy, ix));
+        if (Fmt<St>::SHIFT) fv += WD(i);
+        f[k * Q + i] = fv;
+        g[k * Q + i] = double(ldp(pop, G, Q + i, iy, ix));
+    }
+}
+template <class St>
+__global__ void k_aos_to_pops(St* __restrict__ pop, const double* __restrict__ f, const double* __restrict__ g,
+                              int do_f, int do_g, Geom G) {
+    using A = typename Fmt<St>::A;
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= G.nx || iy >= G.ny) return;
+    const long long k = (long long)iy * G.nx + ix;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        if (do_f) {
+            double fv = f[k * Q + i];
+            if (Fmt<St>::SHIFT) fv -= WD(i);
+            stp(pop, G, i, iy, ix, A(fv));
+        }
+        if (do_g) stp(pop, G, Q + i, iy, ix, A(g[k * Q + i]));
+    }
+}
+
+}  // namespace cav

@@ -1,0 +1,293 @@
+// lattice.cuh -- D2Q9 constants, storage formats and the per-node physics of
+// the differentially heated cavity step (bbrangeo/cfd_cavity
+// src/uniform/solver.rs), shared by every kernel of the library.
+//
+// Populations live on the device as 18 SoA planes (9 for f, 9 for g) of
+// ny rows x pitch columns.  Four storage formats:
+//   double         FP64 arithmetic, unshifted (the parity variant);
+//   float          FP32 arithmetic, f stored as f_i - w_i;
+//   __half         FP32 arithmetic, f_i - w_i and g_i scaled by 2^15 into
+//                  IEEE binary16 (Lehmann et al. 2022, "FP16S" storage);
+//   __nv_bfloat16  FP32 arithmetic, f_i - w_i and g_i in bfloat16.
+// g is shifted by w_i * T0 with T0 = 0, i.e. stored as is: theta is centred
+// on zero in this problem (walls at +-0.5).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+namespace cav {
+
+constexpr int Q = 9;
+constexpr int NPLANES = 18;  // f planes 0..8, g planes 9..17
+
+// Direction order: rest, E, N, NE, NW, W, S, SW, SE  (OPP[i] = i +- 4).
+__host__ __device__ constexpr int CX(int i) {
+    return i == 1 || i == 3 || i == 8 ? 1 : (i == 4 || i == 5 || i == 7 ? -1 : 0);
+}
+__host__ __device__ constexpr int CY(int i) {
+    return i == 2 || i == 3 || i == 4 ? 1 : (i == 6 || i == 7 || i == 8 ? -1 : 0);
+}
+__host__ __device__ constexpr int OPP(int i) { return i == 0 ? 0 : (i <= 4 ? i + 4 : i - 4); }
+__host__ __device__ constexpr double WD(int i) {
+    return i == 0 ? 4.0 / 9.0 : (i == 1 || i == 2 || i == 5 || i == 6 ? 1.0 / 9.0 : 1.0 / 36.0);
+}
+constexpr double CS2 = 1.0 / 3.0;
+constexpr double LAMBDA_TRT = 3.0 / 16.0;
+
+// ---------------------------------------------------------------------------
+// Storage formats.
+// ---------------------------------------------------------------------------
+template <class St>
+struct Fmt;
+
+template <>
+struct Fmt<double> {
+    using A = double;
+    static constexpr bool SHIFT = false;
+    static constexpr int PREC = 0;
+    __host__ __device__ static A load(double v) { return v; }
+    __host__ __device__ static double store(A v) { return v; }
+};
+template <>
+struct Fmt<float> {
+    using A = float;
+    static constexpr bool SHIFT = true;
+    static constexpr int PREC = 1;
+    __host__ __device__ static A load(float v) { return v; }
+    __host__ __device__ static float store(A v) { return v; }
+};
+template <>
+struct Fmt<__half> {
+    using A = float;
+    static constexpr bool SHIFT = true;
+    static constexpr int PREC = 2;
+    static constexpr float SCALE = 32768.0f;
+    static constexpr float INV_SCALE = 1.0f / 32768.0f;
+    __host__ __device__ static A load(__half v) { return __half2float(v) * INV_SCALE; }
+    __host__ __device__ static __half store(A v) { return __float2half_rn(v * SCALE); }
+};
+template <>
+struct Fmt<__nv_bfloat16> {
+    using A = float;
+    static constexpr bool SHIFT = true;
+    static constexpr int PREC = 3;
+    __host__ __device__ static A load(__nv_bfloat16 v) { return __bfloat162float(v); }
+    __host__ __device__ static __nv_bfloat16 store(A v) { return __float2bfloat16_rn(v); }
+};
+
+// Grid geometry of one cavity.
+struct Geom {
+    int nx, ny, pitch;
+    long long plane;  // ny * pitch
+};
+
+// Per-launch scalars of collide (CollideCtx, src/uniform/solver.rs:1034-1043)
+// plus the boundary data.  Computed on the host in FP64 for each step, then
+// converted to the arithmetic type.
+template <class A>
+struct StepScalars {
+    A tau_s;   // tau used for |S|: 0.5 + 3*max(nu_eff, 0.002/3)  (solver.rs:442)
+    A beta;    // ramped beta_eff                                   (solver.rs:433-437)
+    A nu;      // ramped nu_eff                                     (solver.rs:390-400)
+    A alpha;   // ramped alpha_eff                                  (solver.rs:401-408)
+    A cs;      // Smagorinsky constant
+    A pr_t;    // turbulent Prandtl number
+    A t_cold;  // cold-wall theta
+    int geq_order;
+    const A* t_hot;  // [ny] hot-wall theta
+};
+
+// ---------------------------------------------------------------------------
+// Equilibria.  In the unshifted (FP64) form the expressions are those of the
+// reference (feq form restated at src/uniform/tests.rs:314-316); the shifted
+// form returns feq_i - w_i from (drho = rho - 1, rho).
+// ---------------------------------------------------------------------------
+template <class A>
+__host__ __device__ __forceinline__ A feq_full(int i, A rho, A ux, A uy) {
+    const A cs2 = A(CS2);
+    A eu = A(CX(i)) * ux + A(CY(i)) * uy;
+    A u2 = ux * ux + uy * uy;
+    return A(WD(i)) * rho * (A(1.0) + eu / cs2 + eu * eu / (A(2.0) * cs2 * cs2) - u2 / (A(2.0) * cs2));
+}
+
+template <class A>
+__host__ __device__ __forceinline__ A geq_full(int i, A t, A ux, A uy, int order) {
+    const A cs2 = A(CS2);
+    A eu = A(CX(i)) * ux + A(CY(i)) * uy;
+    if (order == 1) return A(WD(i)) * t * (A(1.0) + eu / cs2);
+    A u2 = ux * ux + uy * uy;
+    return A(WD(i)) * t * (A(1.0) + eu / cs2 + eu * eu / (A(2.0) * cs2 * cs2) - u2 / (A(2.0) * cs2));
+}
+
+// FP32 shifted equilibrium: feq_i - w_i = w_i*(drho + rho*P_i),
+// P_i = 3 e.u + 4.5 (e.u)^2 - 1.5 u^2.
+__device__ __forceinline__ float feq_shift_f32(int i, float drho, float rho, float ux, float uy) {
+    float eu = float(CX(i)) * ux + float(CY(i)) * uy;
+    float u2 = ux * ux + uy * uy;
+    float P = 3.0f * eu + 4.5f * eu * eu - 1.5f * u2;
+    return float(WD(i)) * (drho + rho * P);
+}
+__device__ __forceinline__ float geq_f32(int i, float t, float ux, float uy, int order) {
+    float eu = float(CX(i)) * ux + float(CY(i)) * uy;
+    if (order == 1) return float(WD(i)) * t * (1.0f + 3.0f * eu);
+    float u2 = ux * ux + uy * uy;
+    return float(WD(i)) * t * (1.0f + 3.0f * eu + 4.5f * eu * eu - 1.5f * u2);
+}
+
+// ---------------------------------------------------------------------------
+// Macroscopic update of one node (update_macroscopic, src/uniform/solver.rs:
+// 298-367, then enforce_wall_velocity :992-1009 when `wall`).  Sums run in
+// the reference's direction order so that FP64 results are bit-identical.
+// ---------------------------------------------------------------------------
+template <class A, bool SHIFT>
+struct Macro {
+    A rho, drho, ux, uy, t;
+};
+
+template <class A, bool SHIFT>
+__device__ __forceinline__ Macro<A, SHIFT> macro_node(const A (&f)[Q], const A (&g)[Q], A fy_prev, bool wall) {
+    Macro<A, SHIFT> m;
+    A s = f[0];
+#pragma unroll
+    for (int j = 1; j < Q; ++j) s = s + f[j];
+    A un = ((((f[1] + f[3]) - f[4]) - f[5]) - f[7]) + f[8];
+    A vn = ((((f[2] + f[3]) + f[4]) - f[6]) - f[7]) - f[8];
+    A tn = g[0];
+#pragma unroll
+    for (int j = 1; j < Q; ++j) tn = tn + g[j];
+    A r;
+    if (SHIFT) {
+        m.drho = s;
+        r = A(1.0) + s;
+    } else {
+        r = s;
+        m.drho = s - A(1.0);
+    }
+    if (SHIFT) {
+        A inv = A(1.0) / r;
+        un = un * inv;
+        vn = vn * inv + A(0.5) * fy_prev * inv;
+    } else if (r > A(2.220446049250313e-16)) {
+        un = un / r;
+        vn = vn / r;
+        vn = vn + A(0.5) * fy_prev / r;
+    }
+    m.rho = r;
+    m.ux = wall ? A(0.0) : un;
+    m.uy = wall ? A(0.0) : vn;
+    m.t = tn;
+    return m;
+}
+
+// ---------------------------------------------------------------------------
+// Collision of one node: TRT + Smagorinsky + Guo forcing for f, BGK for g
+// (collide_node, src/uniform/solver.rs:1054-1185, fixed-Cs branch).
+// f and g are updated in place; returns fy and nu_t.
+// FP64 follows the reference expression by expression; the FP32 variant
+// works on f_i - w_i and replaces divisions by constants with products.
+// ---------------------------------------------------------------------------
+template <class A, bool SHIFT>
+__device__ __forceinline__ void collide_node(A (&f)[Q], A (&g)[Q], const Macro<A, SHIFT>& m,
+                                             const StepScalars<A>& c, A& fy_out, A& nut_out) {
+    const A r = m.rho, u = m.ux, v = m.uy, temp = m.t;
+    if constexpr (!SHIFT) {
+        // ---- FP64: expression order of the reference ----------------------
+        const double cs2 = CS2;
+        double fyv = r * c.beta * 1.0 * (temp - 0.0);
+        fy_out = fyv;
+        double f_eq[Q], g_eq[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            f_eq[i] = feq_full<double>(i, r, u, v);
+            g_eq[i] = geq_full<double>(i, temp, u, v, c.geq_order);
+        }
+        double d_f[Q], d_g[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            d_f[i] = f[i] - f_eq[i];
+            d_g[i] = g[i] - g_eq[i];
+        }
+        // pi_neq, solver.rs:1096-1106 (terms with c = 0 add +-0).
+        double pxx = ((((d_f[1] + d_f[3]) + d_f[4]) + d_f[5]) + d_f[7]) + d_f[8];
+        double pxy = ((d_f[3] - d_f[4]) + d_f[7]) - d_f[8];
+        double pyy = ((((d_f[2] + d_f[3]) + d_f[4]) + d_f[6]) + d_f[7]) + d_f[8];
+        double pi2 = pxx * pxx + 2.0 * pxy * pxy + pyy * pyy;
+        double rho_m = r > 1e-12 ? r : 1e-12;
+        double s_mag = sqrt(pi2) / (2.0 * cs2 * c.tau_s * rho_m);
+        double nut = c.cs * c.cs * s_mag;
+        nut_out = nut;
+        double tau_plus = 0.5 + 3.0 * (c.nu + nut);
+        double tau_minus = 0.5 + LAMBDA_TRT / (tau_plus - 0.5);
+        double alpha_t = nut / c.pr_t;
+        double tau_t_plus = 0.5 + 3.0 * (c.alpha + alpha_t);
+        double tau_t_minus = tau_t_plus;
+        double a_f = 0.5 * (1.0 / tau_plus + 1.0 / tau_minus);
+        double b_f = 0.5 * (1.0 / tau_plus - 1.0 / tau_minus);
+        double a_g = 0.5 * (1.0 / tau_t_plus + 1.0 / tau_t_minus);
+        double b_g = 0.5 * (1.0 / tau_t_plus - 1.0 / tau_t_minus);
+        double k_minus = 1.0 - 0.5 / tau_minus;
+        double k_plus = 1.0 - 0.5 / tau_plus;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const double cx = CX(i), cy = CY(i);
+            double ei_u = cx * u + cy * v;
+            double s_i = WD(i) * ((cy - v) / cs2 + ei_u * cy / (cs2 * cs2)) * fyv;
+            double s_minus = WD(i) * (cy / cs2) * fyv;
+            double s_plus = s_i - s_minus;
+            f[i] = f[i] + (-a_f * d_f[i] - b_f * d_f[OPP(i)] + k_minus * s_minus + k_plus * s_plus);
+        }
+#pragma unroll
+        for (int i = 0; i < Q; ++i) g[i] = g[i] + (-a_g * d_g[i] - b_g * d_g[OPP(i)]);
+    } else {
+        // ---- FP32 on f_i - w_i ---------------------------------------------
+        float fyv = r * c.beta * temp;
+        fy_out = fyv;
+        float d_f[Q], d_g[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            d_f[i] = f[i] - feq_shift_f32(i, m.drho, r, u, v);
+            d_g[i] = g[i] - geq_f32(i, temp, u, v, c.geq_order);
+        }
+        float pxx = ((((d_f[1] + d_f[3]) + d_f[4]) + d_f[5]) + d_f[7]) + d_f[8];
+        float pxy = ((d_f[3] - d_f[4]) + d_f[7]) - d_f[8];
+        float pyy = ((((d_f[2] + d_f[3]) + d_f[4]) + d_f[6]) + d_f[7]) + d_f[8];
+        float pi2 = pxx * pxx + 2.0f * pxy * pxy + pyy * pyy;
+        float rho_m = fmaxf(r, 1e-12f);
+        // |S| = sqrt(pi:pi) / (2 cs^2 tau rho), 2 cs^2 = 2/3.
+        float s_mag = sqrtf(pi2) / ((2.0f / 3.0f) * c.tau_s * rho_m);
+        float nut = c.cs * c.cs * s_mag;
+        nut_out = nut;
+        float tau_plus = 0.5f + 3.0f * (c.nu + nut);
+        float tau_minus = 0.5f + float(LAMBDA_TRT) / (tau_plus - 0.5f);
+        float tau_t = 0.5f + 3.0f * (c.alpha + nut / c.pr_t);
+        float om_p = 1.0f / tau_plus, om_m = 1.0f / tau_minus;
+        float a_f = 0.5f * (om_p + om_m);
+        float b_f = 0.5f * (om_p - om_m);
+        float a_g = 1.0f / tau_t;  // BGK for g (tau_t- = tau_t+), b_g = 0
+        float k_minus = 1.0f - 0.5f * om_m;
+        float k_plus = 1.0f - 0.5f * om_p;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const float cx = CX(i), cy = CY(i);
+            float ei_u = cx * u + cy * v;
+            // S_i = w_i [3 (c_y - u_y) + 9 (e.u) c_y] fy ; odd part w_i 3 c_y fy.
+            float s_i = float(WD(i)) * (3.0f * (cy - v) + 9.0f * ei_u * cy) * fyv;
+            float s_minus = float(WD(i)) * (3.0f * cy) * fyv;
+            float s_plus = s_i - s_minus;
+            f[i] = f[i] + (-a_f * d_f[i] - b_f * d_f[OPP(i)] + k_minus * s_minus + k_plus * s_plus);
+        }
+#pragma unroll
+        for (int i = 0; i < Q; ++i) g[i] = g[i] - a_g * d_g[i];
+    }
+}
+
+// Wall-node equilibrium of g (apply_thermal_boundary_conditions,
+// src/uniform/solver.rs:957-970): geq(T_wall, 0, 0) = w_i T_wall.
+template <class A>
+__device__ __forceinline__ A geq_rest(int i, A t, int order) {
+    return geq_full<A>(i, t, A(0.0), A(0.0), order);
+}
+
+}  // namespace cav

@@ -1,0 +1,182 @@
+/* cavity.h -- C ABI of the B200 lattice-Boltzmann step for the 2D
+ * differentially heated cavity (drop-in for bbrangeo/cfd_cavity's step).
+ *
+ * The reference exposes its step through the Rust type
+ * `uniform::solver::CavitySolver` (src/uniform/solver.rs:35-104); it has no
+ * FFI of its own.  Each entry point below replaces one method of that type,
+ * or one direct field access its callers make, and names the reference
+ * interface it stands for.  A Rust caller binds them with `extern "C"`
+ * (see INTEGRATION.md).
+ *
+ * Conventions
+ *  - Every function returns an int status (CAV_OK = 0) and never aborts or
+ *    traps; cav_last_error() gives a one-line message for the last failure
+ *    on a handle.  The reference panics or exit()s instead
+ *    (src/uniform/solver.rs:130-132, 152-154, 236-240; src/main.rs:209-276).
+ *  - Host arrays are caller-owned, row-major k = iy*nx + ix (the reference
+ *    index, src/uniform/solver.rs:224-226), FP64, copied synchronously.
+ *  - Populations cross the ABI in the reference's AoS layout [k][9]; the
+ *    direction order is D2Q9 rest, E, N, NE, NW, W, S, SW, SE
+ *    (c_{i+4} = -c_i for i = 1..4).
+ *  - One handle is driven by one host thread at a time; it owns one CUDA
+ *    stream and all of its device buffers.  Results are deterministic (no
+ *    floating-point atomics).
+ */
+#ifndef CAVITY_B200_H
+#define CAVITY_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define CAV_OK 0
+#define CAV_ERR_ARG 1      /* invalid argument or size                       */
+#define CAV_ERR_TAU 2      /* tau+ or tau_t too close to 1/2 (solver.rs:152-154) */
+#define CAV_ERR_DIVERGED 3 /* non-finite field (post.rs:406-411, main.rs:230-275) */
+#define CAV_ERR_MAXU 4     /* max|u| above the 0.10 guard (main.rs:46, 209-228) */
+#define CAV_ERR_TIMEOUT 5  /* a bounded device wait gave up                 */
+#define CAV_ERR_CUDA 6     /* CUDA runtime error                             */
+#define CAV_ERR_STATE 7    /* call not valid in the handle's current state   */
+#define CAV_ERR_NOMEM 8    /* device allocation failed                       */
+
+/* ---- enumerations -------------------------------------------------------- */
+/* Storage precision of the populations (arithmetic: FP64 for CAV_PREC_F64,
+ * FP32 otherwise; the 16-bit formats store f_i - w_i). */
+#define CAV_PREC_F64 0
+#define CAV_PREC_F32 1
+#define CAV_PREC_F16 2
+#define CAV_PREC_BF16 3
+
+/* Initial temperature field. */
+#define CAV_INIT_LINEAR 0 /* linear theta + noise, CavitySolver::new (solver.rs:159-176) */
+#define CAV_INIT_ZERO 1   /* theta = 0 + noise (benchmark configurations)     */
+
+/* Debug phases: the pub(crate) methods the reference tests call
+ * (src/uniform/tests.rs:154-169). */
+#define CAV_PHASE_COLLIDE 0     /* collide(step)               solver.rs:421-540 */
+#define CAV_PHASE_STREAM 1      /* stream()                    solver.rs:838-913 */
+#define CAV_PHASE_BOUNCE_BACK 2 /* apply_bounce_back()         solver.rs:920-946 */
+#define CAV_PHASE_THERMAL_BC 3  /* apply_thermal_boundary_conditions() :951-988 */
+#define CAV_PHASE_MACRO 4       /* update_macroscopic()        solver.rs:298-367 */
+#define CAV_PHASE_NOSLIP 5      /* enforce_wall_velocity()     solver.rs:992-1009 */
+/* step_arg + 1 passes of the fused step kernel's stream + boundary code with
+ * the collision replaced by the identity, then macroscopic + no-slip: checks
+ * the streaming / bounce-back / thermal-BC index maps of the production
+ * kernel against stream() + apply_thermal_boundary_conditions() bit for bit. */
+#define CAV_PHASE_FUSED_IDENTITY 6
+
+/* ---- parameters ------------------------------------------------------------ */
+/* Arguments of CavitySolver::new (src/uniform/solver.rs:108) plus the
+ * B200-side choices.  Fill with cav_default_params() first. */
+typedef struct cav_params {
+    int32_t nx, ny;          /* nodes in x (width) and y (height)             */
+    double ra, pr, cs, pr_t; /* Rayleigh, Prandtl, Smagorinsky Cs, turbulent Pr */
+    double utarget;          /* velocity target of the nu calibration         */
+    uint64_t seed;           /* xorshift64* seed of the initial noise         */
+    int32_t jobs;            /* accepted for API parity; unused on the GPU    */
+    double alpha_mult;       /* alpha multiplier                              */
+    double nu_start_mult;    /* initial viscosity multiplier (spin-up ramp)   */
+    int32_t has_nu_override; /* 1: use nu_override (the reference's --nu)     */
+    double nu_override;
+    int32_t init_mode;       /* CAV_INIT_*                                    */
+    double noise_amp;        /* amplitude of the uniform noise (ref: 1e-3)    */
+    int32_t geq_order;       /* 2: quadratic g equilibrium (default), 1: linear */
+    const double* t_hot_profile; /* [ny] hot-wall theta per row, or NULL (+0.5) */
+    double t_cold;           /* cold-wall theta (-0.5)                        */
+    int32_t precision;       /* CAV_PREC_*                                    */
+    int32_t device;          /* CUDA device ordinal                           */
+} cav_params;
+
+/* Solver scalars the reference callers read as pub fields
+ * (src/main.rs:131-145: sim.nu, sim.alpha, sim.lbm.tau, ...). */
+typedef struct cav_info {
+    double nu, alpha, alpha_phys, beta_eff, lz, lx, tau, tau_t;
+    int64_t time_step, spin_up_steps;
+    int32_t nx, ny, pitch, precision;
+} cav_info;
+
+/* Diagnostics of the current state (src/uniform/post.rs, src/main.rs:168-276),
+ * reduced on the device in FP64 with a fixed-order tree. */
+typedef struct cav_diag_out {
+    double nusselt_hot;           /* post.rs:68-78  (2nd link, Lz scale)   */
+    double nusselt_cold;          /* post.rs:100-111                        */
+    double nusselt_hot_wall_link; /* post.rs:87-97  (1st link)              */
+    double total_mass;            /* solver.rs:1012-1014  sum rho           */
+    double total_f_mass;          /* solver.rs:1018-1020  sum f             */
+    double max_u;                 /* main.rs:209-214  max(|ux|,|uy|)        */
+    double max_uy;                /* post.rs:153-155                        */
+    double nu_t_max;              /* main.rs:172-175                        */
+    double y_plus_hot;            /* post.rs:182-199                        */
+    double nusselt_volume;        /* post.rs:117-134                        */
+    int32_t finite;               /* post.rs:406-411  (1 = all finite, rho > 0) */
+} cav_diag_out;
+
+typedef struct cav_handle cav_handle;
+
+/* Library version string. */
+const char* cav_version(void);
+/* Default parameters: the reference CLI defaults (src/cli.rs:94-130),
+ * FP64 storage. */
+int cav_default_params(cav_params* p);
+/* CavitySolver::new (src/uniform/solver.rs:108-210). */
+int cav_create(const cav_params* p, cav_handle** out);
+int cav_destroy(cav_handle* h);
+/* Message of the last failure on h (or of the last failed cav_create when h is NULL). */
+const char* cav_last_error(const cav_handle* h);
+/* CavitySolver::init_from_fields (src/uniform/solver.rs:232-262). */
+int cav_init_from_fields(cav_handle* h, const double* rho, const double* ux, const double* uy,
+                         const double* t);
+/* n x CavitySolver::step (src/uniform/solver.rs:279-293). */
+int cav_step(cav_handle* h, int64_t n);
+/* Reads lbm.{rho,ux,uy,temperature}, nu_t, fy_node (any pointer may be NULL). */
+int cav_get_fields(cav_handle* h, double* rho, double* ux, double* uy, double* t, double* nu_t,
+                   double* fy);
+/* Writes lbm.{rho,ux,uy,temperature} and fy_node (NULL = leave unchanged). */
+int cav_set_fields(cav_handle* h, const double* rho, const double* ux, const double* uy,
+                   const double* t, const double* fy);
+/* Reads / writes lbm.f and lbm.g, AoS [k][9] (NULL = skip). */
+int cav_get_populations(cav_handle* h, double* f, double* g);
+int cav_set_populations(cav_handle* h, const double* f, const double* g);
+/* Solver scalars (pub fields, src/uniform/solver.rs:35-104). */
+int cav_get_info(cav_handle* h, cav_info* out);
+/* Sets time_step (the spin-up ramps read it; solver.rs:67, 433). */
+int cav_set_time_step(cav_handle* h, int64_t t);
+/* Diagnostics of the current state. */
+int cav_diag(cav_handle* h, cav_diag_out* out);
+/* Guards of the driver loop (src/main.rs:209-276): CAV_ERR_MAXU when
+ * max|u| > max_u_abort, CAV_ERR_DIVERGED when a field is not finite. */
+int cav_check_guards(cav_handle* h, double max_u_abort);
+/* One pub(crate) phase (CAV_PHASE_*); step_arg is collide's step index. */
+int cav_debug_phase(cav_handle* h, int32_t phase, int64_t step_arg);
+
+/* TimeAverager (src/uniform/post.rs:11-57) kept on the device in FP64.
+ * cav_sample = averager.accumulate(&sim) (src/main.rs:279-281). */
+int cav_sample(cav_handle* h);
+int cav_reset_means(cav_handle* h);
+/* means of ux, uy, T, nu_t, |u|^2 (post.rs:52-56); *n_samples may be NULL. */
+int cav_get_means(cav_handle* h, double* ux, double* uy, double* t, double* nu_t, double* uu,
+                  int64_t* n_samples);
+/* nusselt_from_mean on the mean temperature (src/main.rs:740-753). */
+int cav_nusselt_from_mean(cav_handle* h, int32_t hot, double* out);
+
+/* Per-step Nusselt accumulation: while enabled, every completed step adds the
+ * instantaneous nusselt_hot / nusselt_cold of the new state (post.rs:68-111)
+ * to FP64 accumulators on the device. */
+int cav_nu_accumulate(cav_handle* h, int32_t enable);
+int cav_nu_accumulated(cav_handle* h, double* nu_hot_mean, double* nu_cold_mean, int64_t* n);
+
+/* Blocks until all work queued on the handle's stream has finished. */
+int cav_sync(cav_handle* h);
+/* The handle's CUDA stream (cudaStream_t), for callers that time or order
+ * their own work against the step (no counterpart in the reference). */
+int cav_get_stream(cav_handle* h, void** stream);
+/* Number of kernels the handle has launched so far (graph replays count
+ * every kernel they contain; no counterpart in the reference). */
+int cav_launch_count(cav_handle* h, int64_t* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CAVITY_B200_H */

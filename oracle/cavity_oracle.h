@@ -1,0 +1,78 @@
+/* cavity_oracle.h -- TEST INFRASTRUCTURE ONLY (the oracle).
+ *
+ * C ABI of the CPU FP64 restatement of the reference solver
+ * (bbrangeo/cfd_cavity src/uniform/solver.rs, post.rs, rng.rs).  Loaded by
+ * the tests and by bench.py's CPU baseline through ctypes; never by the
+ * product library.  See cavity_oracle.hpp for the parity status.
+ */
+#ifndef CAVITY_ORACLE_H
+#define CAVITY_ORACLE_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_params {
+    int32_t nx, ny;
+    double ra, pr, cs, pr_t, utarget;
+    uint64_t seed;
+    int32_t jobs;
+    double alpha_mult, nu_start_mult;
+    int32_t has_nu_override;
+    double nu_override;
+    int32_t init_mode;   /* 0 linear theta + noise (reference), 1 theta = 0 + noise */
+    double noise_amp;    /* reference: 1e-3 */
+    int32_t geq_order;   /* 2 quadratic (default), 1 linear */
+    const double* t_hot_profile; /* [ny] or NULL */
+    double t_cold;
+} orc_params;
+
+/* Scalars of the solver: nu, alpha, alpha_phys, beta_eff, lz, lx, tau, tau_t,
+ * time_step, spin_up_steps (10 doubles). */
+#define ORC_INFO_LEN 10
+/* Diagnostics: nusselt_hot, nusselt_cold, nusselt_hot_wall_link, total_mass,
+ * total_f_mass, max_u, max_uy, nu_t_max, finite (1/0), y_plus_hot,
+ * nusselt_volume (11 doubles). */
+#define ORC_DIAG_LEN 11
+
+void* orc_create(const orc_params* p, int32_t* err);
+void orc_destroy(void* h);
+void orc_step(void* h, int64_t n);
+void orc_collide(void* h, int64_t step);
+void orc_stream(void* h);
+void orc_bounce_back(void* h);
+void orc_thermal_bc(void* h);
+void orc_macro(void* h);
+void orc_noslip(void* h);
+void orc_init_from_fields(void* h, const double* rho, const double* ux, const double* uy, const double* t);
+void orc_get_fields(void* h, double* rho, double* ux, double* uy, double* t, double* nu_t, double* fy);
+void orc_set_fields(void* h, const double* rho, const double* ux, const double* uy, const double* t,
+                    const double* fy);
+void orc_get_pops(void* h, double* f, double* g);
+void orc_set_pops(void* h, const double* f, const double* g);
+void orc_info(void* h, double* out);
+void orc_diag(void* h, double* out);
+void orc_set_time_step(void* h, int64_t t);
+
+/* Equilibria and lattice weights (crate oxiphysics_lbm, pinned by
+ * src/uniform/tests.rs:116-133). */
+double orc_feq(int32_t i, double rho, double ux, double uy);
+double orc_geq(int32_t i, double t, double ux, double uy, int32_t order);
+double orc_weight(int32_t i);
+void orc_velocity(int32_t i, int32_t* cx, int32_t* cy);
+/* nusselt_hot, nusselt_cold of the current state (post.rs:68-111). */
+void orc_nusselt(void* h, double* hot, double* cold);
+
+/* TimeAverager (src/uniform/post.rs:11-57). */
+void* orc_avg_create(int64_t n);
+void orc_avg_destroy(void* a);
+void orc_avg_accumulate(void* a, void* h);
+/* means: ux, uy, t, nu_t, uu; returns the sample count. */
+int64_t orc_avg_means(void* a, double* ux, double* uy, double* t, double* nu_t, double* uu);
+/* nusselt_from_mean, src/main.rs:740-753. */
+double orc_nusselt_from_mean(void* h, const double* t_mean, int32_t hot);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

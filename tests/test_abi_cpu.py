@@ -1,0 +1,98 @@
+"""C ABI checks that need no GPU: the library loads, exports every symbol
+include/*.h declares, validates its arguments before touching CUDA, and the
+product never reaches the oracle."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+from cfd_cavity_b200 import _lib as L
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+
+
+def declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"^\s*(?:const\s+)?[\w\s\*]+?\b(cav\w*)\s*\(", text, flags=re.M))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(L.LIB_PATH)
+    syms = declared_symbols()
+    assert len(syms) >= 25, syms
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_default_params_are_the_reference_cli_defaults():
+    """src/cli.rs:94-130."""
+    lib = L.load()
+    p = L.CavParams()
+    assert lib.cav_default_params(ctypes.byref(p)) == 0
+    assert (p.nx, p.ny) == (64, 256)
+    assert (p.ra, p.pr, p.cs, p.pr_t, p.utarget, p.seed) == (1e6, 0.71, 0.10, 0.9, 0.02, 42)
+    assert (p.alpha_mult, p.nu_start_mult, p.has_nu_override) == (1.0, 1.0, 0)
+    assert p.noise_amp == 1e-3 and p.init_mode == L.CAV_INIT_LINEAR and p.geq_order == 2
+
+
+def _create(**kw):
+    lib = L.load()
+    p = L.CavParams()
+    lib.cav_default_params(ctypes.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    h = ctypes.c_void_p()
+    rc = lib.cav_create(ctypes.byref(p), ctypes.byref(h))
+    if rc == 0:
+        lib.cav_destroy(h)
+    return rc, lib.cav_last_error(None).decode()
+
+
+@pytest.mark.parametrize("kw,code", [
+    (dict(nx=2), L.CAV_ERR_ARG),
+    (dict(ny=3), L.CAV_ERR_ARG),
+    (dict(precision=9), L.CAV_ERR_ARG),
+    (dict(geq_order=3), L.CAV_ERR_ARG),
+    (dict(init_mode=5), L.CAV_ERR_ARG),
+    (dict(has_nu_override=1, nu_override=-1.0), L.CAV_ERR_ARG),
+    (dict(has_nu_override=1, nu_override=1e-5), L.CAV_ERR_TAU),
+    (dict(alpha_mult=1e-3), L.CAV_ERR_TAU),
+])
+def test_create_rejects_bad_arguments_before_cuda(kw, code):
+    """The reference asserts (src/uniform/solver.rs:130-132, 152-154); the ABI
+    returns a status and a message instead."""
+    rc, msg = _create(**kw)
+    assert rc == code, (rc, msg)
+    assert msg
+
+
+def test_null_handle_is_an_error():
+    lib = L.load()
+    assert lib.cav_step(None, 1) == L.CAV_ERR_ARG
+    assert lib.cav_destroy(None) == L.CAV_ERR_ARG
+
+
+def test_product_sources_never_reach_the_oracle():
+    pkg = os.path.join(ROOT, "cfd_cavity_b200")
+    for path in glob.glob(os.path.join(pkg, "**", "*"), recursive=True):
+        if not path.endswith((".py", ".cu", ".cuh", ".h", ".cpp")):
+            continue
+        text = open(path).read()
+        assert not re.search(r"^\s*(from|import)\s+oracle\b", text, flags=re.M), path
+        assert "cavity_oracle" not in text, path
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    with pytest.raises(RuntimeError):
+        L._lib_saved = L._lib
+        try:
+            L._lib = None
+            L.load(str(tmp_path / "nope.so"))
+        finally:
+            L._lib = L._lib_saved

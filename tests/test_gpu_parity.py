@@ -1,0 +1,313 @@
+"""Parity of the CUDA path with the FP64 oracle, through the C ABI.
+
+Tolerances (stated here, used below):
+  * index maps (streaming, bounce-back, thermal BC) with the collision
+    replaced by the identity: bit-exact in every storage format;
+  * FP64 storage: relative L-inf <= 1e-12 on f, g, rho, u, T after 1000 steps
+    (the FP64 kernels are built without fused multiply-add and follow the
+    reference's expression order, so the observed difference is 0);
+  * FP32 storage: |drho| <= 1e-6, |dT| <= 2e-5, |du| <= 1e-3 * max|u| after
+    1000 steps; 16-bit storage: |dT| <= 3e-3, |du| <= 0.05 * max|u| + 1e-6;
+  * time-averaged Nusselt: within 0.5 % of the oracle (golden fixtures).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from cfd_cavity_b200 import CavitySolver, TimeAverager
+from cfd_cavity_b200 import _lib as L
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def pair(nx, ny, ra, *, precision="f64", cs=0.1, init_mode=0, noise=1e-3, nu=None, seed=42,
+         t_hot=None, utarget=0.02):
+    kw = dict(init_mode=init_mode, noise_amp=noise, t_hot_profile=t_hot)
+    o = oracle.OracleSolver(nx, ny, ra, 0.71, cs, 0.9, utarget, seed, 4, 1.0, 1.0, nu, **kw)
+    g = CavitySolver(nx, ny, ra, 0.71, cs, 0.9, utarget, seed, 1, 1.0, 1.0, nu, precision=precision, **kw)
+    return o, g
+
+
+def rel_linf(a, b):
+    scale = max(np.max(np.abs(b)), 1e-300)
+    return float(np.max(np.abs(a - b)) / scale)
+
+
+def assert_same_state(o, g, tol=0.0):
+    fo, fg = o.fields(), g.fields()
+    for k in ("rho", "ux", "uy", "temperature", "fy_node"):
+        assert rel_linf(fg[k], fo[k]) <= tol, (k, rel_linf(fg[k], fo[k]))
+    po, pg = o.populations(), g.populations()
+    for a, b, n in ((pg[0], po[0], "f"), (pg[1], po[1], "g")):
+        assert rel_linf(a, b) <= tol, (n, rel_linf(a, b))
+
+
+# ---------------------------------------------------------------------------
+# Index maps with the collision disabled.
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("precision", ["f64", "f32", "f16", "bf16"])
+@pytest.mark.parametrize("shape", [(16, 40), (37, 23), (5, 4)])
+def test_stream_bounce_back_bc_index_maps_bitexact(precision, shape):
+    """The fused kernel's pull/bounce-back/thermal-BC maps against the
+    reference's stream() + apply_thermal_boundary_conditions(), bit for bit.
+    Random populations are first rounded through the storage format (read
+    back from the device), so every later value is a moved copy."""
+    nx, ny = shape
+    o, g = pair(nx, ny, 1e5, precision=precision)
+    rng = np.random.default_rng(nx * 1000 + ny)
+    n = nx * ny
+    f = 0.11 + 0.01 * rng.standard_normal((n, 9))
+    gg = 0.05 * rng.standard_normal((n, 9))
+    g.set_populations(f, gg)
+    f, gg = g.populations()  # storage-rounded values
+    # wall g values are computed (geq of the wall temperature): use wall
+    # temperatures that are exact in every format.
+    o.set_populations(f, gg)
+    passes = 6
+    g._ck(L.load().cav_debug_phase(g._h, L.CAV_PHASE_FUSED_IDENTITY, passes - 1))
+    for _ in range(passes):
+        o.stream()
+        o.apply_thermal_boundary_conditions()
+    pf, pg_ = g.populations()
+    of, og = o.populations()
+    assert np.array_equal(pf, of)
+    # interior g values are moved copies; wall g = geq(T_wall) is computed in
+    # the storage's arithmetic (exact for FP64).
+    wall = np.zeros((ny, nx), bool)
+    wall[:, 0] = wall[:, -1] = True
+    wall = wall.reshape(-1)
+    assert np.array_equal(pg_[~wall], og[~wall])
+    if precision == "f64":
+        assert np.array_equal(pg_, og)
+    else:
+        assert np.max(np.abs(pg_[wall] - og[wall])) < 3e-3 * 0.5
+
+
+def test_debug_phases_bitexact_fp64():
+    """Each pub(crate) phase (src/uniform/tests.rs:154-169) against the oracle."""
+    o, g = pair(16, 40, 1e5)
+    steps = [("collide", (100,)), ("stream", ()), ("apply_bounce_back", ()),
+             ("apply_thermal_boundary_conditions", ()), ("update_macroscopic", ()),
+             ("enforce_wall_velocity", ()), ("collide", (3,)), ("stream", ()),
+             ("apply_thermal_boundary_conditions", ()), ("update_macroscopic", ())]
+    for name, args in steps:
+        getattr(o, name)(*args)
+        getattr(g, name)(*args)
+        assert_same_state(o, g, 0.0)
+
+
+# ---------------------------------------------------------------------------
+# Full steps.
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("cfg", [
+    dict(nx=16, ny=40, ra=1e5, init_mode=0, noise=1e-3, steps=1000),
+    dict(nx=64, ny=256, ra=1e6, init_mode=1, noise=1e-4, steps=1000),
+    dict(nx=37, ny=61, ra=1e7, init_mode=0, noise=1e-3, steps=700),
+])
+def test_fp64_fields_after_1000_steps(cfg):
+    """FP64 fields and populations vs the oracle after 1000 steps; the
+    tolerance is 1e-12 relative L-inf and the FP64 path is expected to be
+    bit-identical."""
+    o, g = pair(cfg["nx"], cfg["ny"], cfg["ra"], init_mode=cfg["init_mode"], noise=cfg["noise"])
+    o.step(cfg["steps"])
+    g.step(cfg["steps"])
+    assert_same_state(o, g, 1e-12)
+    fo, fg = o.fields(), g.fields()
+    assert np.array_equal(fo["temperature"], fg["temperature"])
+    assert np.array_equal(fo["nu_t"], fg["nu_t"])
+
+
+def test_fp64_chunked_and_graph_steps_are_identical():
+    """step(n) in one call (CUDA-graph replays after the spin-up) equals n
+    single steps, bit for bit."""
+    a = CavitySolver(24, 40, 1e6, 0.71, 0.1, 0.9, 0.02, 5, precision="f64")
+    b = CavitySolver(24, 40, 1e6, 0.71, 0.1, 0.9, 0.02, 5, precision="f64")
+    a.step(460)
+    for _ in range(460):
+        b.step(1)
+    fa, fb = a.fields(), b.fields()
+    for k in fa:
+        assert np.array_equal(fa[k], fb[k]), k
+    assert a.info()["time_step"] == 460
+
+
+def test_hot_wall_profile_and_corners_fp64():
+    """A per-row hot-wall temperature replaces T_HOT (solver.rs:957-963); the
+    corners take the row-1 / row-(ny-2) wall value (vertical loop first)."""
+    ny = 40
+    rng = np.random.default_rng(11)
+    th = 0.5 + 0.01 * (2 * rng.random(ny) - 1)
+    o, g = pair(16, ny, 1e6, t_hot=th)
+    o.step(300)
+    g.step(300)
+    assert_same_state(o, g, 0.0)
+
+
+def test_init_from_fields_fp64():
+    """init_from_fields (solver.rs:232-262): equilibria of given fields,
+    wall velocity zeroed, time_step reset."""
+    o, g = pair(20, 30, 1e6)
+    rng = np.random.default_rng(5)
+    n = 20 * 30
+    rho = 1 + 1e-3 * rng.standard_normal(n)
+    ux = 1e-2 * rng.standard_normal(n)
+    uy = 1e-2 * rng.standard_normal(n)
+    t = 0.3 * rng.standard_normal(n)
+    o.step(10)
+    g.step(10)
+    o.init_from_fields(rho, ux, uy, t)
+    g.init_from_fields(rho, ux, uy, t)
+    assert g.info()["time_step"] == 0
+    assert_same_state(o, g, 0.0)
+    o.step(250)
+    g.step(250)
+    assert_same_state(o, g, 0.0)
+
+
+def test_diagnostics_match_oracle_fp64():
+    o, g = pair(64, 256, 1e6, init_mode=1, noise=1e-4)
+    o.step(1500)
+    g.step(1500)
+    do, dg = o.diag(), g.diag()
+    for k in ("nusselt_hot", "nusselt_cold", "nusselt_hot_wall_link", "total_mass",
+              "total_f_mass", "max_u", "max_uy", "nu_t_max", "y_plus_hot", "nusselt_volume"):
+        assert abs(dg[k] - do[k]) <= 1e-12 * max(abs(do[k]), 1e-30), (k, dg[k], do[k])
+    assert dg["finite"] == 1 and do["finite"] == 1.0
+
+
+def test_time_averager_and_nusselt_of_mean_fp64():
+    """TimeAverager (post.rs:11-57) + nusselt_from_mean (main.rs:740-753)."""
+    o, g = pair(32, 64, 1e6)
+    ao = oracle.OracleAverager(32 * 64)
+    ag = TimeAverager(g)
+    for _ in range(6):
+        o.step(37)
+        g.step(37)
+        ao.accumulate(o)
+        ag.accumulate()
+    no, mo = ao.means()
+    ng, mg = ag.means()
+    assert no == ng == 6
+    for a, b in zip(mg, mo):
+        assert rel_linf(a, b) <= 1e-13
+    assert abs(ag.nusselt_from_mean(True) - o.nusselt_from_mean(mo[2], True)) < 1e-12
+    assert abs(ag.nusselt_from_mean(False) - o.nusselt_from_mean(mo[2], False)) < 1e-12
+
+
+def test_per_step_nusselt_accumulation_fp64():
+    """Per-step Nu accumulation on the device equals the mean of the oracle's
+    instantaneous nusselt_hot/cold over the same states."""
+    o, g = pair(32, 64, 1e6)
+    o.step(150)
+    g.step(150)
+    g.nu_accumulate(True)
+    sh = sc = 0.0
+    for chunk in (1, 5, 130, 64):
+        g.step(chunk)
+        for _ in range(chunk):
+            o.step(1)
+            h, c = o.nusselt()
+            sh += h
+            sc += c
+    hot, cold, n = g.nu_accumulated()
+    assert n == 200
+    assert abs(hot - sh / n) < 1e-11 * abs(sh / n)
+    assert abs(cold - sc / n) < 1e-11 * abs(sc / n)
+
+
+@pytest.mark.parametrize("precision,tol", [
+    ("f32", dict(rho=1e-6, t=2e-5, u=1e-3)),
+    ("f16", dict(rho=2e-4, t=3e-3, u=5e-2)),
+    ("bf16", dict(rho=2e-3, t=3e-2, u=2e-1)),
+])
+def test_reduced_precision_fields_after_1000_steps(precision, tol):
+    o, g = pair(64, 256, 1e6, precision=precision, init_mode=1, noise=1e-4)
+    o.step(1000)
+    g.step(1000)
+    fo, fg = o.fields(), g.fields()
+    umax = max(np.max(np.abs(fo["ux"])), np.max(np.abs(fo["uy"])))
+    assert np.max(np.abs(fg["rho"] - fo["rho"])) <= tol["rho"]
+    assert np.max(np.abs(fg["temperature"] - fo["temperature"])) <= tol["t"]
+    assert np.max(np.abs(fg["ux"] - fo["ux"])) <= tol["u"] * umax + 1e-9
+    assert np.max(np.abs(fg["uy"] - fo["uy"])) <= tol["u"] * umax + 1e-9
+
+
+def _golden(name):
+    with open(os.path.join(GOLDEN, name)) as fh:
+        return json.load(fh)
+
+
+def _run_golden(gd, precision):
+    c = gd["config"]
+    g = CavitySolver(c["nx"], c["ny"], c["ra"], c["pr"], c["cs"], c["pr_t"], c["utarget"], c["seed"],
+                     precision=precision, init_mode=1, noise_amp=c["noise_amp"])
+    start = c["steps"] - c["window"]
+    g.step(start)
+    g.nu_accumulate(True)
+    avg = TimeAverager(g)
+    # sample every 100 steps from the first state of the window (main.rs:279-281)
+    done = 0
+    while done < c["window"]:
+        g.step(1)
+        avg.accumulate()
+        chunk = min(c["sample_every"] - 1, c["window"] - done - 1)
+        if chunk > 0:
+            g.step(chunk)
+        done += 1 + max(chunk, 0)
+    hot, cold, n = g.nu_accumulated()
+    return g, hot, cold, n, avg
+
+
+def test_c1_golden_fp64():
+    """64x256 Ra=1e6 FP64, 20 000 steps vs the oracle fixture (bit-identical
+    fields expected; the mean Nu is reduced in a different order)."""
+    gd = _golden("c1_64x256_ra1e6.json")
+    g, hot, cold, n, avg = _run_golden(gd, "f64")
+    assert n == gd["config"]["window"]
+    assert abs(hot - gd["nu_hot_step_mean"]) < 1e-10 * gd["nu_hot_step_mean"]
+    assert abs(cold - gd["nu_cold_step_mean"]) < 1e-10 * gd["nu_cold_step_mean"]
+    assert abs(avg.nusselt_from_mean(True) - gd["nu_hot_of_mean_t"]) < 1e-10 * gd["nu_hot_of_mean_t"]
+    t = g.fields()["temperature"]
+    assert np.array_equal(t[::gd["fingerprint_stride"]], np.array(gd["t_fingerprint"]))
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32", "f16", "bf16"])
+def test_c1_nusselt_within_half_percent(precision):
+    gd = _golden("c1_64x256_ra1e6.json")
+    g, hot, cold, n, avg = _run_golden(gd, precision)
+    for got, ref in ((hot, gd["nu_hot_step_mean"]), (cold, gd["nu_cold_step_mean"]),
+                     (avg.nusselt_from_mean(True), gd["nu_hot_of_mean_t"])):
+        assert abs(got - ref) <= 5e-3 * abs(ref), (precision, got, ref)
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(GOLDEN, "c2_128x512_ra1e8.json")),
+                    reason="C2 fixture not generated")
+@pytest.mark.parametrize("precision", ["f64", "f32", "f16", "bf16"])
+def test_c2_time_averaged_nusselt_within_half_percent(precision):
+    """128x512 Ra=1e8, 200 000 steps, Nu averaged over steps 150 001-200 000:
+    each storage format within 0.5 % of the FP64 oracle."""
+    gd = _golden("c2_128x512_ra1e8.json")
+    g, hot, cold, n, avg = _run_golden(gd, precision)
+    assert n == gd["config"]["window"]
+    for got, ref in ((hot, gd["nu_hot_step_mean"]), (cold, gd["nu_cold_step_mean"]),
+                     (avg.nusselt_from_mean(True), gd["nu_hot_of_mean_t"])):
+        assert abs(got - ref) <= 5e-3 * abs(ref), (precision, got, ref)
+
+
+def test_guards_report_status_without_faulting():
+    """max_u and finiteness guards (main.rs:209-276) as status codes."""
+    g = CavitySolver(16, 40, 1e5, 0.71, 0.1, 0.9, 0.02, 42)
+    assert g.check_guards() == 0
+    n = 16 * 40
+    ux = np.zeros(n)
+    ux[100] = 0.5
+    g.set_fields(ux=ux)
+    assert g.check_guards() == L.CAV_ERR_MAXU
+    t = g.fields()["temperature"]
+    t[77] = np.nan
+    g.set_fields(ux=np.zeros(n), temperature=t)
+    assert g.check_guards() == L.CAV_ERR_DIVERGED
