@@ -41,7 +41,8 @@ sys.path.insert(0, ROOT)
 NX, NY, RA = 128, 512, 1e8
 PHYS = dict(pr=0.71, cs=0.10, pr_t=0.9, utarget=0.02, seed=42)
 CHUNK = 2000
-BYTES_PER_NODE = {"f64": 304, "f32": 152, "f16": 80, "bf16": 80}
+BYTES_PER_NODE = {"f64": 304, "f32": 152, "f16": 80, "bf16": 80, "f16g": 80, "f16sr": 80,
+                  "bf16sr": 80, "f16gsr": 80}
 PRECISION = "f16"
 L2_FLUSH_BYTES = 256 << 20
 

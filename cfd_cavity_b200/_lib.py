@@ -20,8 +20,11 @@ CAV_ERR_CUDA = 6
 CAV_ERR_STATE = 7
 CAV_ERR_NOMEM = 8
 
-CAV_PREC_F64, CAV_PREC_F32, CAV_PREC_F16, CAV_PREC_BF16 = 0, 1, 2, 3
-PRECISIONS = {"f64": CAV_PREC_F64, "f32": CAV_PREC_F32, "f16": CAV_PREC_F16, "bf16": CAV_PREC_BF16}
+(CAV_PREC_F64, CAV_PREC_F32, CAV_PREC_F16, CAV_PREC_BF16, CAV_PREC_F16G, CAV_PREC_F16SR,
+ CAV_PREC_BF16SR, CAV_PREC_F16GSR) = range(8)
+PRECISIONS = {"f64": CAV_PREC_F64, "f32": CAV_PREC_F32, "f16": CAV_PREC_F16, "bf16": CAV_PREC_BF16,
+              "f16g": CAV_PREC_F16G, "f16sr": CAV_PREC_F16SR, "bf16sr": CAV_PREC_BF16SR,
+              "f16gsr": CAV_PREC_F16GSR}
 CAV_INIT_LINEAR, CAV_INIT_ZERO = 0, 1
 (CAV_PHASE_COLLIDE, CAV_PHASE_STREAM, CAV_PHASE_BOUNCE_BACK, CAV_PHASE_THERMAL_BC,
  CAV_PHASE_MACRO, CAV_PHASE_NOSLIP, CAV_PHASE_FUSED_IDENTITY) = range(7)

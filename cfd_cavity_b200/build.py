@@ -27,6 +27,10 @@ UNITS = {
     "prec_f32.cu": [],
     "prec_f16.cu": [],
     "prec_bf16.cu": [],
+    "prec_f16g.cu": [],
+    "prec_f16sr.cu": [],
+    "prec_bf16sr.cu": [],
+    "prec_f16gsr.cu": [],
 }
 
 

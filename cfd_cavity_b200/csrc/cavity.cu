@@ -77,7 +77,7 @@ int cav_create(const cav_params* pp, cav_handle** out) {
     const cav_params& p = *pp;
     if (p.nx < 4 || p.ny < 4 || p.nx > 65536 || p.ny > 65536)
         return fail(nullptr, CAV_ERR_ARG, "nx and ny must be in [4, 65536]");
-    if (p.precision < CAV_PREC_F64 || p.precision > CAV_PREC_BF16)
+    if (p.precision < CAV_PREC_F64 || p.precision > CAV_PREC_F16GSR)
         return fail(nullptr, CAV_ERR_ARG, "unknown precision");
     if (p.geq_order != 1 && p.geq_order != 2) return fail(nullptr, CAV_ERR_ARG, "geq_order must be 1 or 2");
     if (p.init_mode != CAV_INIT_LINEAR && p.init_mode != CAV_INIT_ZERO)
@@ -282,13 +282,21 @@ Solver* make_solver_f64();
 Solver* make_solver_f32();
 Solver* make_solver_f16();
 Solver* make_solver_bf16();
+Solver* make_solver_f16g();
+Solver* make_solver_f16sr();
+Solver* make_solver_bf16sr();
+Solver* make_solver_f16gsr();
 
 Solver* make_solver(int precision) {
     switch (precision) {
         case CAV_PREC_F64: return make_solver_f64();
         case CAV_PREC_F32: return make_solver_f32();
         case CAV_PREC_F16: return make_solver_f16();
-        default: return make_solver_bf16();
+        case CAV_PREC_BF16: return make_solver_bf16();
+        case CAV_PREC_F16G: return make_solver_f16g();
+        case CAV_PREC_F16SR: return make_solver_f16sr();
+        case CAV_PREC_BF16SR: return make_solver_bf16sr();
+        default: return make_solver_f16gsr();
     }
 }
 }  // namespace cav

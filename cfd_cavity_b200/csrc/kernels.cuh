@@ -19,13 +19,37 @@ namespace cav {
 template <class St>
 __device__ __forceinline__ typename Fmt<St>::A ldp(const St* __restrict__ buf, const Geom& G, int q, int iy,
                                                   int ix) {
-    return Fmt<St>::load(buf[(long long)q * G.plane + (long long)iy * G.pitch + ix]);
+    return Fmt<St>::load(buf[(long long)q * G.plane + (long long)iy * G.pitch + ix], q);
 }
 template <class St>
 __device__ __forceinline__ void stp(St* __restrict__ buf, const Geom& G, int q, int iy, int ix,
-                                    typename Fmt<St>::A v) {
-    buf[(long long)q * G.plane + (long long)iy * G.pitch + ix] = Fmt<St>::store(v);
+                                    typename Fmt<St>::A v, uint32_t r = RN_BITS) {
+    buf[(long long)q * G.plane + (long long)iy * G.pitch + ix] = Fmt<St>::store(v, q, r);
 }
+
+// Stores the 18 populations of one node; the stochastically rounded formats
+// draw their random bits from the (seed, step, node) stream.
+template <class St>
+__device__ __forceinline__ void store_node(St* __restrict__ dst, const Geom& G, int iy, int ix,
+                                           const typename Fmt<St>::A (&f)[Q], const typename Fmt<St>::A (&g)[Q],
+                                           const StepScalars<typename Fmt<St>::A>& c) {
+    if constexpr (Fmt<St>::SR) {
+        const long long step = c.step_dev ? *c.step_dev + c.step : c.step;
+        NodeRng rng(c.sr_seed, step, (long long)iy * G.nx + ix);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) stp(dst, G, i, iy, ix, f[i], rng.next());
+#pragma unroll
+        for (int i = 0; i < Q; ++i) stp(dst, G, Q + i, iy, ix, g[i], rng.next());
+    } else {
+#pragma unroll
+        for (int i = 0; i < Q; ++i) stp(dst, G, i, iy, ix, f[i]);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) stp(dst, G, Q + i, iy, ix, g[i]);
+    }
+}
+
+static __global__ void k_set_step(long long* p, long long v) { *p = v; }
+static __global__ void k_add_step(long long* p, long long d) { *p += d; }
 
 // Pull-stream of one node from a PC buffer (stream, solver.rs:838-913) fused
 // with the thermal boundary conditions (solver.rs:951-988):
@@ -129,10 +153,7 @@ __global__ void __launch_bounds__(256) k_fused(const St* __restrict__ src, St* _
         fy[k] = fyv;
         if (WRITE_NUT) nut[k] = nutv;
     }
-#pragma unroll
-    for (int i = 0; i < Q; ++i) stp(dst, G, i, iy, ix, f[i]);
-#pragma unroll
-    for (int i = 0; i < Q; ++i) stp(dst, G, Q + i, iy, ix, g[i]);
+    store_node<St>(dst, G, iy, ix, f, g, c);
 }
 
 // collide(step) on a REF state (populations + fields), writing PC to dst.
@@ -169,10 +190,7 @@ __global__ void __launch_bounds__(256) k_collide_ref(const St* __restrict__ src,
     collide_node<A, SH>(f, g, m, c, fyv, nutv);
     fy[k] = fyv;
     nut[k] = nutv;
-#pragma unroll
-    for (int i = 0; i < Q; ++i) stp(dst, G, i, iy, ix, f[i]);
-#pragma unroll
-    for (int i = 0; i < Q; ++i) stp(dst, G, Q + i, iy, ix, g[i]);
+    store_node<St>(dst, G, iy, ix, f, g, c);
 }
 
 // PC(src) -> REF(dst): stream + thermal BC + macroscopic + no-slip, without
@@ -259,11 +277,7 @@ __global__ void k_dbg_collide(St* __restrict__ pop, const typename Fmt<St>::A* _
     collide_node<A, SH>(f, g, m, c, fyv, nutv);
     fy[k] = fyv;
     nut[k] = nutv;
-#pragma unroll
-    for (int i = 0; i < Q; ++i) {
-        stp(pop, G, i, iy, ix, f[i]);
-        stp(pop, G, Q + i, iy, ix, g[i]);
-    }
+    store_node<St>(pop, G, iy, ix, f, g, c);
 }
 
 // stream(), src/uniform/solver.rs:838-913: pull, bounce-back for f, g kept

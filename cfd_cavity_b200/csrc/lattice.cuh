@@ -6,16 +6,21 @@
 // ny rows x pitch columns.  Four storage formats:
 //   double         FP64 arithmetic, unshifted (the parity variant);
 //   float          FP32 arithmetic, f stored as f_i - w_i;
-//   __half         FP32 arithmetic, f_i - w_i and g_i scaled by 2^15 into
+//   Half16         FP32 arithmetic, f_i - w_i and g_i scaled by 2^15 into
 //                  IEEE binary16 (Lehmann et al. 2022, "FP16S" storage);
-//   __nv_bfloat16  FP32 arithmetic, f_i - w_i and g_i in bfloat16.
+//   Bf16           FP32 arithmetic, f_i - w_i and g_i in bfloat16;
+//   Mix16          FP32 arithmetic, f_i - w_i in binary16 and g_i in 16-bit
+//                  fixed point;
+//   *SR            the same 16-bit encodings with stochastic rounding.
 // g is shifted by w_i * T0 with T0 = 0, i.e. stored as is: theta is centred
 // on zero in this problem (walls at +-0.5).
 #pragma once
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <math.h>
 #include <stdint.h>
+#include <string.h>
 
 namespace cav {
 
@@ -37,44 +42,155 @@ constexpr double CS2 = 1.0 / 3.0;
 constexpr double LAMBDA_TRT = 3.0 / 16.0;
 
 // ---------------------------------------------------------------------------
-// Storage formats.
+// Storage formats.  load(v, q) / store(x, q, r) take the plane index q
+// (0..8 f, 9..17 g) so that a format may encode f and g differently; every
+// plane keeps one encoding, so raw copies between planes of one population
+// set stay exact.  r carries 32 random bits for the stochastically rounded
+// formats (ignored by the others); r = RN_BITS asks for round-to-nearest.
+// Every load -> store round trip is exact, so moved (streamed) values are
+// never re-rounded.
 // ---------------------------------------------------------------------------
+constexpr uint32_t RN_BITS = 0x80000000u;
+
 template <class St>
 struct Fmt;
 
 template <>
 struct Fmt<double> {
     using A = double;
-    static constexpr bool SHIFT = false;
-    static constexpr int PREC = 0;
-    __host__ __device__ static A load(double v) { return v; }
-    __host__ __device__ static double store(A v) { return v; }
+    static constexpr bool SHIFT = false, SR = false;
+    __host__ __device__ static A load(double v, int) { return v; }
+    __host__ __device__ static double store(A v, int, uint32_t) { return v; }
 };
 template <>
 struct Fmt<float> {
     using A = float;
-    static constexpr bool SHIFT = true;
-    static constexpr int PREC = 1;
-    __host__ __device__ static A load(float v) { return v; }
-    __host__ __device__ static float store(A v) { return v; }
+    static constexpr bool SHIFT = true, SR = false;
+    __host__ __device__ static A load(float v, int) { return v; }
+    __host__ __device__ static float store(A v, int, uint32_t) { return v; }
 };
-template <>
-struct Fmt<__half> {
-    using A = float;
-    static constexpr bool SHIFT = true;
-    static constexpr int PREC = 2;
-    static constexpr float SCALE = 32768.0f;
-    static constexpr float INV_SCALE = 1.0f / 32768.0f;
-    __host__ __device__ static A load(__half v) { return __half2float(v) * INV_SCALE; }
-    __host__ __device__ static __half store(A v) { return __float2half_rn(v * SCALE); }
+
+// binary16 of x * 2^15 (the 2^15 keeps |f - w| >= 2e-9 out of the subnormals).
+constexpr float H_SCALE = 32768.0f, H_INV = 1.0f / 32768.0f;
+
+__host__ __device__ __forceinline__ float h16_load(unsigned short bits) {
+    __half_raw r;
+    r.x = bits;
+    return __half2float(__half(r)) * H_INV;
+}
+// Round to nearest (ties to even), or stochastically: add 13 random bits
+// below binary16's last mantissa bit to the binary32 magnitude, then
+// truncate (Croci et al., "Stochastic rounding: implementation, error
+// analysis and applications", R. Soc. open sci. 2022).  Unbiased:
+// E[round(x)] = x.
+__host__ __device__ __forceinline__ unsigned short h16_store(float x, bool sr, uint32_t r) {
+    float s = x * H_SCALE;
+    __half h;
+    if (sr) {
+        uint32_t u;
+        memcpy(&u, &s, 4);
+        if ((u & 0x7f800000u) != 0x7f800000u) u += (r >> 19);
+        memcpy(&s, &u, 4);
+        h = __float2half_rz(s);
+    } else {
+        h = __float2half_rn(s);
+    }
+    return __half_raw(h).x;
+}
+
+__host__ __device__ __forceinline__ float bf16_load(unsigned short bits) {
+    uint32_t u = uint32_t(bits) << 16;
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+}
+__host__ __device__ __forceinline__ unsigned short bf16_store(float x, bool sr, uint32_t r) {
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    if ((u & 0x7f800000u) == 0x7f800000u) return (unsigned short)(u >> 16);  // inf / nan
+    if (sr) return (unsigned short)((u + (r >> 16)) >> 16);
+    return (unsigned short)((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);        // nearest, ties to even
+}
+
+// 16-bit fixed point of g_i with a power-of-two scale per direction class:
+// 2^16 on the rest population (|g_0| <= 4/9 |T| < 0.5), 2^17 on the axes
+// (|g| <= 1/9 |T| (1 + 3|u| + ...) < 0.25), 2^19 on the diagonals
+// (< 0.0625), for |T| <= 0.51 and |u| <= 0.1 (the driver's max_u guard).
+// Saturates instead of wrapping.  Absolute error: 1.5e-5, 7.6e-6, 1.9e-6.
+__host__ __device__ constexpr int fx_shift(int q) {
+    return q == 9 ? 16 : (q == 10 || q == 11 || q == 14 || q == 15 ? 17 : 19);
+}
+__host__ __device__ __forceinline__ float fx_load(unsigned short bits, int q) {
+    return float(short(bits)) * ldexpf(1.0f, -fx_shift(q));
+}
+__host__ __device__ __forceinline__ unsigned short fx_store(float x, int q, bool sr, uint32_t r) {
+    float s = x * ldexpf(1.0f, fx_shift(q));
+    s = fminf(fmaxf(s, -32767.0f), 32767.0f);
+    float fl = floorf(s);
+    float frac = s - fl;
+    int iv;
+    if (sr) {
+        iv = int(fl) + ((float(r >> 8) * (1.0f / 16777216.0f)) < frac ? 1 : 0);
+    } else {
+        iv = int(fl) + (frac > 0.5f || (frac == 0.5f && (int(fl) & 1)) ? 1 : 0);
+    }
+    if (iv > 32767) iv = 32767;
+    return (unsigned short)(short)iv;
+}
+
+// Tag types of the 16-bit formats (one distinct type per encoding).
+template <int KIND, bool SRND>
+struct P16 {
+    unsigned short bits;
 };
-template <>
-struct Fmt<__nv_bfloat16> {
+constexpr int K_HALF = 0, K_BF16 = 1, K_MIX = 2;  // MIX: binary16 f - w, fixed-point g
+
+template <int KIND, bool SRND>
+struct Fmt<P16<KIND, SRND>> {
     using A = float;
-    static constexpr bool SHIFT = true;
-    static constexpr int PREC = 3;
-    __host__ __device__ static A load(__nv_bfloat16 v) { return __bfloat162float(v); }
-    __host__ __device__ static __nv_bfloat16 store(A v) { return __float2bfloat16_rn(v); }
+    using St = P16<KIND, SRND>;
+    static constexpr bool SHIFT = true, SR = SRND;
+    __host__ __device__ static A load(St v, int q) {
+        if (KIND == K_BF16) return bf16_load(v.bits);
+        if (KIND == K_MIX && q >= 9) return fx_load(v.bits, q);
+        return h16_load(v.bits);
+    }
+    __host__ __device__ static St store(A x, int q, uint32_t r) {
+        const bool sr = SRND && r != RN_BITS;
+        St o;
+        if (KIND == K_BF16) o.bits = bf16_store(x, sr, r);
+        else if (KIND == K_MIX && q >= 9) o.bits = fx_store(x, q, sr, r);
+        else o.bits = h16_store(x, sr, r);
+        return o;
+    }
+};
+using Half16 = P16<K_HALF, false>;
+using Half16SR = P16<K_HALF, true>;
+using Bf16 = P16<K_BF16, false>;
+using Bf16SR = P16<K_BF16, true>;
+using Mix16 = P16<K_MIX, false>;
+using Mix16SR = P16<K_MIX, true>;
+
+// Per-node stream of random words for the stochastic rounding: a MurmurHash3
+// finaliser of (seed, step, node) seeds a 32-bit LCG (Numerical Recipes
+// constants); the rounding uses the high bits.  Depends only on
+// (seed, step, node), so every run, graph replay or not, is reproducible.
+__host__ __device__ __forceinline__ uint32_t mix32(uint32_t h) {
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+struct NodeRng {
+    uint32_t s;
+    __host__ __device__ NodeRng(uint32_t seed, long long step, long long node)
+        : s(mix32(uint32_t(node) * 0x9E3779B1u + mix32(uint32_t(step) ^ seed))) {}
+    __host__ __device__ uint32_t next() {
+        s = s * 1664525u + 1013904223u;
+        return s;
+    }
 };
 
 // Grid geometry of one cavity.
@@ -97,6 +213,9 @@ struct StepScalars {
     A t_cold;  // cold-wall theta
     int geq_order;
     const A* t_hot;  // [ny] hot-wall theta
+    uint32_t sr_seed;  // seed of the stochastic rounding
+    long long step;    // step index of this collision (used by the rounding)
+    const long long* step_dev;  // if set, the step is *step_dev + step (graph replays)
 };
 
 // ---------------------------------------------------------------------------

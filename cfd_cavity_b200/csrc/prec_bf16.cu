@@ -1,6 +1,6 @@
-// prec_bf16.cu -- instantiates the cavity solver for __nv_bfloat16 population storage.
+// prec_bf16.cu -- instantiates the cavity solver for bfloat16 f - w and g storage.
 #include "solver.cuh"
 
 namespace cav {
-Solver* make_solver_bf16() { return new Impl<__nv_bfloat16>; }
+Solver* make_solver_bf16() { return new Impl<Bf16>; }
 }  // namespace cav

@@ -1,0 +1,6 @@
+// prec_bf16sr.cu -- instantiates the cavity solver for bfloat16 f - w and g, stochastically rounded storage.
+#include "solver.cuh"
+
+namespace cav {
+Solver* make_solver_bf16sr() { return new Impl<Bf16SR>; }
+}  // namespace cav

@@ -1,6 +1,6 @@
-// prec_f16.cu -- instantiates the cavity solver for __half population storage.
+// prec_f16.cu -- instantiates the cavity solver for binary16 f - w and g storage.
 #include "solver.cuh"
 
 namespace cav {
-Solver* make_solver_f16() { return new Impl<__half>; }
+Solver* make_solver_f16() { return new Impl<Half16>; }
 }  // namespace cav

@@ -1,0 +1,6 @@
+// prec_f16g.cu -- instantiates the cavity solver for binary16 f - w, fixed-point g storage.
+#include "solver.cuh"
+
+namespace cav {
+Solver* make_solver_f16g() { return new Impl<Mix16>; }
+}  // namespace cav

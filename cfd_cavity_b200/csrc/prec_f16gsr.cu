@@ -1,0 +1,6 @@
+// prec_f16gsr.cu -- instantiates the cavity solver for binary16 f - w and fixed-point g, stochastically rounded storage.
+#include "solver.cuh"
+
+namespace cav {
+Solver* make_solver_f16gsr() { return new Impl<Mix16SR>; }
+}  // namespace cav

@@ -1,0 +1,6 @@
+// prec_f16sr.cu -- instantiates the cavity solver for binary16 f - w and g, stochastically rounded storage.
+#include "solver.cuh"
+
+namespace cav {
+Solver* make_solver_f16sr() { return new Impl<Half16SR>; }
+}  // namespace cav

@@ -145,6 +145,8 @@ struct Impl final : Solver {
     double *partials = nullptr, *diag_out = nullptr;
     double* sums = nullptr;
     double* aos = nullptr;
+    long long* step_dev = nullptr;   // step counter read by graph-replayed kernels
+    long long step_dev_val = -1;     // host mirror of *step_dev
     int64_t n_samples = 0, n_acc = 0;
     bool acc_on = false;
     int cur = 0;
@@ -158,7 +160,7 @@ struct Impl final : Solver {
             for (auto& gx : row)
                 if (gx) cudaGraphExecDestroy(gx);
         void* bufs[] = {pop[0], pop[1], rho, ux, uy, tt, fy, nut, t_hot_d, acc_hot, acc_cold,
-                        partials, diag_out, sums, aos};
+                        partials, diag_out, sums, aos, step_dev};
         for (void* b : bufs)
             if (b) cudaFree(b);
         if (stream) cudaStreamDestroy(stream);
@@ -193,6 +195,7 @@ struct Impl final : Solver {
         CK(cudaMemsetAsync(acc_cold, 0, sizeof(double) * p.ny, stream));
         CK(cudaMalloc(&partials, sizeof(double) * DIAG_NPART * DIAG_BLOCKS_MAX));
         CK(cudaMalloc(&diag_out, sizeof(double) * 16));
+        CK(cudaMalloc(&step_dev, sizeof(long long)));
         CK(cudaStreamSynchronize(stream));
     }
 
@@ -218,6 +221,9 @@ struct Impl final : Solver {
         c.t_cold = A(p.t_cold);
         c.geq_order = p.geq_order;
         c.t_hot = t_hot_d;
+        c.sr_seed = uint32_t(p.seed) ^ uint32_t(p.seed >> 32) ^ 0x5bd1e995u;
+        c.step = s;
+        c.step_dev = nullptr;
         return c;
     }
 
@@ -230,15 +236,15 @@ struct Impl final : Solver {
     void upload_ref(const std::vector<double>& f, const std::vector<double>& g, const std::vector<double>& r,
                     const std::vector<double>& u, const std::vector<double>& v, const std::vector<double>& t) {
         const int nx = p.nx, ny = p.ny;
-        std::vector<St> hp(NPLANES * field_elems(), Fmt<St>::store(A(0)));
+        std::vector<St> hp(NPLANES * field_elems(), Fmt<St>::store(A(0), 0, RN_BITS));
         for (int iy = 0; iy < ny; ++iy)
             for (int ix = 0; ix < nx; ++ix) {
                 const size_t k = size_t(iy) * nx + ix, d = size_t(iy) * pitch + ix;
                 for (int i = 0; i < Q; ++i) {
                     double fv = f[k * Q + i];
                     if (SH) fv -= WD(i);
-                    hp[size_t(i) * field_elems() + d] = Fmt<St>::store(A(fv));
-                    hp[size_t(Q + i) * field_elems() + d] = Fmt<St>::store(A(g[k * Q + i]));
+                    hp[size_t(i) * field_elems() + d] = Fmt<St>::store(A(fv), i, RN_BITS);
+                    hp[size_t(Q + i) * field_elems() + d] = Fmt<St>::store(A(g[k * Q + i]), Q + i, RN_BITS);
                 }
             }
         cur = 0;
@@ -322,8 +328,12 @@ struct Impl final : Solver {
     }
 
     // ---- the step loop -----------------------------------------------------------
-    void launch_fused(int64_t s, bool write_nut, bool acc) {
+    void launch_fused(int64_t s, bool write_nut, bool acc, const long long* sdev = nullptr, int64_t off = 0) {
         StepScalars<A> c = scalars(s);
+        if (sdev) {
+            c.step_dev = sdev;
+            c.step = off;
+        }
         if (write_nut) {
             if (acc)
                 k_fused<St, true, true, false><<<grd, blk, 0, stream>>>(pop[cur], pop[cur ^ 1], fy, nut, acc_hot,
@@ -350,7 +360,8 @@ struct Impl final : Solver {
         const int cur0 = cur;
         const int64_t launches0 = launches;
         CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        for (int j = 0; j < GRAPH_STEPS; ++j) launch_fused(spin_up, false, acc);
+        for (int j = 0; j < GRAPH_STEPS; ++j) launch_fused(spin_up, false, acc, step_dev, j);
+        k_add_step<<<1, 1, 0, stream>>>(step_dev, GRAPH_STEPS);
         cudaGraph_t gr;
         CK(cudaStreamEndCapture(stream, &gr));
         cur = cur0;
@@ -373,8 +384,15 @@ struct Impl final : Solver {
                 cur ^= 1;
                 pc_form = true;
             } else if (!first && time_step >= spin_up && n > GRAPH_STEPS) {
-                CK(cudaGraphLaunch(get_graph(acc_on), stream));
-                launches += GRAPH_STEPS;
+                cudaGraphExec_t gx = get_graph(acc_on);
+                if (step_dev_val != time_step) {
+                    k_set_step<<<1, 1, 0, stream>>>(step_dev, time_step);
+                    check_launch();
+                    step_dev_val = time_step;
+                }
+                CK(cudaGraphLaunch(gx, stream));
+                step_dev_val += GRAPH_STEPS;
+                launches += GRAPH_STEPS + 1;
                 time_step += GRAPH_STEPS;
                 n -= GRAPH_STEPS;
                 ref_cached = false;

@@ -43,11 +43,18 @@ extern "C" {
 
 /* ---- enumerations -------------------------------------------------------- */
 /* Storage precision of the populations (arithmetic: FP64 for CAV_PREC_F64,
- * FP32 otherwise; the 16-bit formats store f_i - w_i). */
-#define CAV_PREC_F64 0
-#define CAV_PREC_F32 1
-#define CAV_PREC_F16 2
-#define CAV_PREC_BF16 3
+ * FP32 otherwise; every reduced format stores f_i - w_i). */
+#define CAV_PREC_F64 0  /* FP64 f and g                                        */
+#define CAV_PREC_F32 1  /* FP32 f - w and g                                    */
+#define CAV_PREC_F16 2  /* binary16 f - w and g (scaled by 2^15)               */
+#define CAV_PREC_BF16 3 /* bfloat16 f - w and g                                */
+#define CAV_PREC_F16G 4 /* binary16 f - w, 16-bit fixed-point g               */
+/* The same three 16-bit encodings with stochastic rounding of every value
+ * the collision writes (unbiased; the random bits are a hash of seed, step
+ * and node, so results are reproducible). */
+#define CAV_PREC_F16SR 5
+#define CAV_PREC_BF16SR 6
+#define CAV_PREC_F16GSR 7
 
 /* Initial temperature field. */
 #define CAV_INIT_LINEAR 0 /* linear theta + noise, CavitySolver::new (solver.rs:159-176) */
