@@ -31,6 +31,7 @@ UNITS = {
     "prec_f16sr.cu": [],
     "prec_bf16sr.cu": [],
     "prec_f16gsr.cu": [],
+    "diag_noalloc.cu": [],
 }
 
 

@@ -183,6 +183,33 @@ int cav_get_stream(cav_handle* h, void** stream);
  * every kernel they contain; no counterpart in the reference). */
 int cav_launch_count(cav_handle* h, int64_t* n);
 
+/* ---- diagnostics without device allocation ------------------------------ */
+/* No counterpart in the reference.  The diagnostics of cav_diag computed on a
+ * cavity state that lives in the caller's own device memory, for callers that
+ * cannot let the library allocate device memory: a framework whose allocator
+ * has already reserved the device memory it may use, or a loop that cannot
+ * afford the device-wide synchronisation cudaMalloc / cudaFree may cause.
+ * This entry point allocates nothing.  Its reduction scratch is a static
+ * device array of CAV_NOALLOC_MAX_ROWS x 8 doubles (512 KiB), held by every
+ * GPU that loads the library until the process exits; larger ny is rejected
+ * with CAV_ERR_ARG.
+ *  - Inputs: device pointers to dense FP64 arrays, k = iy*nx + ix: rho, ux,
+ *    uy, t, nu_t [nx*ny] and the f populations f [nx*ny][9] (direction order
+ *    of this header); nu = molecular viscosity (for y+), lz = ny - 1.
+ *  - Output: out, a device pointer to 11 doubles in the field order of
+ *    cav_diag_out, the last being 1.0 when every field is finite (else 0.0).
+ *  - Runs asynchronously on `stream` (a cudaStream_t; NULL = default stream).
+ *  - The first call on a device (with that device current) looks up the
+ *    scratch's device address; make that first call before any stream
+ *    capture on that device.
+ *  - All calls on a device share the scratch: calls whose kernels can overlap
+ *    on the GPU race on it, so order them (same stream, or an event).
+ * Rejections return CAV_ERR_ARG / CAV_ERR_CUDA and print one line on stderr. */
+#define CAV_NOALLOC_MAX_ROWS 8192
+int cav_diag_noalloc(const double* rho, const double* ux, const double* uy, const double* t,
+                     const double* nu_t, const double* f, int32_t nx, int32_t ny, double nu, double lz,
+                     double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
