@@ -64,25 +64,27 @@ __device__ __forceinline__ void pull_node(const St* __restrict__ src, const Geom
                                           const StepScalars<typename Fmt<St>::A>& c,
                                           typename Fmt<St>::A (&f)[Q], typename Fmt<St>::A (&g)[Q]) {
     using A = typename Fmt<St>::A;
+    // 32-bit element offsets: 18 * plane < 2^31 is checked at allocation.
+    const int P = int(G.plane), W = G.pitch;
+    const int k = iy * W + ix;
+    const bool xm = ix > 0, xp = ix < G.nx - 1, ym = iy > 0, yp = iy < G.ny - 1;
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
-        const int sx = ix - CX(i), sy = iy - CY(i);
-        if (sx >= 0 && sx < G.nx && sy >= 0 && sy < G.ny)
-            f[i] = ldp(src, G, i, sy, sx);
-        else
-            f[i] = ldp(src, G, OPP(i), iy, ix);
+        const int cx = CX(i), cy = CY(i);
+        const bool ok = (cx > 0 ? xm : (cx < 0 ? xp : true)) && (cy > 0 ? ym : (cy < 0 ? yp : true));
+        const int idx = ok ? i * P + k - cx - cy * W : OPP(i) * P + k;  // else bounce-back
+        f[i] = Fmt<St>::load(src[idx], i);
     }
     const int gy = iy == 0 ? 1 : (iy == G.ny - 1 ? G.ny - 2 : iy);
-    if (ix == 0) {
-        const A tw = c.t_hot[gy];
+    const bool wall_col = (ix == 0) || (ix == G.nx - 1);
+    const A tw = ix == 0 ? c.t_hot[gy] : c.t_cold;
+    const int kg = wall_col ? k : gy * W + ix;
 #pragma unroll
-        for (int i = 0; i < Q; ++i) g[i] = geq_rest<A>(i, tw, c.geq_order);
-    } else if (ix == G.nx - 1) {
-#pragma unroll
-        for (int i = 0; i < Q; ++i) g[i] = geq_rest<A>(i, c.t_cold, c.geq_order);
-    } else {
-#pragma unroll
-        for (int i = 0; i < Q; ++i) g[i] = ldp(src, G, Q + i, gy - CY(i), ix - CX(i));
+    for (int i = 0; i < Q; ++i) {
+        // wall columns read their own node (a valid address) and discard it
+        const int idx = (Q + i) * P + (wall_col ? kg : kg - CX(i) - CY(i) * W);
+        const A v = Fmt<St>::load(src[idx], Q + i);
+        g[i] = wall_col ? geq_rest<A>(i, tw, c.geq_order) : v;
     }
 }
 
@@ -183,6 +185,7 @@ __global__ void __launch_bounds__(256) k_collide_ref(const St* __restrict__ src,
     Macro<A, SH> m;
     m.rho = rho[k];
     m.drho = m.rho - A(1.0);
+    m.inv_rho = A(1.0) / m.rho;
     m.ux = ux[k];
     m.uy = uy[k];
     m.t = tt[k];
@@ -270,6 +273,7 @@ __global__ void k_dbg_collide(St* __restrict__ pop, const typename Fmt<St>::A* _
     Macro<A, SH> m;
     m.rho = rho[k];
     m.drho = m.rho - A(1.0);
+    m.inv_rho = A(1.0) / m.rho;
     m.ux = ux[k];
     m.uy = uy[k];
     m.t = tt[k];

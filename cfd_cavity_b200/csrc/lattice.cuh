@@ -210,6 +210,8 @@ struct StepScalars {
     A alpha;   // ramped alpha_eff                                  (solver.rs:401-408)
     A cs;      // Smagorinsky constant
     A pr_t;    // turbulent Prandtl number
+    A inv_tau_s;  // 1 / tau_s
+    A inv_pr_t;   // 1 / pr_t
     A t_cold;  // cold-wall theta
     int geq_order;
     const A* t_hot;  // [ny] hot-wall theta
@@ -262,7 +264,7 @@ __device__ __forceinline__ float geq_f32(int i, float t, float ux, float uy, int
 // ---------------------------------------------------------------------------
 template <class A, bool SHIFT>
 struct Macro {
-    A rho, drho, ux, uy, t;
+    A rho, drho, ux, uy, t, inv_rho;
 };
 
 template <class A, bool SHIFT>
@@ -277,6 +279,7 @@ __device__ __forceinline__ Macro<A, SHIFT> macro_node(const A (&f)[Q], const A (
 #pragma unroll
     for (int j = 1; j < Q; ++j) tn = tn + g[j];
     A r;
+    m.inv_rho = A(0.0);
     if (SHIFT) {
         m.drho = s;
         r = A(1.0) + s;
@@ -284,10 +287,11 @@ __device__ __forceinline__ Macro<A, SHIFT> macro_node(const A (&f)[Q], const A (
         r = s;
         m.drho = s - A(1.0);
     }
-    if (SHIFT) {
-        A inv = A(1.0) / r;
+    if constexpr (SHIFT) {
+        const A inv = __fdividef(1.0f, r);
+        m.inv_rho = inv;
         un = un * inv;
-        vn = vn * inv + A(0.5) * fy_prev * inv;
+        vn = (vn + A(0.5) * fy_prev) * inv;
     } else if (r > A(2.220446049250313e-16)) {
         un = un / r;
         vn = vn / r;
@@ -360,45 +364,70 @@ __device__ __forceinline__ void collide_node(A (&f)[Q], A (&g)[Q], const Macro<A
 #pragma unroll
         for (int i = 0; i < Q; ++i) g[i] = g[i] + (-a_g * d_g[i] - b_g * d_g[OPP(i)]);
     } else {
-        // ---- FP32 on f_i - w_i ---------------------------------------------
-        float fyv = r * c.beta * temp;
+        // ---- FP32 on h_i = f_i - w_i, pairwise (i, opp(i)) form --------------
+        // For each pair p = (i, i+4), i = 1..4, split populations and
+        // equilibria into symmetric / antisymmetric parts: the TRT update
+        //   f_i += -a d_i - b d_opp + (1 - 1/2tau-) S-_i + (1 - 1/2tau+) S+_i
+        // with a = (w+ + w-)/2, b = (w+ - w-)/2 is exactly
+        //   f_p += E + O, f_opp += E - O,
+        //   E = -w+ (d_p + d_opp)/2 + k+ S+_p,  O = -w- (d_p - d_opp)/2 + k- S-_p,
+        // and pi_neq only needs the symmetric parts.  Same arithmetic as the
+        // reference up to rounding (FP32), a third of the operations.
+        const float fyv = r * c.beta * temp;
         fy_out = fyv;
-        float d_f[Q], d_g[Q];
+        const float u2 = u * u + v * v;
+        const float inv_r = m.inv_rho;
+        // rest population
+        const float feq0 = float(WD(0)) * (m.drho - 1.5f * r * u2);
+        const float d0 = f[0] - feq0;
+        float dS[5], dD[5], feS[5], feA[5];
 #pragma unroll
-        for (int i = 0; i < Q; ++i) {
-            d_f[i] = f[i] - feq_shift_f32(i, m.drho, r, u, v);
-            d_g[i] = g[i] - geq_f32(i, temp, u, v, c.geq_order);
+        for (int p = 1; p <= 4; ++p) {
+            const float cx = CX(p), cy = CY(p);
+            const float eu = cx * u + cy * v;
+            feS[p] = float(WD(p)) * (m.drho + r * (4.5f * eu * eu - 1.5f * u2));
+            feA[p] = float(WD(p)) * (r * 3.0f * eu);
+            dS[p] = (f[p] + f[p + 4]) - 2.0f * feS[p];
+            dD[p] = (f[p] - f[p + 4]) - 2.0f * feA[p];
         }
-        float pxx = ((((d_f[1] + d_f[3]) + d_f[4]) + d_f[5]) + d_f[7]) + d_f[8];
-        float pxy = ((d_f[3] - d_f[4]) + d_f[7]) - d_f[8];
-        float pyy = ((((d_f[2] + d_f[3]) + d_f[4]) + d_f[6]) + d_f[7]) + d_f[8];
-        float pi2 = pxx * pxx + 2.0f * pxy * pxy + pyy * pyy;
-        float rho_m = fmaxf(r, 1e-12f);
-        // |S| = sqrt(pi:pi) / (2 cs^2 tau rho), 2 cs^2 = 2/3.
-        float s_mag = sqrtf(pi2) / ((2.0f / 3.0f) * c.tau_s * rho_m);
-        float nut = c.cs * c.cs * s_mag;
+        // pi_neq (solver.rs:1096-1106) from the symmetric parts.
+        const float pxx = dS[1] + dS[3] + dS[4];
+        const float pxy = dS[3] - dS[4];
+        const float pyy = dS[2] + dS[3] + dS[4];
+        const float pi2 = pxx * pxx + 2.0f * pxy * pxy + pyy * pyy;
+        // |S| = sqrt(pi:pi) / (2 cs^2 tau rho) = sqrt(pi:pi) * (1.5 / tau) / rho
+        const float s_mag = __fsqrt_rn(pi2) * (1.5f * c.inv_tau_s) * inv_r;
+        const float nut = c.cs * c.cs * s_mag;
         nut_out = nut;
-        float tau_plus = 0.5f + 3.0f * (c.nu + nut);
-        float tau_minus = 0.5f + float(LAMBDA_TRT) / (tau_plus - 0.5f);
-        float tau_t = 0.5f + 3.0f * (c.alpha + nut / c.pr_t);
-        float om_p = 1.0f / tau_plus, om_m = 1.0f / tau_minus;
-        float a_f = 0.5f * (om_p + om_m);
-        float b_f = 0.5f * (om_p - om_m);
-        float a_g = 1.0f / tau_t;  // BGK for g (tau_t- = tau_t+), b_g = 0
-        float k_minus = 1.0f - 0.5f * om_m;
-        float k_plus = 1.0f - 0.5f * om_p;
+        const float e = 3.0f * (c.nu + nut);             // tau+ - 1/2
+        const float om_p = __fdividef(1.0f, 0.5f + e);   // 1/tau+
+        const float om_m = __fdividef(e, 0.5f * e + float(LAMBDA_TRT));  // 1/tau-, tau- = 1/2 + Lambda/e
+        const float om_g = __fdividef(1.0f, 0.5f + 3.0f * (c.alpha + nut * c.inv_pr_t));  // BGK g
+        const float k_p = 1.0f - 0.5f * om_p, k_m = 1.0f - 0.5f * om_m;
+        // Guo source: S+_p = w_p (-3 u_y + 9 (e.u) c_y) fy, S-_p = w_p 3 c_y fy.
+        f[0] = f[0] - om_p * d0 + k_p * float(WD(0)) * (-3.0f * v) * fyv;
 #pragma unroll
-        for (int i = 0; i < Q; ++i) {
-            const float cx = CX(i), cy = CY(i);
-            float ei_u = cx * u + cy * v;
-            // S_i = w_i [3 (c_y - u_y) + 9 (e.u) c_y] fy ; odd part w_i 3 c_y fy.
-            float s_i = float(WD(i)) * (3.0f * (cy - v) + 9.0f * ei_u * cy) * fyv;
-            float s_minus = float(WD(i)) * (3.0f * cy) * fyv;
-            float s_plus = s_i - s_minus;
-            f[i] = f[i] + (-a_f * d_f[i] - b_f * d_f[OPP(i)] + k_minus * s_minus + k_plus * s_plus);
+        for (int p = 1; p <= 4; ++p) {
+            const float cx = CX(p), cy = CY(p);
+            const float eu = cx * u + cy * v;
+            const float E = -0.5f * om_p * dS[p] + k_p * float(WD(p)) * (-3.0f * v + 9.0f * eu * cy) * fyv;
+            const float O = -0.5f * om_m * dD[p] + k_m * float(WD(p)) * (3.0f * cy) * fyv;
+            f[p] = f[p] + (E + O);
+            f[p + 4] = f[p + 4] + (E - O);
         }
+        // g: BGK towards geq (quadratic or linear in u).
+        const float one_m = 1.0f - om_g;
+        const float q2 = c.geq_order == 1 ? 0.0f : 1.0f;
+        g[0] = one_m * g[0] + om_g * float(WD(0)) * temp * (1.0f - q2 * 1.5f * u2);
 #pragma unroll
-        for (int i = 0; i < Q; ++i) g[i] = g[i] - a_g * d_g[i];
+        for (int p = 1; p <= 4; ++p) {
+            const float cx = CX(p), cy = CY(p);
+            const float eu = cx * u + cy * v;
+            const float gS = om_g * float(WD(p)) * temp * (1.0f + q2 * (4.5f * eu * eu - 1.5f * u2));
+            const float gA = om_g * float(WD(p)) * temp * (3.0f * eu);
+            g[p] = one_m * g[p] + (gS + gA);
+            g[p + 4] = one_m * g[p + 4] + (gS - gA);
+        }
     }
 }
 

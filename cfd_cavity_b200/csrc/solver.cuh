@@ -36,7 +36,7 @@
 namespace cav {
 
 constexpr int GRAPH_STEPS = 64;  // even: a replay leaves the buffer parity unchanged
-constexpr int BX = 32, BY = 8;
+constexpr int BX = 32, BY = 4;
 constexpr int DIAG_BLOCKS_MAX = 592;  // 4 x 148 SMs
 
 // xorshift64* (src/uniform/rng.rs:5-31) for the initial temperature noise.
@@ -173,6 +173,8 @@ struct Impl final : Solver {
         G.ny = p.ny;
         G.pitch = pitch;
         G.plane = (long long)p.ny * pitch;
+        if ((long long)NPLANES * G.plane >= (1ll << 31))
+            throw ArgError{CAV_ERR_ARG, "grid too large: 18 * ny * pitch must stay below 2^31 elements"};
         grd = dim3((p.nx + BX - 1) / BX, (p.ny + BY - 1) / BY);
         CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         const size_t pop_bytes = sizeof(St) * NPLANES * field_elems();
@@ -218,6 +220,8 @@ struct Impl final : Solver {
         c.alpha = A(alpha_eff);
         c.cs = A(p.cs);
         c.pr_t = A(p.pr_t);
+        c.inv_tau_s = A(1.0 / (0.5 + 3.0 * std::fmax(nu_eff, 0.002 / 3.0)));
+        c.inv_pr_t = A(1.0 / p.pr_t);
         c.t_cold = A(p.t_cold);
         c.geq_order = p.geq_order;
         c.t_hot = t_hot_d;
