@@ -43,7 +43,7 @@ PHYS = dict(pr=0.71, cs=0.10, pr_t=0.9, utarget=0.02, seed=42)
 CHUNK = 2000
 BYTES_PER_NODE = {"f64": 304, "f32": 152, "f16": 80, "bf16": 80, "f16g": 80, "f16sr": 80,
                   "bf16sr": 80, "f16gsr": 80}
-PRECISION = "f16"
+PRECISION = "f16sr"
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -126,6 +126,43 @@ def cpu_baseline(seconds=12.0, jobs=None):
                       f"({jobs} row-band threads)"}
 
 
+def batched_sweep(precisions, dev, steps=300):
+    """The 64-cavity sweep (configs[2]: Ra log-uniform in [1e6, 1e8], grids
+    {64x256, 96x384, 128x512}, Cs in [0.08, 0.12]) as one batched launch per
+    step: MLUPS and HBM roofline fraction per storage format, after the
+    autotuner picks the tile height and CTAs per SM."""
+    import torch
+
+    from cfd_cavity_b200 import CavityBatch, sweep_configs
+
+    cfg = sweep_configs(64)
+    nodes = sum(c["nx"] * c["ny"] for c in cfg)
+    peak, _ = measured_peaks()
+    out = {"cavities": len(cfg), "nodes": nodes}
+    for p in precisions:
+        bt = CavityBatch(cfg, precision=p, device=dev)
+        tun = bt.autotune(trial_steps=64)
+        bt.step(250)  # past the 200-step spin-up ramps of these grids
+        st = torch.cuda.ExternalStream(bt.stream_handle(), device=dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        bt.step(64)
+        with torch.cuda.stream(st):
+            e0.record(st)
+        bt.step(steps)
+        with torch.cuda.stream(st):
+            e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        mlups = nodes * steps / (ms * 1e-3) / 1e6
+        gbs = BYTES_PER_NODE[p] * nodes * steps / (ms * 1e-3) / 1e9
+        out[p] = {"mlups": mlups, "us_per_step": ms * 1e3 / steps, "achieved_gbs": gbs,
+                  "frac": gbs / peak, "tuning": tun}
+        bt.close()
+    if "f32" in out and "f16sr" in out:
+        out["f16sr_over_f32"] = out["f16sr"]["mlups"] / out["f32"]["mlups"]
+    return out
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -169,6 +206,7 @@ def main():
     ap.add_argument("--precision", default=PRECISION, choices=list(BYTES_PER_NODE))
     ap.add_argument("--chunk", type=int, default=CHUNK)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched-sweep and FP32 extras")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local, dist = dist_setup(args)
@@ -263,6 +301,25 @@ def main():
         te = float(tt.item())
     e2e_value = nodes * args.chunk * e2e_steps * world / te / 1e6
 
+    extras = {}
+    if not args.no_extras:
+        # FP32 storage on the same single cavity, same timing method
+        s32 = CavitySolver(NX, NY, RA, PHYS["pr"], PHYS["cs"], PHYS["pr_t"], PHYS["utarget"],
+                           PHYS["seed"], precision="f32", init_mode=L.CAV_INIT_ZERO, noise_amp=1e-4,
+                           device=dev)
+        st32 = torch.cuda.ExternalStream(s32.stream_handle(), device=dev)
+        s32.step(s32.info()["spin_up_steps"] + 64 + args.chunk)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(st32):
+            e0.record(st32)
+        s32.step(args.chunk * 3)
+        with torch.cuda.stream(st32):
+            e1.record(st32)
+        e1.synchronize()
+        extras["fp32_single_cavity_mlups"] = nodes * args.chunk * 3 / (e0.elapsed_time(e1) * 1e-3) / 1e6
+        s32.close()
+        extras["batched_sweep"] = batched_sweep(["f32", "f16sr", "f16gsr", "bf16sr", "f16"], dev)
+
     line = None
     if rank == 0:
         base = None
@@ -292,6 +349,7 @@ def main():
                     "note": "restart from host fields + CHUNK steps + read fields, per bench step"},
             "gpu_launches": launches,
             "clocks": clk,
+            "extras": extras,
         }
         print(json.dumps(line), flush=True)
     s.close()

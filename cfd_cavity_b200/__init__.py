@@ -5,6 +5,8 @@ Drop-in for the step of bbrangeo/cfd_cavity (``uniform::solver::CavitySolver``,
 ``include/cavity.h``; this package is its Python host mirror.
 """
 from ._lib import CavError, load  # noqa: F401
+from .batch import CavityBatch, sweep_configs  # noqa: F401
 from .solver import DELTA_T, T_COLD, T_HOT, CavitySolver, TimeAverager  # noqa: F401
 
-__all__ = ["CavitySolver", "TimeAverager", "CavError", "load", "T_HOT", "T_COLD", "DELTA_T"]
+__all__ = ["CavitySolver", "CavityBatch", "TimeAverager", "CavError", "load", "sweep_configs",
+           "T_HOT", "T_COLD", "DELTA_T"]

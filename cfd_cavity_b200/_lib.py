@@ -63,6 +63,10 @@ class CavDiag(ctypes.Structure):
                  "nusselt_volume")] + [("finite", ctypes.c_int32)]
 
 
+class CavBatchTuning(ctypes.Structure):
+    _fields_ = [("rows_per_item", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32)]
+
+
 class CavError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"[{code}] {msg}")
@@ -109,6 +113,20 @@ def load(path: str | None = None):
         "cav_sync": (i32, [vp]),
         "cav_get_stream": (i32, [vp, ctypes.POINTER(vp)]),
         "cav_launch_count": (i32, [vp, ctypes.POINTER(i64)]),
+        "cav_batch_create": (i32, [pp, i32, ctypes.POINTER(vp)]),
+        "cav_batch_destroy": (i32, [vp]),
+        "cav_batch_last_error": (ctypes.c_char_p, [vp]),
+        "cav_batch_step": (i32, [vp, i64]),
+        "cav_batch_get_fields": (i32, [vp, i32, _dp, _dp, _dp, _dp, _dp, _dp]),
+        "cav_batch_get_populations": (i32, [vp, i32, _dp, _dp]),
+        "cav_batch_diag": (i32, [vp, i32, ctypes.POINTER(CavDiag)]),
+        "cav_batch_info": (i32, [vp, ctypes.POINTER(i32), ctypes.POINTER(i64), ctypes.POINTER(i64)]),
+        "cav_batch_get_tuning": (i32, [vp, ctypes.POINTER(CavBatchTuning)]),
+        "cav_batch_set_tuning": (i32, [vp, ctypes.POINTER(CavBatchTuning)]),
+        "cav_batch_autotune": (i32, [vp, i32, ctypes.POINTER(CavBatchTuning)]),
+        "cav_batch_sync": (i32, [vp]),
+        "cav_batch_get_stream": (i32, [vp, ctypes.POINTER(vp)]),
+        "cav_batch_launch_count": (i32, [vp, ctypes.POINTER(i64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -121,4 +139,10 @@ def load(path: str | None = None):
 def check(rc: int, h=None):
     if rc != CAV_OK:
         msg = load().cav_last_error(h)
+        raise CavError(rc, msg.decode() if msg else "")
+
+
+def check_batch(rc: int, b=None):
+    if rc != CAV_OK:
+        msg = load().cav_batch_last_error(b)
         raise CavError(rc, msg.decode() if msg else "")

@@ -1,0 +1,276 @@
+// batch.cuh -- many cavities of uneven size and Rayleigh number advanced by
+// one launch per lattice step.
+//
+// Each cavity is an ordinary Impl<St> (own buffers, REF/PC state machine,
+// diagnostics); the batch only replaces their per-cavity fused launches by
+// one persistent-grid kernel over a work list of (cavity, 32-column x
+// `rows`-row) tiles: grid = ctas_per_sm x #SMs CTAs of 128 threads that
+// stride over the list.  Tiles are ordered cavity-major, row-block-minor, so
+// the tiles in flight at one time are neighbours and the halo rows they
+// share are served by L2.  Per-cavity step scalars (ramps, seeds, wall
+// temperature pointers) come from a device table precomputed on the host with
+// the single-cavity code (Impl::scalars), row min(step, spin_up), and every
+// node runs the same fused_node() as k_fused: a cavity advanced in a batch
+// is bit-identical to the same cavity advanced alone.  Steps run as CUDA
+// graphs of GRAPH_STEPS launches reading a device step counter.
+#pragma once
+
+#include "solver.cuh"
+
+namespace cav {
+
+template <class St>
+struct BatchCav {
+    St* pop[2];
+    typename Fmt<St>::A* fy;
+    typename Fmt<St>::A* nut;
+    Geom G;
+    int parity;   // buffer holding the state at batch step s: pop[(parity + s) & 1]
+    int spin_up;  // scalar-table row of the steady state
+};
+
+struct BatchItem {
+    int cav, tx0, ty0, rows;
+};
+
+constexpr int BATCH_THREADS = 128;
+
+template <class St, bool WRITE_NUT>
+__global__ void __launch_bounds__(BATCH_THREADS)
+    k_batch(const BatchCav<St>* __restrict__ cavs, const BatchItem* __restrict__ items, int n_items,
+            const StepScalars<typename Fmt<St>::A>* __restrict__ table, int n_cav, long long step,
+            const long long* __restrict__ step_dev) {
+    using A = typename Fmt<St>::A;
+    const long long s = step_dev ? *step_dev + step : step;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const BatchItem item = items[it];
+        const BatchCav<St> cv = cavs[item.cav];
+        const Geom G = cv.G;
+        const int row = s < cv.spin_up ? int(s) : cv.spin_up;
+        StepScalars<A> c = table[(long long)row * n_cav + item.cav];
+        c.step = s;
+        c.step_dev = nullptr;
+        const int cur = (cv.parity + int(s & 1)) & 1;
+        const St* src = cv.pop[cur];
+        St* dst = cv.pop[cur ^ 1];
+        const int ix = item.tx0 + lane;
+        if (ix < G.nx) {
+            for (int r = w; r < item.rows; r += BATCH_THREADS / 32)
+                fused_node<St, WRITE_NUT, false, false>(src, dst, cv.fy, cv.nut, nullptr, nullptr, G, ix,
+                                                        item.ty0 + r, c);
+        }
+    }
+}
+
+struct BatchTuning {
+    int rows_per_item = 8;
+    int ctas_per_sm = 8;
+};
+
+struct BatchBase {
+    virtual ~BatchBase() = default;
+    virtual void setup() = 0;
+    virtual void step(int64_t n) = 0;
+    virtual void set_tuning(const BatchTuning& t) = 0;
+    virtual double time_steps(int steps) = 0;  // ms for `steps` batched steps (advances the state)
+    virtual void sync() = 0;
+    std::vector<Solver*> cavs;  // owned
+    BatchTuning tun;
+    cudaStream_t stream = nullptr;
+    int64_t time_step = 0;
+    int64_t launches = 0;
+    long long total_nodes = 0;
+    std::string err;
+};
+
+template <class St>
+struct Batch final : BatchBase {
+    using A = typename Fmt<St>::A;
+    std::vector<Impl<St>*> cv;
+    BatchCav<St>* d_cavs = nullptr;
+    BatchItem* d_items = nullptr;
+    StepScalars<A>* d_table = nullptr;
+    long long* step_dev = nullptr;
+    long long step_dev_val = -1;
+    int n_items = 0, grid = 0, n_sm = 0, table_rows = 0;
+    cudaGraphExec_t graph = nullptr;
+    bool cavs_dirty = true;
+
+    ~Batch() override {
+        if (graph) cudaGraphExecDestroy(graph);
+        void* bufs[] = {d_cavs, d_items, d_table, step_dev};
+        for (void* b : bufs)
+            if (b) cudaFree(b);
+        for (Solver* s : cavs) delete s;
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    // Builds the device tables once all cavities exist (sharing `stream`).
+    void setup() override {
+        for (Solver* s : cavs) cv.push_back(static_cast<Impl<St>*>(s));
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+        const int n = int(cv.size());
+        int max_spin = 0;
+        for (auto* c : cv) {
+            max_spin = std::max<int>(max_spin, int(c->spin_up));
+            total_nodes += (long long)c->p.nx * c->p.ny;
+        }
+        table_rows = max_spin + 1;
+        std::vector<StepScalars<A>> tab(size_t(table_rows) * n);
+        for (int r = 0; r < table_rows; ++r)
+            for (int i = 0; i < n; ++i) tab[size_t(r) * n + i] = cv[i]->scalars(std::min<int64_t>(r, cv[i]->spin_up));
+        CK(cudaMalloc(&d_table, sizeof(StepScalars<A>) * tab.size()));
+        CK(cudaMemcpyAsync(d_table, tab.data(), sizeof(StepScalars<A>) * tab.size(), cudaMemcpyHostToDevice,
+                           stream));
+        CK(cudaMalloc(&d_cavs, sizeof(BatchCav<St>) * n));
+        CK(cudaMalloc(&step_dev, sizeof(long long)));
+        set_tuning(tun);
+        CK(cudaStreamSynchronize(stream));
+    }
+
+    void set_tuning(const BatchTuning& t) override {
+        if (t.rows_per_item < 1 || t.rows_per_item > 1024 || t.ctas_per_sm < 1 || t.ctas_per_sm > 32)
+            throw ArgError{CAV_ERR_ARG, "tuning out of range"};
+        tun = t;
+        std::vector<BatchItem> items;
+        for (int i = 0; i < int(cv.size()); ++i) {
+            const int nx = cv[i]->p.nx, ny = cv[i]->p.ny;
+            for (int y0 = 0; y0 < ny; y0 += t.rows_per_item)
+                for (int x0 = 0; x0 < nx; x0 += 32) items.push_back({i, x0, y0, std::min(t.rows_per_item, ny - y0)});
+        }
+        if (d_items) CK(cudaFree(d_items));
+        n_items = int(items.size());
+        CK(cudaMalloc(&d_items, sizeof(BatchItem) * items.size()));
+        CK(cudaMemcpyAsync(d_items, items.data(), sizeof(BatchItem) * items.size(), cudaMemcpyHostToDevice,
+                           stream));
+        grid = std::max(1, std::min(n_items, t.ctas_per_sm * n_sm));
+        if (graph) {
+            cudaGraphExecDestroy(graph);
+            graph = nullptr;
+        }
+        CK(cudaStreamSynchronize(stream));
+    }
+
+    // Brings every cavity to PC form at the shared step and refreshes the
+    // cavity table (buffer parity relative to the batch clock).
+    void enter() {
+        for (auto* c : cv) {
+            if (!c->pc_form) {
+                k_collide_ref<St><<<c->grd, c->blk, 0, stream>>>(c->pop[c->cur], c->pop[c->cur ^ 1], c->rho, c->ux,
+                                                                   c->uy, c->tt, c->fy, c->nut, c->G,
+                                                                   c->scalars(c->time_step));
+                c->check_launch();
+                c->cur ^= 1;
+                c->pc_form = true;
+                c->ref_cached = false;
+                c->time_step += 1;
+                cavs_dirty = true;
+            }
+        }
+        time_step = cv[0]->time_step;
+        for (auto* c : cv)
+            if (c->time_step != time_step) throw ArgError{CAV_ERR_STATE, "cavities of a batch out of step"};
+        if (cavs_dirty) {
+            std::vector<BatchCav<St>> h(cv.size());
+            for (size_t i = 0; i < cv.size(); ++i) {
+                auto* c = cv[i];
+                h[i].pop[0] = c->pop[0];
+                h[i].pop[1] = c->pop[1];
+                h[i].fy = c->fy;
+                h[i].nut = c->nut;
+                h[i].G = c->G;
+                h[i].parity = (c->cur + int(time_step & 1)) & 1;
+                h[i].spin_up = int(c->spin_up);
+            }
+            CK(cudaMemcpyAsync(d_cavs, h.data(), sizeof(BatchCav<St>) * h.size(), cudaMemcpyHostToDevice, stream));
+            CK(cudaStreamSynchronize(stream));
+            cavs_dirty = false;
+        }
+    }
+
+    void launch(bool write_nut, const long long* sdev, long long step) {
+        if (write_nut)
+            k_batch<St, true><<<grid, BATCH_THREADS, 0, stream>>>(d_cavs, d_items, n_items, d_table, int(cv.size()),
+                                                                   step, sdev);
+        else
+            k_batch<St, false><<<grid, BATCH_THREADS, 0, stream>>>(d_cavs, d_items, n_items, d_table,
+                                                                    int(cv.size()), step, sdev);
+        ++launches;
+        CK(cudaGetLastError());
+    }
+
+    cudaGraphExec_t get_graph() {
+        if (graph) return graph;
+        const int64_t l0 = launches;
+        CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        for (int j = 0; j < GRAPH_STEPS; ++j) launch(false, step_dev, j);
+        k_add_step<<<1, 1, 0, stream>>>(step_dev, GRAPH_STEPS);
+        cudaGraph_t gr;
+        CK(cudaStreamEndCapture(stream, &gr));
+        launches = l0;
+        CK(cudaGraphInstantiate(&graph, gr, 0));
+        cudaGraphDestroy(gr);
+        return graph;
+    }
+
+    void advance_cavities(int64_t k) {
+        for (auto* c : cv) {
+            if (k & 1) c->cur ^= 1;
+            c->time_step += k;
+            c->ref_cached = false;
+        }
+        time_step += k;
+    }
+
+    void step(int64_t n) override {
+        if (n <= 0) return;
+        bool entered_with_collide = false;
+        for (auto* c : cv) entered_with_collide |= !c->pc_form;
+        enter();  // may run one collision (the first step from a REF state)
+        if (entered_with_collide) n -= 1;
+        while (n > 0) {
+            if (n > GRAPH_STEPS) {
+                cudaGraphExec_t gx = get_graph();
+                if (step_dev_val != time_step) {
+                    k_set_step<<<1, 1, 0, stream>>>(step_dev, time_step);
+                    CK(cudaGetLastError());
+                    ++launches;
+                    step_dev_val = time_step;
+                }
+                CK(cudaGraphLaunch(gx, stream));
+                launches += GRAPH_STEPS + 1;
+                step_dev_val += GRAPH_STEPS;
+                advance_cavities(GRAPH_STEPS);
+                n -= GRAPH_STEPS;
+            } else {
+                launch(n == 1, nullptr, time_step);
+                advance_cavities(1);
+                n -= 1;
+            }
+        }
+    }
+
+    double time_steps(int steps) override {
+        enter();
+        cudaEvent_t a, b;
+        CK(cudaEventCreate(&a));
+        CK(cudaEventCreate(&b));
+        step(GRAPH_STEPS + 1);  // warm-up, builds the graph
+        CK(cudaEventRecord(a, stream));
+        step(steps);
+        CK(cudaEventRecord(b, stream));
+        CK(cudaEventSynchronize(b));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, a, b));
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        return ms;
+    }
+
+    void sync() override { CK(cudaStreamSynchronize(stream)); }
+};
+
+}  // namespace cav

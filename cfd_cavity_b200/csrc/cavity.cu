@@ -3,6 +3,10 @@
 // Every entry point maps one CavitySolver method or field access of the
 // reference (cited in include/cavity.h) onto a cav::Solver object; errors
 // become status codes and a per-handle message instead of panics.
+#include <map>
+#include <mutex>
+
+#include "batch.cuh"
 #include "solver.cuh"
 
 using namespace cav;
@@ -13,6 +17,10 @@ thread_local std::string g_create_error;
 
 struct cav_handle {
     std::unique_ptr<Solver> s;
+};
+
+struct cav_batch {
+    std::unique_ptr<BatchBase> b;
 };
 
 namespace {
@@ -37,6 +45,44 @@ int guarded(cav_handle* h, F&& fn) {
     } catch (const std::bad_alloc&) {
         return fail(h, CAV_ERR_NOMEM, "host allocation failed");
     }
+}
+
+// CavitySolver::new (src/uniform/solver.rs:108-210) on the device: validates
+// the parameters, derives the lattice units, allocates and uploads the
+// initial state.  Throws ArgError / CudaError.  `shared` (may be null) is a
+// stream the solver adopts instead of creating its own.
+Solver* build_solver(const cav_params& p, cudaStream_t shared) {
+    if (p.nx < 4 || p.ny < 4 || p.nx > 65536 || p.ny > 65536)
+        throw ArgError{CAV_ERR_ARG, "nx and ny must be in [4, 65536]"};
+    if (p.precision < CAV_PREC_F64 || p.precision > CAV_PREC_F16GSR) throw ArgError{CAV_ERR_ARG, "unknown precision"};
+    if (p.geq_order != 1 && p.geq_order != 2) throw ArgError{CAV_ERR_ARG, "geq_order must be 1 or 2"};
+    if (p.init_mode != CAV_INIT_LINEAR && p.init_mode != CAV_INIT_ZERO) throw ArgError{CAV_ERR_ARG, "unknown init_mode"};
+    Units U = derive_units(p);
+    std::unique_ptr<Solver> s(make_solver(p.precision));
+    s->p = p;
+    s->p.t_hot_profile = nullptr;
+    s->U = U;
+    s->spin_up = std::min<int64_t>(std::max<int64_t>(p.ny / 10, 200), 2000);
+    s->nu_start_mult = std::fmax(p.nu_start_mult, 1.0);
+    s->t_hot.assign(p.ny, 0.5);
+    if (p.t_hot_profile)
+        for (int i = 0; i < p.ny; ++i) s->t_hot[i] = p.t_hot_profile[i];
+    s->pitch = (p.nx + 31) / 32 * 32;
+    s->stream = shared;
+    CK(cudaSetDevice(p.device));
+    s->alloc();
+    // Initial temperature, src/uniform/solver.rs:159-176 (row-major RNG order).
+    std::vector<double> t0(size_t(p.nx) * p.ny);
+    Rng rng(p.seed);
+    for (int iy = 0; iy < p.ny; ++iy)
+        for (int ix = 0; ix < p.nx; ++ix) {
+            double xf = double(ix) / double(p.nx - 1);
+            double t_lin = 0.5 + (-0.5 - 0.5) * xf;
+            double pert = p.noise_amp * (2.0 * rng.next_f64() - 1.0);
+            t0[size_t(iy) * p.nx + ix] = (p.init_mode == CAV_INIT_LINEAR) ? t_lin + pert : pert;
+        }
+    s->init_default(t0);
+    return s.release();
 }
 
 }  // namespace
@@ -74,40 +120,9 @@ int cav_default_params(cav_params* p) {
 int cav_create(const cav_params* pp, cav_handle** out) {
     if (!pp || !out) return fail(nullptr, CAV_ERR_ARG, "null argument");
     *out = nullptr;
-    const cav_params& p = *pp;
-    if (p.nx < 4 || p.ny < 4 || p.nx > 65536 || p.ny > 65536)
-        return fail(nullptr, CAV_ERR_ARG, "nx and ny must be in [4, 65536]");
-    if (p.precision < CAV_PREC_F64 || p.precision > CAV_PREC_F16GSR)
-        return fail(nullptr, CAV_ERR_ARG, "unknown precision");
-    if (p.geq_order != 1 && p.geq_order != 2) return fail(nullptr, CAV_ERR_ARG, "geq_order must be 1 or 2");
-    if (p.init_mode != CAV_INIT_LINEAR && p.init_mode != CAV_INIT_ZERO)
-        return fail(nullptr, CAV_ERR_ARG, "unknown init_mode");
-    std::unique_ptr<Solver> s;
+    Solver* s = nullptr;
     try {
-        Units U = derive_units(p);
-        s.reset(make_solver(p.precision));
-        s->p = p;
-        s->p.t_hot_profile = nullptr;
-        s->U = U;
-        s->spin_up = std::min<int64_t>(std::max<int64_t>(p.ny / 10, 200), 2000);
-        s->nu_start_mult = std::fmax(p.nu_start_mult, 1.0);
-        s->t_hot.assign(p.ny, 0.5);
-        if (p.t_hot_profile)
-            for (int i = 0; i < p.ny; ++i) s->t_hot[i] = p.t_hot_profile[i];
-        s->pitch = (p.nx + 31) / 32 * 32;
-        CK(cudaSetDevice(p.device));
-        s->alloc();
-        // Initial temperature, src/uniform/solver.rs:159-176 (row-major RNG order).
-        std::vector<double> t0(size_t(p.nx) * p.ny);
-        Rng rng(p.seed);
-        for (int iy = 0; iy < p.ny; ++iy)
-            for (int ix = 0; ix < p.nx; ++ix) {
-                double xf = double(ix) / double(p.nx - 1);
-                double t_lin = 0.5 + (-0.5 - 0.5) * xf;
-                double pert = p.noise_amp * (2.0 * rng.next_f64() - 1.0);
-                t0[size_t(iy) * p.nx + ix] = (p.init_mode == CAV_INIT_LINEAR) ? t_lin + pert : pert;
-            }
-        s->init_default(t0);
+        s = build_solver(*pp, nullptr);
     } catch (const CudaError& e) {
         return fail(nullptr, e.e == cudaErrorMemoryAllocation ? CAV_ERR_NOMEM : CAV_ERR_CUDA,
                     std::string(e.where) + ": " + cudaGetErrorString(e.e));
@@ -117,7 +132,7 @@ int cav_create(const cav_params* pp, cav_handle** out) {
         return fail(nullptr, CAV_ERR_NOMEM, "host allocation failed");
     }
     cav_handle* h = new cav_handle;
-    h->s = std::move(s);
+    h->s.reset(s);
     *out = h;
     return CAV_OK;
 }
@@ -287,6 +302,28 @@ Solver* make_solver_f16sr();
 Solver* make_solver_bf16sr();
 Solver* make_solver_f16gsr();
 
+BatchBase* make_batch_f64();
+BatchBase* make_batch_f32();
+BatchBase* make_batch_f16();
+BatchBase* make_batch_bf16();
+BatchBase* make_batch_f16g();
+BatchBase* make_batch_f16sr();
+BatchBase* make_batch_bf16sr();
+BatchBase* make_batch_f16gsr();
+
+BatchBase* make_batch(int precision) {
+    switch (precision) {
+        case CAV_PREC_F64: return make_batch_f64();
+        case CAV_PREC_F32: return make_batch_f32();
+        case CAV_PREC_F16: return make_batch_f16();
+        case CAV_PREC_BF16: return make_batch_bf16();
+        case CAV_PREC_F16G: return make_batch_f16g();
+        case CAV_PREC_F16SR: return make_batch_f16sr();
+        case CAV_PREC_BF16SR: return make_batch_bf16sr();
+        default: return make_batch_f16gsr();
+    }
+}
+
 Solver* make_solver(int precision) {
     switch (precision) {
         case CAV_PREC_F64: return make_solver_f64();
@@ -300,3 +337,224 @@ Solver* make_solver(int precision) {
     }
 }
 }  // namespace cav
+
+// ---------------------------------------------------------------------------
+// Batches.
+// ---------------------------------------------------------------------------
+namespace cav {
+BatchBase* make_batch(int precision);
+}
+
+namespace {
+
+std::mutex g_tune_mutex;
+std::map<std::string, BatchTuning> g_tune_cache;  // grid class -> tuning chosen by the autotuner
+
+// Grid class of a batch: storage format and the multiset of cavity sizes.
+std::string grid_class(const BatchBase& b) {
+    std::map<std::pair<int, int>, int> sizes;
+    for (Solver* s : b.cavs) sizes[{s->p.nx, s->p.ny}] += 1;
+    std::string key = "prec" + std::to_string(b.cavs[0]->p.precision);
+    for (auto& kv : sizes)
+        key += ":" + std::to_string(kv.first.first) + "x" + std::to_string(kv.first.second) + "*" +
+               std::to_string(kv.second);
+    return key;
+}
+
+BatchBase* build_batch(const cav_params* ps, int n) {
+    if (n < 1) throw ArgError{CAV_ERR_ARG, "a batch needs at least one cavity"};
+    for (int i = 1; i < n; ++i)
+        if (ps[i].precision != ps[0].precision || ps[i].device != ps[0].device)
+            throw ArgError{CAV_ERR_ARG, "all cavities of a batch share one precision and one device"};
+    if (ps[0].precision < CAV_PREC_F64 || ps[0].precision > CAV_PREC_F16GSR)
+        throw ArgError{CAV_ERR_ARG, "unknown precision"};
+    CK(cudaSetDevice(ps[0].device));
+    std::unique_ptr<BatchBase> b(make_batch(ps[0].precision));
+    CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    for (int i = 0; i < n; ++i) b->cavs.push_back(build_solver(ps[i], b->stream));
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mutex);
+        auto it = g_tune_cache.find(grid_class(*b));
+        if (it != g_tune_cache.end()) b->tun = it->second;
+    }
+    b->setup();
+    return b.release();
+}
+
+int bfail(cav_batch* b, int code, const std::string& msg) {
+    if (b && b->b) b->b->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+template <class F>
+int bguarded(cav_batch* b, F&& fn) {
+    if (!b || !b->b) return bfail(nullptr, CAV_ERR_ARG, "null batch");
+    try {
+        cudaSetDevice(b->b->cavs[0]->p.device);
+        fn(*b->b);
+        return CAV_OK;
+    } catch (const CudaError& e) {
+        return bfail(b, CAV_ERR_CUDA, std::string(e.where) + ": " + cudaGetErrorString(e.e));
+    } catch (const ArgError& e) {
+        return bfail(b, e.code, e.msg);
+    } catch (const std::bad_alloc&) {
+        return bfail(b, CAV_ERR_NOMEM, "host allocation failed");
+    }
+}
+
+Solver* cavity_of(BatchBase& b, int32_t i) {
+    if (i < 0 || i >= int32_t(b.cavs.size())) throw ArgError{CAV_ERR_ARG, "cavity index out of range"};
+    return b.cavs[i];
+}
+
+}  // namespace
+
+extern "C" {
+
+int cav_batch_create(const cav_params* params, int32_t n, cav_batch** out) {
+    if (!params || !out) return bfail(nullptr, CAV_ERR_ARG, "null argument");
+    *out = nullptr;
+    BatchBase* b = nullptr;
+    try {
+        b = build_batch(params, n);
+    } catch (const CudaError& e) {
+        return bfail(nullptr, e.e == cudaErrorMemoryAllocation ? CAV_ERR_NOMEM : CAV_ERR_CUDA,
+                     std::string(e.where) + ": " + cudaGetErrorString(e.e));
+    } catch (const ArgError& e) {
+        return bfail(nullptr, e.code, e.msg);
+    } catch (const std::bad_alloc&) {
+        return bfail(nullptr, CAV_ERR_NOMEM, "host allocation failed");
+    }
+    cav_batch* h = new cav_batch;
+    h->b.reset(b);
+    *out = h;
+    return CAV_OK;
+}
+
+int cav_batch_destroy(cav_batch* b) {
+    if (!b) return CAV_ERR_ARG;
+    if (b->b) cudaSetDevice(b->b->cavs[0]->p.device);
+    delete b;
+    return CAV_OK;
+}
+
+const char* cav_batch_last_error(const cav_batch* b) {
+    if (b && b->b) return b->b->err.c_str();
+    return g_create_error.c_str();
+}
+
+int cav_batch_step(cav_batch* b, int64_t n) {
+    if (n < 0) return bfail(b, CAV_ERR_ARG, "negative step count");
+    return bguarded(b, [&](BatchBase& x) { x.step(n); });
+}
+
+int cav_batch_get_fields(cav_batch* b, int32_t i, double* rho, double* ux, double* uy, double* t, double* nu_t,
+                         double* fy) {
+    return bguarded(b, [&](BatchBase& x) { cavity_of(x, i)->get_fields(rho, ux, uy, t, nu_t, fy); });
+}
+
+int cav_batch_get_populations(cav_batch* b, int32_t i, double* f, double* g) {
+    return bguarded(b, [&](BatchBase& x) { cavity_of(x, i)->get_pops(f, g); });
+}
+
+int cav_batch_diag(cav_batch* b, int32_t i, cav_diag_out* o) {
+    if (!o) return bfail(b, CAV_ERR_ARG, "null output");
+    return bguarded(b, [&](BatchBase& x) {
+        double v[11];
+        cavity_of(x, i)->diag(v);
+        o->nusselt_hot = v[0];
+        o->nusselt_cold = v[1];
+        o->nusselt_hot_wall_link = v[2];
+        o->total_mass = v[3];
+        o->total_f_mass = v[4];
+        o->max_u = v[5];
+        o->max_uy = v[6];
+        o->nu_t_max = v[7];
+        o->y_plus_hot = v[8];
+        o->nusselt_volume = v[9];
+        o->finite = v[10] == 0.0 ? 1 : 0;
+    });
+}
+
+int cav_batch_info(cav_batch* b, int32_t* n_cavities, int64_t* total_nodes, int64_t* time_step) {
+    return bguarded(b, [&](BatchBase& x) {
+        if (n_cavities) *n_cavities = int32_t(x.cavs.size());
+        if (total_nodes) *total_nodes = x.total_nodes;
+        if (time_step) *time_step = x.cavs[0]->time_step;
+    });
+}
+
+int cav_batch_get_tuning(cav_batch* b, cav_batch_tuning* t) {
+    if (!t) return bfail(b, CAV_ERR_ARG, "null output");
+    return bguarded(b, [&](BatchBase& x) {
+        t->rows_per_item = x.tun.rows_per_item;
+        t->ctas_per_sm = x.tun.ctas_per_sm;
+    });
+}
+
+int cav_batch_set_tuning(cav_batch* b, const cav_batch_tuning* t) {
+    if (!t) return bfail(b, CAV_ERR_ARG, "null tuning");
+    return bguarded(b, [&](BatchBase& x) {
+        BatchTuning bt;
+        bt.rows_per_item = t->rows_per_item;
+        bt.ctas_per_sm = t->ctas_per_sm;
+        x.set_tuning(bt);
+    });
+}
+
+int cav_batch_autotune(cav_batch* b, int32_t trial_steps, cav_batch_tuning* chosen) {
+    if (trial_steps < 1) return bfail(b, CAV_ERR_ARG, "trial_steps must be positive");
+    return bguarded(b, [&](BatchBase& x) {
+        // Trials run on a twin batch built from the same parameters, so the
+        // state of this batch is untouched.
+        std::vector<cav_params> ps;
+        for (Solver* s : x.cavs) {
+            cav_params p = s->p;
+            p.t_hot_profile = s->t_hot.data();
+            ps.push_back(p);
+        }
+        std::unique_ptr<BatchBase> twin(build_batch(ps.data(), int(ps.size())));
+        const int rows_c[] = {2, 4, 8, 16, 32};
+        const int ctas_c[] = {4, 8, 12, 16};
+        BatchTuning best = x.tun;
+        double best_ms = 1e300;
+        for (int r : rows_c)
+            for (int c : ctas_c) {
+                BatchTuning t;
+                t.rows_per_item = r;
+                t.ctas_per_sm = c;
+                twin->set_tuning(t);
+                double ms = twin->time_steps(trial_steps);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = t;
+                }
+            }
+        x.set_tuning(best);
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mutex);
+            g_tune_cache[grid_class(x)] = best;
+        }
+        if (chosen) {
+            chosen->rows_per_item = best.rows_per_item;
+            chosen->ctas_per_sm = best.ctas_per_sm;
+        }
+    });
+}
+
+int cav_batch_sync(cav_batch* b) {
+    return bguarded(b, [&](BatchBase& x) { x.sync(); });
+}
+
+int cav_batch_get_stream(cav_batch* b, void** stream) {
+    if (!stream) return bfail(b, CAV_ERR_ARG, "null output");
+    return bguarded(b, [&](BatchBase& x) { *stream = (void*)x.stream; });
+}
+
+int cav_batch_launch_count(cav_batch* b, int64_t* n) {
+    if (!n) return bfail(b, CAV_ERR_ARG, "null output");
+    return bguarded(b, [&](BatchBase& x) { *n = x.launches; });
+}
+
+}  // extern "C"

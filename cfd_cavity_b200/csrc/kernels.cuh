@@ -27,24 +27,29 @@ __device__ __forceinline__ void stp(St* __restrict__ buf, const Geom& G, int q, 
     buf[(long long)q * G.plane + (long long)iy * G.pitch + ix] = Fmt<St>::store(v, q, r);
 }
 
-// Stores the 18 populations of one node; the stochastically rounded formats
-// draw their random bits from the (seed, step, node) stream.
+// Stores the 18 populations of one node (32-bit offsets, like pull_node);
+// the stochastically rounded formats draw their random bits from the
+// (seed, step, node) stream, two 16-bit draws per generator step.
 template <class St>
 __device__ __forceinline__ void store_node(St* __restrict__ dst, const Geom& G, int iy, int ix,
                                            const typename Fmt<St>::A (&f)[Q], const typename Fmt<St>::A (&g)[Q],
                                            const StepScalars<typename Fmt<St>::A>& c) {
+    const int P = int(G.plane);
+    const int k = iy * G.pitch + ix;
     if constexpr (Fmt<St>::SR) {
         const long long step = c.step_dev ? *c.step_dev + c.step : c.step;
         NodeRng rng(c.sr_seed, step, (long long)iy * G.nx + ix);
+        uint32_t r = 0;
 #pragma unroll
-        for (int i = 0; i < Q; ++i) stp(dst, G, i, iy, ix, f[i], rng.next());
-#pragma unroll
-        for (int i = 0; i < Q; ++i) stp(dst, G, Q + i, iy, ix, g[i], rng.next());
+        for (int q = 0; q < NPLANES; ++q) {
+            // high half of an LCG output, then its bits 0..15 shifted up
+            if ((q & 1) == 0) r = rng.next();
+            const uint32_t bits = (q & 1) == 0 ? (r & 0xffff0000u) : (r << 16);
+            dst[q * P + k] = Fmt<St>::store_sr(q < Q ? f[q] : g[q - Q], q, bits);
+        }
     } else {
 #pragma unroll
-        for (int i = 0; i < Q; ++i) stp(dst, G, i, iy, ix, f[i]);
-#pragma unroll
-        for (int i = 0; i < Q; ++i) stp(dst, G, Q + i, iy, ix, g[i]);
+        for (int q = 0; q < NPLANES; ++q) dst[q * P + k] = Fmt<St>::store(q < Q ? f[q] : g[q - Q], q, RN_BITS);
     }
 }
 
@@ -124,17 +129,14 @@ __device__ __forceinline__ bool is_wall(const Geom& G, int ix, int iy) {
 //  NO_COLLIDE  identity collision: checks the streaming / bounce-back /
 //              boundary index maps bit for bit.
 template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE>
-__global__ void __launch_bounds__(256) k_fused(const St* __restrict__ src, St* __restrict__ dst,
-                                               typename Fmt<St>::A* __restrict__ fy,
-                                               typename Fmt<St>::A* __restrict__ nut, double* __restrict__ acc_hot,
-                                               double* __restrict__ acc_cold, Geom G,
-                                               StepScalars<typename Fmt<St>::A> c) {
+__device__ __forceinline__ void fused_node(const St* __restrict__ src, St* __restrict__ dst,
+                                           typename Fmt<St>::A* __restrict__ fy,
+                                           typename Fmt<St>::A* __restrict__ nut, double* __restrict__ acc_hot,
+                                           double* __restrict__ acc_cold, const Geom& G, int ix, int iy,
+                                           const StepScalars<typename Fmt<St>::A>& c) {
     using A = typename Fmt<St>::A;
     constexpr bool SH = Fmt<St>::SHIFT;
-    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
-    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
-    if (ix >= G.nx || iy >= G.ny) return;
-    const long long k = (long long)iy * G.pitch + ix;
+    const int k = iy * G.pitch + ix;
     A f[Q], g[Q];
     pull_node<St>(src, G, ix, iy, c, f, g);
     const bool wall = is_wall(G, ix, iy);
@@ -156,6 +158,25 @@ __global__ void __launch_bounds__(256) k_fused(const St* __restrict__ src, St* _
         if (WRITE_NUT) nut[k] = nutv;
     }
     store_node<St>(dst, G, iy, ix, f, g, c);
+}
+
+// One full reference step, PC(src) -> PC(dst), one thread per node.
+//  WRITE_NUT   store nu_t of this collision (only the last step of a call
+//              needs it: the reference reads nu_t after step()).
+//  ACC_NU      add |T(1)-T(2)| and |T(nx-2)-T(nx-3)| of the streamed state
+//              to the per-row FP64 accumulators (nusselt_hot/cold, post.rs:68-111).
+//  NO_COLLIDE  identity collision: checks the streaming / bounce-back /
+//              boundary index maps bit for bit.
+template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE>
+__global__ void __launch_bounds__(256) k_fused(const St* __restrict__ src, St* __restrict__ dst,
+                                               typename Fmt<St>::A* __restrict__ fy,
+                                               typename Fmt<St>::A* __restrict__ nut, double* __restrict__ acc_hot,
+                                               double* __restrict__ acc_cold, Geom G,
+                                               StepScalars<typename Fmt<St>::A> c) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= G.nx || iy >= G.ny) return;
+    fused_node<St, WRITE_NUT, ACC_NU, NO_COLLIDE>(src, dst, fy, nut, acc_hot, acc_cold, G, ix, iy, c);
 }
 
 // collide(step) on a REF state (populations + fields), writing PC to dst.

@@ -87,9 +87,10 @@ __host__ __device__ __forceinline__ unsigned short h16_store(float x, bool sr, u
     float s = x * H_SCALE;
     __half h;
     if (sr) {
+        // (a non-finite input stays non-finite: inf + dither becomes NaN)
         uint32_t u;
         memcpy(&u, &s, 4);
-        if ((u & 0x7f800000u) != 0x7f800000u) u += (r >> 19);
+        u += (r >> 19);
         memcpy(&s, &u, 4);
         h = __float2half_rz(s);
     } else {
@@ -161,6 +162,14 @@ struct Fmt<P16<KIND, SRND>> {
         if (KIND == K_BF16) o.bits = bf16_store(x, sr, r);
         else if (KIND == K_MIX && q >= 9) o.bits = fx_store(x, q, sr, r);
         else o.bits = h16_store(x, sr, r);
+        return o;
+    }
+    // Always stochastic (the collision's writes).
+    __host__ __device__ static St store_sr(A x, int q, uint32_t r) {
+        St o;
+        if (KIND == K_BF16) o.bits = bf16_store(x, true, r);
+        else if (KIND == K_MIX && q >= 9) o.bits = fx_store(x, q, true, r);
+        else o.bits = h16_store(x, true, r);
         return o;
     }
 };

@@ -127,7 +127,8 @@ struct Solver {
     double nu_start_mult = 1.0;
     std::vector<double> t_hot;
     int pitch = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;  // set before alloc() to share a stream (batches)
+    bool own_stream = true;
     int64_t launches = 0;
     std::string err;
 };
@@ -163,7 +164,7 @@ struct Impl final : Solver {
                         partials, diag_out, sums, aos, step_dev};
         for (void* b : bufs)
             if (b) cudaFree(b);
-        if (stream) cudaStreamDestroy(stream);
+        if (stream && own_stream) cudaStreamDestroy(stream);
     }
 
     size_t field_elems() const { return size_t(G.ny) * G.pitch; }
@@ -176,7 +177,12 @@ struct Impl final : Solver {
         if ((long long)NPLANES * G.plane >= (1ll << 31))
             throw ArgError{CAV_ERR_ARG, "grid too large: 18 * ny * pitch must stay below 2^31 elements"};
         grd = dim3((p.nx + BX - 1) / BX, (p.ny + BY - 1) / BY);
-        CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        if (!stream) {
+            CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+            own_stream = true;
+        } else {
+            own_stream = false;
+        }
         const size_t pop_bytes = sizeof(St) * NPLANES * field_elems();
         for (int b = 0; b < 2; ++b) {
             CK(cudaMalloc(&pop[b], pop_bytes));

@@ -183,6 +183,37 @@ int cav_get_stream(cav_handle* h, void** stream);
  * every kernel they contain; no counterpart in the reference). */
 int cav_launch_count(cav_handle* h, int64_t* n);
 
+/* ---- batches: many cavities, one launch per step ------------------------- */
+/* No single counterpart in the reference, which runs one cavity per process
+ * (src/main.rs:42-443); a batch is n CavitySolver::new + lockstep step()
+ * calls.  Cavities may differ in size, Ra, Cs, seeds and wall profiles but
+ * share one precision and one device.  Each cavity of a batch evolves
+ * bit-identically to the same cavity created with cav_create. */
+typedef struct cav_batch cav_batch;
+typedef struct cav_batch_tuning {
+    int32_t rows_per_item; /* tile height (tiles are 32 columns wide)        */
+    int32_t ctas_per_sm;   /* persistent grid = ctas_per_sm x #SMs CTAs     */
+} cav_batch_tuning;
+int cav_batch_create(const cav_params* params, int32_t n, cav_batch** out);
+int cav_batch_destroy(cav_batch* b);
+const char* cav_batch_last_error(const cav_batch* b);
+/* n lockstep steps of every cavity (one kernel launch per step). */
+int cav_batch_step(cav_batch* b, int64_t n);
+int cav_batch_get_fields(cav_batch* b, int32_t i, double* rho, double* ux, double* uy, double* t,
+                         double* nu_t, double* fy);
+int cav_batch_get_populations(cav_batch* b, int32_t i, double* f, double* g);
+int cav_batch_diag(cav_batch* b, int32_t i, cav_diag_out* out);
+int cav_batch_info(cav_batch* b, int32_t* n_cavities, int64_t* total_nodes, int64_t* time_step);
+/* Tile / grid shape: set by hand, or chosen by timing candidates on a twin
+ * batch (the batch's own state is not advanced); the choice is cached per
+ * grid class (precision + multiset of cavity sizes) for later batches. */
+int cav_batch_get_tuning(cav_batch* b, cav_batch_tuning* t);
+int cav_batch_set_tuning(cav_batch* b, const cav_batch_tuning* t);
+int cav_batch_autotune(cav_batch* b, int32_t trial_steps, cav_batch_tuning* chosen);
+int cav_batch_sync(cav_batch* b);
+int cav_batch_get_stream(cav_batch* b, void** stream);
+int cav_batch_launch_count(cav_batch* b, int64_t* n);
+
 /* ---- diagnostics without device allocation ------------------------------ */
 /* No counterpart in the reference.  The diagnostics of cav_diag computed on a
  * cavity state that lives in the caller's own device memory, for callers that

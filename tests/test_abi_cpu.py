@@ -96,3 +96,26 @@ def test_missing_library_fails_loudly(tmp_path):
             L.load(str(tmp_path / "nope.so"))
         finally:
             L._lib = L._lib_saved
+
+
+def test_batch_rejects_bad_arguments_before_cuda():
+    lib = L.load()
+    h = ctypes.c_void_p()
+    ps = (L.CavParams * 2)()
+    for p in ps:
+        lib.cav_default_params(ctypes.byref(p))
+    assert lib.cav_batch_create(ps, 0, ctypes.byref(h)) == L.CAV_ERR_ARG
+    ps[1].precision = L.CAV_PREC_F32
+    assert lib.cav_batch_create(ps, 2, ctypes.byref(h)) == L.CAV_ERR_ARG
+    assert lib.cav_batch_last_error(None)
+    assert lib.cav_batch_step(None, 1) == L.CAV_ERR_ARG
+
+
+def test_sweep_configs_follow_the_benchmark_ranges():
+    from cfd_cavity_b200 import sweep_configs
+
+    cfg = sweep_configs(64, seed=2024)
+    assert len(cfg) == 64
+    assert {(c["nx"], c["ny"]) for c in cfg} == {(64, 256), (96, 384), (128, 512)}
+    assert all(1e6 <= c["ra"] <= 1e8 and 0.08 <= c["cs"] <= 0.12 for c in cfg)
+    assert cfg == sweep_configs(64, seed=2024)
