@@ -163,6 +163,27 @@ def batched_sweep(precisions, dev, steps=300):
     return out
 
 
+def adjoint_c4(dev):
+    """96x384, Ra=1e7, FP32; J = mean hot-wall Nu over steps
+    40 001-60 000 of 60 000, gradient w.r.t. the 384-value hot-wall profile
+    (seeded +-0.01 around 0.5) and Cs, checkpoints every 500 steps.  Ratio =
+    (forward with checkpoints + recomputation + adjoint sweep) / forward."""
+    from cfd_cavity_b200 import CavitySolver
+    from cfd_cavity_b200 import _lib as L
+    from cfd_cavity_b200.batch import Xorshift64Star
+
+    rng = Xorshift64Star(7)
+    th = np.array([0.5 + 0.01 * (2.0 * rng.next_f64() - 1.0) for _ in range(384)])
+    s = CavitySolver(96, 384, 1e7, 0.71, 0.1, 0.9, 0.02, 42, precision="f32", t_hot_profile=th,
+                     init_mode=L.CAV_INIT_ZERO, noise_amp=1e-4, device=dev)
+    J, gth, gcs, info = s.adjoint_nusselt(60_000, 40_001, 500)
+    s.close()
+    return {"ratio": (info["forward_ms"] + info["reverse_ms"]) / info["forward_ms"],
+            "forward_ms": info["forward_ms"], "reverse_ms": info["reverse_ms"], "J": J,
+            "dJ_dCs": gcs, "dJ_dtheta_l2": float(np.linalg.norm(gth)),
+            "checkpoints": info["checkpoints"]}
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -319,6 +340,7 @@ def main():
         extras["fp32_single_cavity_mlups"] = nodes * args.chunk * 3 / (e0.elapsed_time(e1) * 1e-3) / 1e6
         s32.close()
         extras["batched_sweep"] = batched_sweep(["f32", "f16sr", "f16gsr", "bf16sr", "f16"], dev)
+        extras["adjoint_c4"] = adjoint_c4(dev)
 
     line = None
     if rank == 0:

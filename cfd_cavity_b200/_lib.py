@@ -67,6 +67,17 @@ class CavBatchTuning(ctypes.Structure):
     _fields_ = [("rows_per_item", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32)]
 
 
+class CavAdjointSpec(ctypes.Structure):
+    _fields_ = [("n_steps", ctypes.c_int64), ("window_start", ctypes.c_int64),
+                ("checkpoint_every", ctypes.c_int32)]
+
+
+class CavAdjointResult(ctypes.Structure):
+    _fields_ = [("objective", ctypes.c_double), ("grad_cs", ctypes.c_double),
+                ("forward_ms", ctypes.c_double), ("reverse_ms", ctypes.c_double),
+                ("checkpoints", ctypes.c_int64)]
+
+
 class CavError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"[{code}] {msg}")
@@ -113,6 +124,8 @@ def load(path: str | None = None):
         "cav_sync": (i32, [vp]),
         "cav_get_stream": (i32, [vp, ctypes.POINTER(vp)]),
         "cav_launch_count": (i32, [vp, ctypes.POINTER(i64)]),
+        "cav_adjoint_run": (i32, [vp, ctypes.POINTER(CavAdjointSpec), _dp,
+                                  ctypes.POINTER(CavAdjointResult)]),
         "cav_batch_create": (i32, [pp, i32, ctypes.POINTER(vp)]),
         "cav_batch_destroy": (i32, [vp]),
         "cav_batch_last_error": (ctypes.c_char_p, [vp]),

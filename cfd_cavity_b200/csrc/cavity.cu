@@ -276,6 +276,19 @@ int cav_nu_accumulated(cav_handle* h, double* hot, double* cold, int64_t* n) {
     return guarded(h, [&](Solver& s) { s.nu_accumulated(hot, cold, n); });
 }
 
+int cav_adjoint_run(cav_handle* h, const cav_adjoint_spec* spec, double* grad_theta, cav_adjoint_result* res) {
+    if (!spec || !grad_theta || !res) return fail(h, CAV_ERR_ARG, "null argument");
+    return guarded(h, [&](Solver& s) {
+        double out[5];
+        s.adjoint_run(spec->n_steps, spec->window_start, spec->checkpoint_every, grad_theta, out);
+        res->objective = out[0];
+        res->grad_cs = out[1];
+        res->forward_ms = out[2];
+        res->reverse_ms = out[3];
+        res->checkpoints = int64_t(out[4]);
+    });
+}
+
 int cav_sync(cav_handle* h) {
     return guarded(h, [&](Solver& s) { s.sync(); });
 }

@@ -128,19 +128,23 @@ __device__ __forceinline__ bool is_wall(const Geom& G, int ix, int iy) {
 //              to the per-row FP64 accumulators (nusselt_hot/cold, post.rs:68-111).
 //  NO_COLLIDE  identity collision: checks the streaming / bounce-back /
 //              boundary index maps bit for bit.
+// fy_in / fy_out: the Guo force of the previous / this collision (the same
+// array in the production step, where every node reads then rewrites its own
+// entry; separate arrays when states are kept, as in the adjoint's
+// recomputation).
 template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE>
-__device__ __forceinline__ void fused_node(const St* __restrict__ src, St* __restrict__ dst,
-                                           typename Fmt<St>::A* __restrict__ fy,
-                                           typename Fmt<St>::A* __restrict__ nut, double* __restrict__ acc_hot,
-                                           double* __restrict__ acc_cold, const Geom& G, int ix, int iy,
-                                           const StepScalars<typename Fmt<St>::A>& c) {
+__device__ __forceinline__ void fused_node_io(const St* __restrict__ src, St* __restrict__ dst,
+                                              const typename Fmt<St>::A* fy_in, typename Fmt<St>::A* fy_out,
+                                              typename Fmt<St>::A* __restrict__ nut, double* __restrict__ acc_hot,
+                                              double* __restrict__ acc_cold, const Geom& G, int ix, int iy,
+                                              const StepScalars<typename Fmt<St>::A>& c) {
     using A = typename Fmt<St>::A;
     constexpr bool SH = Fmt<St>::SHIFT;
     const int k = iy * G.pitch + ix;
     A f[Q], g[Q];
     pull_node<St>(src, G, ix, iy, c, f, g);
     const bool wall = is_wall(G, ix, iy);
-    Macro<A, SH> m = macro_node<A, SH>(f, g, fy[k], wall);
+    Macro<A, SH> m = macro_node<A, SH>(f, g, fy_in[k], wall);
     if (ACC_NU) {
         if (ix == 1) {
             A t2 = gather_t<St>(src, G, 2, iy, c);
@@ -154,10 +158,18 @@ __device__ __forceinline__ void fused_node(const St* __restrict__ src, St* __res
     A fyv, nutv;
     if (!NO_COLLIDE) {
         collide_node<A, SH>(f, g, m, c, fyv, nutv);
-        fy[k] = fyv;
+        fy_out[k] = fyv;
         if (WRITE_NUT) nut[k] = nutv;
     }
     store_node<St>(dst, G, iy, ix, f, g, c);
+}
+
+template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE>
+__device__ __forceinline__ void fused_node(const St* __restrict__ src, St* __restrict__ dst,
+                                           typename Fmt<St>::A* fy, typename Fmt<St>::A* __restrict__ nut,
+                                           double* __restrict__ acc_hot, double* __restrict__ acc_cold,
+                                           const Geom& G, int ix, int iy, const StepScalars<typename Fmt<St>::A>& c) {
+    fused_node_io<St, WRITE_NUT, ACC_NU, NO_COLLIDE>(src, dst, fy, fy, nut, acc_hot, acc_cold, G, ix, iy, c);
 }
 
 // One full reference step, PC(src) -> PC(dst), one thread per node.

@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -30,6 +31,7 @@
 #include <vector>
 
 #include "../../include/cavity.h"
+#include "adjoint.cuh"
 #include "diag.cuh"
 #include "kernels.cuh"
 
@@ -120,6 +122,10 @@ struct Solver {
     virtual void nu_accumulate(bool on) = 0;
     virtual void nu_accumulated(double* hot, double* cold, int64_t* n) = 0;
     virtual void sync() = 0;
+    // Forward n_steps with checkpoints every ck_every steps, then the adjoint
+    // sweep; see Impl::adjoint_run.  out[0] = J, out[1] = dJ/dCs,
+    // out[2] = forward ms, out[3] = reverse ms, out[4] = checkpoints.
+    virtual void adjoint_run(int64_t n_steps, int64_t ws, int ck_every, double* grad_theta, double* out) = 0;
 
     cav_params p{};
     Units U{};
@@ -585,6 +591,283 @@ struct Impl final : Solver {
         if (hot) *hot = sh / denom * U.lz;
         if (cold) *cold = sc / denom * U.lz;
         if (n) *n = n_acc;
+    }
+
+
+    // ---- adjoint ---------------------------------------------------------------
+    // J = mean over s in [ws, N] of nusselt_hot(state after s steps).
+    // Forward: the production step (graphs included), storing the PC state
+    // every ck_every steps (X_1, X_{1+C}, ...).  Reverse: for each segment,
+    // last first, recompute its states from the checkpoint with k_fwd_slot,
+    // then run k_adj_step backwards through them.  Needs FP32 or FP64 storage
+    // and a fresh state (step 0, as after create or init_from_fields).
+    void adjoint_run(int64_t N, int64_t ws, int C, double* gth, double* out) override {
+        if constexpr (!(std::is_same<St, float>::value || std::is_same<St, double>::value)) {
+            throw ArgError{CAV_ERR_ARG, "the adjoint needs FP32 or FP64 storage"};
+        } else {
+            if (pc_form || time_step != 0)
+                throw ArgError{CAV_ERR_STATE, "adjoint_run starts from step 0 (after create or init_from_fields)"};
+            if (N < 2 || ws < 1 || ws > N || C < 2) throw ArgError{CAV_ERR_ARG, "bad adjoint spec"};
+            const size_t fld = field_elems(), popn = size_t(NPLANES) * fld;
+            const int64_t n_ck = (N - 1 + C - 1) / C;
+            St *ck_pop = nullptr, *seg_pop = nullptr;
+            A *ck_fy = nullptr, *seg_fy = nullptr, *P[2] = {nullptr, nullptr};
+            double *acc_cs_d = nullptr, *acc_th_d = nullptr;
+            cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+            struct Free {
+                std::vector<void*> v;
+                ~Free() {
+                    for (void* q : v)
+                        if (q) cudaFree(q);
+                }
+            } fr;
+            auto dalloc = [&](void** p2, size_t bytes) {
+                CK(cudaMalloc(p2, bytes));
+                fr.v.push_back(*p2);
+            };
+            dalloc((void**)&ck_pop, sizeof(St) * popn * n_ck);
+            dalloc((void**)&ck_fy, sizeof(A) * fld * n_ck);
+            St* seg_pop2 = nullptr;
+            A* seg_fy2 = nullptr;
+            dalloc((void**)&seg_pop, sizeof(St) * popn * C);
+            dalloc((void**)&seg_fy, sizeof(A) * fld * C);
+            dalloc((void**)&seg_pop2, sizeof(St) * popn * C);
+            dalloc((void**)&seg_fy2, sizeof(A) * fld * C);
+            long long* sdev2 = nullptr;
+            dalloc((void**)&sdev2, 2 * sizeof(long long));
+            for (auto& pp : P) dalloc((void**)&pp, sizeof(A) * APLANES * fld);
+            dalloc((void**)&acc_cs_d, sizeof(double) * size_t(p.nx) * p.ny);
+            dalloc((void**)&acc_th_d, sizeof(double) * p.ny);
+            CK(cudaMemsetAsync(acc_cs_d, 0, sizeof(double) * size_t(p.nx) * p.ny, stream));
+            CK(cudaMemsetAsync(acc_th_d, 0, sizeof(double) * p.ny, stream));
+            for (auto& e : ev) CK(cudaEventCreate(&e));
+            struct Ev {
+                cudaEvent_t* e;
+                ~Ev() {
+                    for (int i = 0; i < 3; ++i)
+                        if (e[i]) cudaEventDestroy(e[i]);
+                }
+            } evg{ev};
+            auto save_ck = [&](int64_t k) {
+                CK(cudaMemcpyAsync(ck_pop + popn * k, pop[cur], sizeof(St) * popn, cudaMemcpyDeviceToDevice, stream));
+                CK(cudaMemcpyAsync(ck_fy + fld * k, fy, sizeof(A) * fld, cudaMemcpyDeviceToDevice, stream));
+            };
+            // ---- reverse-sweep setup (before any timing) ----
+            // Per-step scalars as a device table (rows 0..spin_up) so that the
+            // segment sweeps can be captured once as CUDA graphs and replayed
+            // with the device step counter.
+            const int S = int(spin_up);
+            StepScalars<A>* table = nullptr;
+            {
+                std::vector<StepScalars<A>> tab(S + 1);
+                for (int r2 = 0; r2 <= S; ++r2) tab[r2] = scalars(r2);
+                dalloc((void**)&table, sizeof(StepScalars<A>) * tab.size());
+                CK(cudaMemcpyAsync(table, tab.data(), sizeof(StepScalars<A>) * tab.size(), cudaMemcpyHostToDevice,
+                                   stream));
+                CK(cudaStreamSynchronize(stream));
+            }
+            AdjObj<A> obj;
+            obj.ws = ws;
+            obj.coef = A(U.lz / (double(p.ny) * double(N - ws + 1)));
+            // Segments are processed last first.  The recomputation of
+            // segment k-1 (stream rs, slot set (k-1) & 1) overlaps the
+            // adjoint sweep of segment k (the solver's stream, set k & 1):
+            // both are latency-bound on one cavity, so the GPU runs them side
+            // by side.  Events order the reuse of a slot set.  Each stream has
+            // its own device step counter; full segments (length C, even) are
+            // CUDA graphs, one pair per slot set.
+            St* setp[2] = {seg_pop, seg_pop2};
+            A* setf[2] = {seg_fy, seg_fy2};
+            long long* sd_rec = sdev2;
+            long long* sd_adj = sdev2 + 1;
+            cudaStream_t rs = nullptr;
+            CK(cudaStreamCreateWithFlags(&rs, cudaStreamNonBlocking));
+            std::vector<cudaEvent_t> ev_rec(n_ck, nullptr), ev_adj(n_ck, nullptr);
+            cudaGraphExec_t g_rec[2] = {nullptr, nullptr}, g_adj[2] = {nullptr, nullptr};
+            struct Cleanup {
+                cudaStream_t* s;
+                std::vector<cudaEvent_t>* a;
+                std::vector<cudaEvent_t>* b;
+                cudaGraphExec_t* g1;
+                cudaGraphExec_t* g2;
+                ~Cleanup() {
+                    if (*s) {
+                        cudaStreamSynchronize(*s);
+                        cudaStreamDestroy(*s);
+                    }
+                    for (auto* v2 : {a, b})
+                        for (cudaEvent_t e : *v2)
+                            if (e) cudaEventDestroy(e);
+                    for (int i = 0; i < 2; ++i) {
+                        if (g1[i]) cudaGraphExecDestroy(g1[i]);
+                        if (g2[i]) cudaGraphExecDestroy(g2[i]);
+                    }
+                }
+            } cleanup{&rs, &ev_rec, &ev_adj, g_rec, g_adj};
+            for (int64_t k = 0; k < n_ck; ++k) {
+                CK(cudaEventCreateWithFlags(&ev_rec[k], cudaEventDisableTiming));
+                CK(cudaEventCreateWithFlags(&ev_adj[k], cudaEventDisableTiming));
+            }
+            const bool use_graphs = (C % 2) == 0;
+            auto capture = [&](cudaStream_t st, cudaGraphExec_t* out, auto&& body) {
+                const int64_t l0 = launches;
+                CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                body();
+                cudaGraph_t gr;
+                CK(cudaStreamEndCapture(st, &gr));
+                launches = l0;
+                CK(cudaGraphInstantiate(out, gr, 0));
+                cudaGraphDestroy(gr);
+            };
+            auto seg_len = [&](int64_t k) { return std::min<int64_t>(1 + k * C + C, N) - (1 + k * C); };
+            // recomputation of segment k on rs
+            auto recompute = [&](int64_t k) {
+                const int set = int(k & 1);
+                const int64_t a = 1 + k * C, L = seg_len(k);
+                St* sp = setp[set];
+                A* sf = setf[set];
+                if (k + 2 < n_ck) CK(cudaStreamWaitEvent(rs, ev_adj[k + 2], 0));  // set free again
+                CK(cudaMemcpyAsync(sp, ck_pop + popn * k, sizeof(St) * popn, cudaMemcpyDeviceToDevice, rs));
+                CK(cudaMemcpyAsync(sf, ck_fy + fld * k, sizeof(A) * fld, cudaMemcpyDeviceToDevice, rs));
+                if (use_graphs && L == C) {
+                    if (!g_rec[set])
+                        capture(rs, &g_rec[set], [&] {
+                            for (int64_t j = 0; j + 1 < C; ++j)
+                                k_fwd_slot<St><<<grd, blk, 0, rs>>>(sp + popn * j, sp + popn * (j + 1), sf + fld * j,
+                                                                    sf + fld * (j + 1), G, table, S, sd_rec, j);
+                        });
+                    k_set_step<<<1, 1, 0, rs>>>(sd_rec, a);
+                    check_launch();
+                    CK(cudaGraphLaunch(g_rec[set], rs));
+                    launches += C - 1;
+                } else {
+                    for (int64_t j = 0; j + 1 < L; ++j) {
+                        k_fwd_slot<St><<<grd, blk, 0, rs>>>(sp + popn * j, sp + popn * (j + 1), sf + fld * j,
+                                                            sf + fld * (j + 1), G, table, S, nullptr, a + j);
+                        check_launch();
+                    }
+                }
+                CK(cudaEventRecord(ev_rec[k], rs));
+            };
+            int cp = 0;
+            // adjoint sweep of segment k on the solver's stream
+            auto sweep = [&](int64_t k) {
+                const int set = int(k & 1);
+                const int64_t a = 1 + k * C, L = seg_len(k);
+                St* sp = setp[set];
+                A* sf = setf[set];
+                CK(cudaStreamWaitEvent(stream, ev_rec[k], 0));
+                if (use_graphs && L == C) {
+                    if (cp != 0) throw ArgError{CAV_ERR_STATE, "adjoint ping-pong out of phase"};
+                    if (!g_adj[set])
+                        capture(stream, &g_adj[set], [&] {
+                            int q = 0;
+                            for (int64_t j = C - 1; j >= 0; --j) {
+                                k_adj_step<St><<<grd, blk, 0, stream>>>(sp + popn * j, sf + fld * j, P[q], P[q ^ 1],
+                                                                        acc_cs_d, acc_th_d, G, table, S, sd_adj, j,
+                                                                        obj);
+                                q ^= 1;
+                            }
+                        });
+                    k_set_step<<<1, 1, 0, stream>>>(sd_adj, a);
+                    check_launch();
+                    CK(cudaGraphLaunch(g_adj[set], stream));
+                    launches += C;
+                } else {
+                    for (int64_t j = L - 1; j >= 0; --j) {
+                        k_adj_step<St><<<grd, blk, 0, stream>>>(sp + popn * j, sf + fld * j, P[cp], P[cp ^ 1],
+                                                                acc_cs_d, acc_th_d, G, table, S, nullptr, a + j, obj);
+                        check_launch();
+                        cp ^= 1;
+                    }
+                }
+                CK(cudaEventRecord(ev_adj[k], stream));
+            };
+            // Build the segment graphs now, outside the timed passes (they only
+            // depend on the buffers, not on the state).
+            if (use_graphs && N - 1 >= C) {
+                const int64_t l0 = launches;
+                for (int set = 0; set < 2; ++set) {
+                    St* sp = setp[set];
+                    A* sf = setf[set];
+                    capture(rs, &g_rec[set], [&] {
+                        for (int64_t j = 0; j + 1 < C; ++j)
+                            k_fwd_slot<St><<<grd, blk, 0, rs>>>(sp + popn * j, sp + popn * (j + 1), sf + fld * j,
+                                                                sf + fld * (j + 1), G, table, S, sd_rec, j);
+                    });
+                    capture(stream, &g_adj[set], [&] {
+                        int q = 0;
+                        for (int64_t j = C - 1; j >= 0; --j) {
+                            k_adj_step<St><<<grd, blk, 0, stream>>>(sp + popn * j, sf + fld * j, P[q], P[q ^ 1],
+                                                                    acc_cs_d, acc_th_d, G, table, S, sd_adj, j, obj);
+                            q ^= 1;
+                        }
+                    });
+                    CK(cudaGraphUpload(g_rec[set], rs));
+                    CK(cudaGraphUpload(g_adj[set], stream));
+                }
+                launches = l0;
+                CK(cudaStreamSynchronize(rs));
+                CK(cudaStreamSynchronize(stream));
+            }
+            // ---- forward ----
+            CK(cudaEventRecord(ev[0], stream));
+            nu_accumulate(false);
+            if (ws == 1) nu_accumulate(true);
+            step(1);  // X_1
+            save_ck(0);
+            int64_t next_ck = 1;
+            while (time_step < N) {
+                if (!acc_on && time_step == ws - 1) nu_accumulate(true);
+                int64_t stop = N;
+                if (next_ck < n_ck) stop = std::min<int64_t>(stop, 1 + next_ck * C);
+                if (!acc_on && ws - 1 > time_step) stop = std::min<int64_t>(stop, ws - 1);
+                step(stop - time_step);
+                if (next_ck < n_ck && time_step == 1 + next_ck * C) save_ck(next_ck++);
+            }
+            double J = 0.0, jc = 0.0;
+            int64_t nacc = 0;
+            nu_accumulated(&J, &jc, &nacc);
+            nu_accumulate(false);
+            CK(cudaEventRecord(ev[1], stream));
+            // ---- reverse ----
+            // The P ping-pong must sit in P[0] when the first full-segment
+            // graph runs: start in P[1] when the (processed first) partial
+            // last segment has an odd length.
+            {
+                const int64_t L_last = seg_len(n_ck - 1);
+                cp = (use_graphs && L_last != C && (L_last & 1)) ? 1 : 0;
+            }
+            k_adj_final<St><<<grd, blk, 0, stream>>>(pop[cur], P[cp], G, scalars(N), obj, N);
+            check_launch();
+            CK(cudaStreamWaitEvent(rs, ev[1], 0));  // checkpoints complete
+            recompute(n_ck - 1);
+            for (int64_t k = n_ck - 1; k >= 0; --k) {
+                if (k >= 1) recompute(k - 1);
+                sweep(k);
+            }
+            CK(cudaEventRecord(ev[2], stream));
+            std::vector<double> acs(size_t(p.nx) * p.ny), ath(p.ny);
+            CK(cudaMemcpyAsync(acs.data(), acc_cs_d, sizeof(double) * acs.size(), cudaMemcpyDeviceToHost, stream));
+            CK(cudaMemcpyAsync(ath.data(), acc_th_d, sizeof(double) * ath.size(), cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+            double gcs = 0.0;
+            for (double v2 : acs) gcs += v2;
+            // wall rows 0 and ny-1 take theta of rows 1 and ny-2 (solver.rs:974-987)
+            for (int i = 0; i < p.ny; ++i) gth[i] = 0.0;
+            for (int i = 0; i < p.ny; ++i) {
+                const int gy = i == 0 ? 1 : (i == p.ny - 1 ? p.ny - 2 : i);
+                gth[gy] += ath[i];
+            }
+            float ms_f = 0.f, ms_r = 0.f;
+            CK(cudaEventElapsedTime(&ms_f, ev[0], ev[1]));
+            CK(cudaEventElapsedTime(&ms_r, ev[1], ev[2]));
+            out[0] = J;
+            out[1] = gcs;
+            out[2] = ms_f;
+            out[3] = ms_r;
+            out[4] = double(n_ck);
+        }
     }
 
     void sync() override { CK(cudaStreamSynchronize(stream)); }

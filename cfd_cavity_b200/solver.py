@@ -207,6 +207,21 @@ class CavitySolver:
         """``total_f_mass`` (src/uniform/solver.rs:1018-1020)."""
         return self.diag()["total_f_mass"]
 
+    # -- adjoint -----------------------------------------------------------------
+    def adjoint_nusselt(self, n_steps, window_start, checkpoint_every=500):
+        """Gradients of J = mean over s in [window_start, n_steps] of the hot-wall
+        Nusselt number (post.rs:68-78) w.r.t. the hot-wall theta profile and
+        Cs, by the discrete adjoint with checkpoint-and-recompute.  Starts from
+        step 0 and leaves the solver at step n_steps.  Returns
+        (J, dJ/dtheta_w [ny], dJ/dCs, info)."""
+        spec = L.CavAdjointSpec(int(n_steps), int(window_start), int(checkpoint_every))
+        res = L.CavAdjointResult()
+        gth = np.empty(self._ny)
+        self._ck(L.load().cav_adjoint_run(self._h, ctypes.byref(spec), _dp(gth), ctypes.byref(res)))
+        info = {"forward_ms": res.forward_ms, "reverse_ms": res.reverse_ms,
+                "checkpoints": res.checkpoints}
+        return res.objective, gth, res.grad_cs, info
+
     # -- per-step Nusselt accumulation --------------------------------------------
     def nu_accumulate(self, enable=True):
         self._ck(L.load().cav_nu_accumulate(self._h, 1 if enable else 0))

@@ -183,6 +183,31 @@ int cav_get_stream(cav_handle* h, void** stream);
  * every kernel they contain; no counterpart in the reference). */
 int cav_launch_count(cav_handle* h, int64_t* n);
 
+/* ---- adjoint: gradients of the time-averaged hot-wall Nusselt number ------ */
+/* No counterpart in the reference (it has no gradients).  Objective
+ * J = mean over s in [window_start, n_steps] of nusselt_hot (post.rs:68-78)
+ * of the state after s steps.  Runs the forward from step 0 (the handle must
+ * be fresh: just created or re-initialised with cav_init_from_fields),
+ * storing the state every checkpoint_every steps, then the hand-written
+ * adjoint backwards with checkpoint-and-recompute.  FP32 or FP64 storage.
+ * The handle ends at step n_steps, exactly as after cav_step(h, n_steps). */
+typedef struct cav_adjoint_spec {
+    int64_t n_steps;          /* N                                          */
+    int64_t window_start;     /* first state of the average (1 <= ws <= N)  */
+    int32_t checkpoint_every; /* forward states kept every this many steps  */
+} cav_adjoint_spec;
+typedef struct cav_adjoint_result {
+    double objective;  /* J                                                 */
+    double grad_cs;    /* dJ/dCs                                            */
+    double forward_ms; /* forward pass with checkpoints (device time)       */
+    double reverse_ms; /* recomputation + adjoint sweep (device time)       */
+    int64_t checkpoints;
+} cav_adjoint_result;
+/* grad_theta[ny] = dJ/dtheta_w[iy] for the hot-wall profile (cav_params.
+ * t_hot_profile; rows 0 and ny-1 are never used by the boundary condition
+ * and get 0). */
+int cav_adjoint_run(cav_handle* h, const cav_adjoint_spec* spec, double* grad_theta, cav_adjoint_result* res);
+
 /* ---- batches: many cavities, one launch per step ------------------------- */
 /* No single counterpart in the reference, which runs one cavity per process
  * (src/main.rs:42-443); a batch is n CavitySolver::new + lockstep step()

@@ -86,6 +86,8 @@ def lib():
         L.orc_velocity.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
                                    ctypes.POINTER(ctypes.c_int32)]
         L.orc_nusselt.argtypes = [vp, dp, dp]
+        L.orc_tl_nusselt.restype = ctypes.c_int
+        L.orc_tl_nusselt.argtypes = [ctypes.POINTER(OrcParams), i64, i64, dp, ctypes.c_double, dp, dp]
         L.orc_avg_create.restype = vp
         L.orc_avg_create.argtypes = [i64]
         L.orc_avg_destroy.argtypes = [vp]
@@ -125,6 +127,30 @@ def velocities():
 
 class OracleError(RuntimeError):
     pass
+
+
+def tangent_nusselt(nx, ny, ra, pr, cs, pr_t, utarget, seed, n_steps, ws, dtheta=None, dcs=0.0,
+                    *, jobs=1, nu_override=None, init_mode=INIT_LINEAR, noise_amp=1.0e-3,
+                    geq_order=2, t_hot_profile=None, t_cold=T_COLD):
+    """FP64 tangent-linear oracle: (J, dJ . v) with J the mean hot-wall Nusselt
+    number over the states after s steps, s in [ws, n_steps], and
+    v = (dtheta, dcs) a direction in (hot-wall theta profile, Cs)."""
+    p = OrcParams()
+    p.nx, p.ny, p.ra, p.pr, p.cs, p.pr_t, p.utarget = nx, ny, ra, pr, cs, pr_t, utarget
+    p.seed, p.jobs, p.alpha_mult, p.nu_start_mult = seed, jobs, 1.0, 1.0
+    p.has_nu_override = 0 if nu_override is None else 1
+    p.nu_override = 0.0 if nu_override is None else nu_override
+    p.init_mode, p.noise_amp, p.geq_order, p.t_cold = init_mode, noise_amp, geq_order, t_cold
+    th = None
+    if t_hot_profile is not None:
+        th = np.ascontiguousarray(t_hot_profile, dtype=np.float64)
+        p.t_hot_profile = _dp(th)
+    dth = None if dtheta is None else np.ascontiguousarray(dtheta, dtype=np.float64)
+    J, dJ = ctypes.c_double(), ctypes.c_double()
+    rc = lib().orc_tl_nusselt(ctypes.byref(p), n_steps, ws, _dp(dth), dcs, ctypes.byref(J), ctypes.byref(dJ))
+    if rc != 0:
+        raise OracleError(f"orc_tl_nusselt failed with code {rc}")
+    return J.value, dJ.value
 
 
 class OracleSolver:

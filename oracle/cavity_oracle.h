@@ -72,6 +72,12 @@ int64_t orc_avg_means(void* a, double* ux, double* uy, double* t, double* nu_t, 
 /* nusselt_from_mean, src/main.rs:740-753. */
 double orc_nusselt_from_mean(void* h, const double* t_mean, int32_t hot);
 
+/* FP64 tangent-linear oracle: J = mean of nusselt_hot over the states after
+ * s steps, s in [ws, n_steps], and dJ . v for v = (dtheta[ny], dcs) in the
+ * (hot-wall profile, Cs) parameters.  Returns 0 or the orc_create error. */
+int orc_tl_nusselt(const orc_params* p, int64_t n_steps, int64_t ws, const double* dtheta, double dcs,
+                   double* J, double* dJ);
+
 #ifdef __cplusplus
 }
 #endif
