@@ -6,7 +6,8 @@ Drop-in for the step of bbrangeo/cfd_cavity (``uniform::solver::CavitySolver``,
 """
 from ._lib import CavError, load  # noqa: F401
 from .batch import CavityBatch, sweep_configs  # noqa: F401
+from .octree import OctreeSolver  # noqa: F401
 from .solver import DELTA_T, T_COLD, T_HOT, CavitySolver, TimeAverager  # noqa: F401
 
-__all__ = ["CavitySolver", "CavityBatch", "TimeAverager", "CavError", "load", "sweep_configs",
+__all__ = ["CavitySolver", "CavityBatch", "OctreeSolver", "TimeAverager", "CavError", "load", "sweep_configs",
            "T_HOT", "T_COLD", "DELTA_T"]

@@ -78,6 +78,40 @@ class CavAdjointResult(ctypes.Structure):
                 ("checkpoints", ctypes.c_int64)]
 
 
+CAV_OCT_F64, CAV_OCT_F32, CAV_OCT_F32_F16, CAV_OCT_F32_F16G = range(4)
+OCT_PRECISIONS = {"f64": CAV_OCT_F64, "f32": CAV_OCT_F32, "f32_f16": CAV_OCT_F32_F16,
+                  "f32_f16g": CAV_OCT_F32_F16G}
+
+
+class CavOctreeParams(ctypes.Structure):
+    _fields_ = [
+        ("nx0", ctypes.c_int32), ("ny0", ctypes.c_int32), ("bl_width", ctypes.c_int32),
+        ("ra", ctypes.c_double), ("pr", ctypes.c_double), ("utarget", ctypes.c_double),
+        ("seed", ctypes.c_uint64), ("jobs", ctypes.c_int32), ("odd_exact", ctypes.c_int32),
+        ("levels", ctypes.c_int32), ("nu_start_mult", ctypes.c_double),
+        ("has_nu_override", ctypes.c_int32), ("nu_override", ctypes.c_double),
+        ("precision", ctypes.c_int32), ("device", ctypes.c_int32),
+    ]
+
+
+class CavOctreeInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("nu", "alpha", "beta_eff_coarse")] + [
+        ("tau_plus", ctypes.c_double * 3)] + [
+        (n, ctypes.c_double) for n in ("xi_even", "xi_odd", "xi_thermal", "xi_even_sub",
+                                       "xi_odd_sub", "xi_thermal_sub")] + [
+        ("time_step", ctypes.c_int64), ("spin_up_steps", ctypes.c_int64),
+        ("n_nodes_total", ctypes.c_int64), ("levels", ctypes.c_int32),
+        ("precision", ctypes.c_int32), ("nx", ctypes.c_int32 * 5), ("ny", ctypes.c_int32 * 5),
+        ("n_ghosts", ctypes.c_int32), ("n_coincident", ctypes.c_int32),
+        ("n_ghosts_sub", ctypes.c_int32), ("n_coincident_sub", ctypes.c_int32)]
+
+
+class CavOctreeDiag(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in
+                ("nu_hot", "nu_hot_link0", "nu_cold", "nu_hot_fine", "max_u", "mass",
+                 "max_rho_dev", "max_rho_dev_ifaces", "finite", "y_plus_fine")]
+
+
 class CavError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"[{code}] {msg}")
@@ -140,6 +174,20 @@ def load(path: str | None = None):
         "cav_batch_sync": (i32, [vp]),
         "cav_batch_get_stream": (i32, [vp, ctypes.POINTER(vp)]),
         "cav_batch_launch_count": (i32, [vp, ctypes.POINTER(i64)]),
+        "cav_octree_default_params": (i32, [ctypes.POINTER(CavOctreeParams)]),
+        "cav_octree_create": (i32, [ctypes.POINTER(CavOctreeParams), ctypes.POINTER(vp)]),
+        "cav_octree_destroy": (i32, [vp]),
+        "cav_octree_last_error": (ctypes.c_char_p, [vp]),
+        "cav_octree_step": (i32, [vp, i64]),
+        "cav_octree_get_info": (i32, [vp, ctypes.POINTER(CavOctreeInfo)]),
+        "cav_octree_get_level": (i32, [vp, i32, _dp, _dp, _dp, _dp, _dp, _dp]),
+        "cav_octree_set_level": (i32, [vp, i32, _dp, _dp, _dp, _dp, _dp, _dp]),
+        "cav_octree_couple": (i32, [vp, i32]),
+        "cav_octree_diag": (i32, [vp, ctypes.POINTER(CavOctreeDiag)]),
+        "cav_octree_check_guards": (i32, [vp, ctypes.c_double]),
+        "cav_octree_sync": (i32, [vp]),
+        "cav_octree_get_stream": (i32, [vp, ctypes.POINTER(vp)]),
+        "cav_octree_launch_count": (i32, [vp, ctypes.POINTER(i64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -152,6 +200,12 @@ def load(path: str | None = None):
 def check(rc: int, h=None):
     if rc != CAV_OK:
         msg = load().cav_last_error(h)
+        raise CavError(rc, msg.decode() if msg else "")
+
+
+def check_octree(rc: int, h=None):
+    if rc != CAV_OK:
+        msg = load().cav_octree_last_error(h)
         raise CavError(rc, msg.decode() if msg else "")
 
 

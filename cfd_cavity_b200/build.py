@@ -1,8 +1,8 @@
 """Builds the CUDA library ``libcavity_b200.so`` in-tree for sm_100a.
 
 Each translation unit is compiled by nvcc with
-``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3``; the FP64 unit
-(``prec_f64.cu``) additionally with ``-fmad=false`` so that its arithmetic
+``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3``; the FP64 units
+(``prec_f64.cu``, ``oct_f64.cu``) additionally with ``-fmad=false`` so that its arithmetic
 is that of the reference (no fused multiply-add) bit for bit.  The output
 lands in ``cfd_cavity_b200/_build/``.
 """
@@ -32,6 +32,10 @@ UNITS = {
     "prec_bf16sr.cu": [],
     "prec_f16gsr.cu": [],
     "diag_noalloc.cu": [],
+    "octree_api.cu": [],
+    "oct_f64.cu": ["-fmad=false"],
+    "oct_f32.cu": [],
+    "oct_f16.cu": [],
 }
 
 

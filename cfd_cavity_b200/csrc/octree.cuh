@@ -1,0 +1,1402 @@
+// octree.cuh -- the block-refined (octree) cavity of src/octree/ on the GPU.
+//
+// Levels: L0 the full coarse grid; L1 two blocks (hot / cold wall) of
+// (2 w + 3) x (2 (ny0 - 1) + 3) nodes, ghost ring included
+// (OctreeGrid::build, src/octree/grid.rs:103-204); with levels = 3, L2 one
+// strip per L1 block, nested on the L1 grid (src/octree/solver.rs:368-431).
+// One coarse step (step_cavity, src/octree/solver.rs:647-947) is
+//   L0 step; c2f(L0 -> L1); L1 sub-step; [c2f(L1 -> L2); L2 sub-step x 2;
+//   f2c(L2 -> L1) + refresh]; L1 sub-step; f2c(L1 -> L0) + refresh
+// where a (sub-)step is collide -> stream -> thermal BC -> macroscopic (Guo)
+// -> no-slip.  The hot and cold blocks are independent between the two
+// couplings, so every launch covers both (blockIdx.y = block).
+//
+// Each level holds
+//   REF  post-stream populations + rho/u/T (what the reference holds
+//        between its phases; read by the couplings and the diagnostics),
+//   PC   post-collision populations of the level's next collision,
+// both double-buffered.  k_oct_step does pull + BC + macroscopic + no-slip
+// of one (sub-)step, writes REF, then runs the level's NEXT collision and
+// writes PC (the reference order rotated by one phase, as in the uniform
+// solver).  The ghost ring of an L1/L2 level is never collided: interior
+// nodes pull it from REF.  f2c injects into the coarser level's REF,
+// refreshes its moments and runs that node's next collision, so the
+// coarser level's PC stays consistent.
+//
+// Storage: OctImpl<StC, StF> keeps L0 in StC and L1/L2 in StF; A is the
+// arithmetic type of both.  FP64 (double, double) reproduces the FP64 oracle
+// bit for bit (translation unit built without FMA contraction); the shifted
+// formats keep f - w_i and, in the moment planes, rho - 1.
+#pragma once
+
+#include "solver.cuh"
+
+namespace cav {
+namespace oct {
+
+constexpr int OT = 128;          // threads per CTA, node kernels
+constexpr int OCT_GRAPH_STEPS = 16;  // even: a replay leaves every buffer parity unchanged
+constexpr int OSTAT = 6;         // per-CTA statistics: min rho, max rho, max |u|, nonfinite, sum (d)rho, unused
+constexpr int OSTAT_CTAS = 64;
+constexpr double T_HOT_C = 0.5, T_COLD_C = -0.5;
+
+// Collision constants of one level for one coarse step: RelaxTimes::from_nu_alpha
+// (src/octree/lbm.rs:90-98) and the coefficients of collide_node_cavity
+// (src/octree/cavity.rs:100-121), evaluated on the host in FP64.
+template <class A>
+struct LvlScal {
+    A a_f, b_f, a_g, c_m, c_p;           // reference (FP64) form
+    A om_p, om_m, om_g, k_p, k_m;        // pairwise (FP32) form
+    A beta;
+};
+template <class A>
+struct OctScal {
+    LvlScal<A> l[3];
+};
+
+// Rescaling factors (rescaling_factors_multilevel, src/octree/interface.rs:112-131).
+template <class A>
+struct Xi {
+    A even, odd, th;
+    A inv_even, inv_odd, inv_th;
+};
+
+// One level (or one block of a level) as the kernels see it.
+template <class St>
+struct LvlIO {
+    using A = typename Fmt<St>::A;
+    const St* ref_in;
+    St* ref_out;
+    const St* pc_in;
+    St* pc_out;
+    A* mac;   // 4 planes: rho (rho - 1 when shifted), ux, uy, T
+    A* fy;    // Guo force of the last collision (0 on ghosts)
+    int nx, ny;
+    int n;    // nx * ny (plane stride)
+    int hot, cold;
+    int node_off;  // offset of this level's nodes in the rounding streams
+};
+template <class St>
+struct LvlPair {
+    LvlIO<St> b[2];
+};
+
+template <class A>
+struct GhostE {
+    int kf;
+    int kc[4];
+    A w[4];
+};
+struct CoinE {
+    int kc;  // node on the coarser grid
+    int a, b;  // centre of the 3x3 stencil on the finer grid
+};
+
+template <class A>
+__device__ __forceinline__ const OctScal<A>& row_of(const OctScal<A>* tab, int S, const long long* step_dev, int off,
+                                                    long long* s_out) {
+    const long long s = *step_dev + off;
+    *s_out = s;
+    return tab[s < S ? s : S];
+}
+
+// ---------------------------------------------------------------------------
+// Collision of one node (collide_node_cavity, src/octree/cavity.rs:70-150,
+// nu_t = 0): TRT + Guo forcing for f, BGK for g.
+// ---------------------------------------------------------------------------
+template <class A, bool SHIFT>
+__device__ __forceinline__ void oct_collide(A (&f)[Q], A (&g)[Q], const Macro<A, SHIFT>& m, const LvlScal<A>& c,
+                                            A& fy_out) {
+    if constexpr (!SHIFT) {
+        const double r = m.rho, u = m.ux, v = m.uy, temp = m.t;
+        const double fyv = r * c.beta * 1.0 * (temp - 0.0);
+        fy_out = fyv;
+        double d_f[Q], d_g[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            d_f[i] = f[i] - feq_full<double>(i, r, u, v);
+            d_g[i] = g[i] - geq_full<double>(i, temp, u, v, 2);
+        }
+        double fo[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const double cx = CX(i), cy = CY(i);
+            const double ei_u = cx * u + cy * v;
+            const double s_i = WD(i) * ((cy - v) / CS2 + ei_u * cy / (CS2 * CS2)) * fyv;
+            const double s_minus = WD(i) * (cy / CS2) * fyv;
+            const double s_plus = s_i - s_minus;
+            fo[i] = f[i] + (-c.a_f * d_f[i] - c.b_f * d_f[OPP(i)] + c.c_m * s_minus + c.c_p * s_plus);
+        }
+#pragma unroll
+        for (int i = 0; i < Q; ++i) f[i] = fo[i];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) g[i] = g[i] + (-c.a_g * d_g[i] - 0.0 * d_g[OPP(i)]);
+    } else {
+        // Pairwise (i, opp(i)) TRT on h_i = f_i - w_i, as in the uniform FP32
+        // collision, with the level's fixed relaxation rates.
+        const float r = m.rho, u = m.ux, v = m.uy, temp = m.t;
+        const float fyv = r * c.beta * temp;
+        fy_out = fyv;
+        const float u2 = u * u + v * v;
+        const float om_p = c.om_p, om_m = c.om_m, k_p = c.k_p, k_m = c.k_m;
+        const float feq0 = float(WD(0)) * (m.drho - 1.5f * r * u2);
+        const float d0 = f[0] - feq0;
+        f[0] = f[0] - om_p * d0 + k_p * float(WD(0)) * (-3.0f * v) * fyv;
+#pragma unroll
+        for (int p = 1; p <= 4; ++p) {
+            const float cx = CX(p), cy = CY(p);
+            const float eu = cx * u + cy * v;
+            const float feS = float(WD(p)) * (m.drho + r * (4.5f * eu * eu - 1.5f * u2));
+            const float feA = float(WD(p)) * (r * 3.0f * eu);
+            const float dS = (f[p] + f[p + 4]) - 2.0f * feS;
+            const float dD = (f[p] - f[p + 4]) - 2.0f * feA;
+            const float E = -0.5f * om_p * dS + k_p * float(WD(p)) * (-3.0f * v + 9.0f * eu * cy) * fyv;
+            const float O = -0.5f * om_m * dD + k_m * float(WD(p)) * (3.0f * cy) * fyv;
+            f[p] = f[p] + (E + O);
+            f[p + 4] = f[p + 4] + (E - O);
+        }
+        const float om_g = c.om_g, one_m = 1.0f - om_g;
+        g[0] = one_m * g[0] + om_g * float(WD(0)) * temp * (1.0f - 1.5f * u2);
+#pragma unroll
+        for (int p = 1; p <= 4; ++p) {
+            const float cx = CX(p), cy = CY(p);
+            const float eu = cx * u + cy * v;
+            const float gS = om_g * float(WD(p)) * temp * (1.0f + (4.5f * eu * eu - 1.5f * u2));
+            const float gA = om_g * float(WD(p)) * temp * (3.0f * eu);
+            g[p] = one_m * g[p] + (gS + gA);
+            g[p + 4] = one_m * g[p + 4] + (gS - gA);
+        }
+    }
+}
+
+// f_i^eq in the storage convention (f - w_i when shifted) from the stored moments.
+template <class A, bool SHIFT>
+__device__ __forceinline__ A feq_st(int i, A rho0, A ux, A uy) {
+    if constexpr (SHIFT) {
+        const A drho = rho0, r = A(1.0) + rho0;
+        const A eu = A(CX(i)) * ux + A(CY(i)) * uy;
+        const A u2 = ux * ux + uy * uy;
+        return A(WD(i)) * (drho + r * (A(3.0) * eu + A(4.5) * eu * eu - A(1.5) * u2));
+    } else {
+        return feq_full<A>(i, rho0, ux, uy);
+    }
+}
+
+template <class St>
+__device__ __forceinline__ void store_pops(St* __restrict__ dst, int n, int k, const typename Fmt<St>::A (&f)[Q],
+                                          const typename Fmt<St>::A (&g)[Q], bool sr, uint32_t seed, long long key,
+                                          long long node) {
+    if constexpr (Fmt<St>::SR) {
+        if (sr) {
+            NodeRng rng(seed, key, node);
+            uint32_t r = 0;
+#pragma unroll
+            for (int q = 0; q < NPLANES; ++q) {
+                if ((q & 1) == 0) r = rng.next();
+                const uint32_t bits = (q & 1) == 0 ? (r & 0xffff0000u) : (r << 16);
+                dst[q * n + k] = Fmt<St>::store_sr(q < Q ? f[q] : g[q - Q], q, bits);
+            }
+            return;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < NPLANES; ++q) dst[q * n + k] = Fmt<St>::store(q < Q ? f[q] : g[q - Q], q, RN_BITS);
+}
+
+template <class St>
+__device__ __forceinline__ void load_pops(const St* __restrict__ src, int n, int k, typename Fmt<St>::A (&f)[Q],
+                                          typename Fmt<St>::A (&g)[Q]) {
+#pragma unroll
+    for (int i = 0; i < Q; ++i) f[i] = Fmt<St>::load(src[i * n + k], i);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) g[i] = Fmt<St>::load(src[(Q + i) * n + k], Q + i);
+}
+
+// ---------------------------------------------------------------------------
+// Streaming sources.  L0 (stream, src/octree/lbm.rs:152-180): pull inside
+// the grid, bounce-back (f) / keep (g) outside.  L1/L2 blocks
+// (stream_cavity_block, src/octree/cavity.rs:393-495, wall_bottom =
+// wall_top = true): interior nodes only; a source in a wall-side ghost line
+// bounces back, a source in an interface ghost column is pulled from REF
+// (the injected value), any other source from PC.
+// ---------------------------------------------------------------------------
+template <class St, bool COARSE>
+__device__ __forceinline__ typename Fmt<St>::A pull_one(const LvlIO<St>& L, int x, int y, int q_plane, int i) {
+    // Branch-free: the source index, plane and buffer are selected, so the
+    // 9 (18) loads of a node are all in flight together.
+    const int sx = x - CX(i), sy = y - CY(i);
+    const int k = y * L.nx + x;
+    bool bb;
+    const St* base = L.pc_in;
+    if constexpr (COARSE) {
+        bb = sx < 0 || sx >= L.nx || sy < 0 || sy >= L.ny;
+    } else {
+        bb = (sx == 0 && L.hot) || (sx == L.nx - 1 && L.cold) || sy == 0 || sy == L.ny - 1;
+        const bool ghost = !bb && (sx == 0 || sx == L.nx - 1);
+        base = ghost ? L.ref_in : L.pc_in;
+    }
+    const int qs = (bb && q_plane < Q) ? OPP(i) : q_plane;
+    const int ks = bb ? k : sy * L.nx + sx;
+    return Fmt<St>::load(base[qs * L.n + ks], qs);
+}
+
+// Post-boundary-condition g of node (x, y).  L0
+// (apply_thermal_boundary_conditions, src/octree/cavity.rs:501-534): wall
+// columns geq(T_w, 0, 0), rows 0 / ny-1 copy rows 1 / ny-2.  Blocks
+// (apply_thermal_boundary_conditions_block, :543-605): wall column 1 / nx-2
+// geq(T_w); rows 1 / ny-2 copy rows 2 / ny-3 (columns 1..nx-2); ghost
+// columns copy columns 1 / nx-2; ghost rows copy rows 1 / ny-2.  Resolving
+// the copy chain: g(x, y) is the post-stream g of (x', y'') with x' the
+// column clamped to 1..nx-2 and y'' the row clamped to 2..ny-3, or the wall
+// equilibrium when x' is a wall column.
+template <class St, bool COARSE>
+__device__ __forceinline__ void bc_g(const LvlIO<St>& L, int x, int y, typename Fmt<St>::A (&g)[Q]) {
+    using A = typename Fmt<St>::A;
+    int xs, ys;
+    bool wall;
+    A tw;
+    if constexpr (COARSE) {
+        wall = x == 0 || x == L.nx - 1;
+        tw = x == 0 ? A(T_HOT_C) : A(T_COLD_C);
+        xs = x;
+        ys = y < 1 ? 1 : (y > L.ny - 2 ? L.ny - 2 : y);
+    } else {
+        xs = x < 1 ? 1 : (x > L.nx - 2 ? L.nx - 2 : x);
+        const int y1 = y < 1 ? 1 : (y > L.ny - 2 ? L.ny - 2 : y);
+        ys = y1 == 1 ? 2 : (y1 == L.ny - 2 ? L.ny - 3 : y1);
+        wall = (L.hot && xs == 1) || (L.cold && xs == L.nx - 2);
+        tw = (L.hot && xs == 1) ? A(T_HOT_C) : A(T_COLD_C);
+    }
+    if (wall) {
+#pragma unroll
+        for (int i = 0; i < Q; ++i) g[i] = geq_full<A>(i, tw, A(0.0), A(0.0), 2);
+    } else {
+#pragma unroll
+        for (int i = 0; i < Q; ++i) g[i] = pull_one<St, COARSE>(L, xs, ys, Q + i, i);
+    }
+}
+
+// One (sub-)step of a level: pull + BC + macroscopic (update_macroscopic_guo,
+// src/octree/cavity.rs:252-325) + no-slip (enforce_wall_velocity[_block],
+// :609-656) -> REF; then the level's next collision -> PC.
+template <class St, bool COARSE>
+__global__ void __launch_bounds__(OT) k_oct_step(LvlPair<St> P, const OctScal<typename Fmt<St>::A>* __restrict__ tab,
+                                                 int S, const long long* __restrict__ step_dev, int off, int lvl,
+                                                 uint32_t seed, int phase) {
+    using A = typename Fmt<St>::A;
+    constexpr bool SH = Fmt<St>::SHIFT;
+    const LvlIO<St>& L = P.b[blockIdx.y];
+    const int k = blockIdx.x * OT + threadIdx.x;
+    if (k >= L.n) return;
+    // the step index and the collision constants first: the stores below
+    // may alias them as far as the compiler knows
+    long long s;
+    const LvlScal<A> sc = row_of<A>(tab, S, step_dev, off, &s).l[lvl];
+    const int x = k % L.nx, y = k / L.nx;
+    const bool ghost = !COARSE && (x == 0 || x == L.nx - 1 || y == 0 || y == L.ny - 1);
+    A f[Q], g[Q];
+    if (ghost) {
+#pragma unroll
+        for (int i = 0; i < Q; ++i) f[i] = Fmt<St>::load(L.ref_in[i * L.n + k], i);
+    } else {
+#pragma unroll
+        for (int i = 0; i < Q; ++i) f[i] = pull_one<St, COARSE>(L, x, y, i, i);
+    }
+    bc_g<St, COARSE>(L, x, y, g);
+    bool wall;
+    if constexpr (COARSE)
+        wall = x == 0 || x == L.nx - 1 || y == 0 || y == L.ny - 1;
+    else
+        wall = (L.hot && x == 1) || (L.cold && x == L.nx - 2) || y == 1 || y == L.ny - 2;
+    const A fy_prev = L.fy[k];
+    const Macro<A, SH> m = macro_node<A, SH>(f, g, fy_prev, wall);
+    store_pops<St>(L.ref_out, L.n, k, f, g, false, 0, 0, 0);
+    L.mac[k] = SH ? m.drho : m.rho;
+    L.mac[L.n + k] = m.ux;
+    L.mac[2 * L.n + k] = m.uy;
+    L.mac[3 * L.n + k] = m.t;
+    if (ghost) return;
+    A fy_new;
+    oct_collide<A, SH>(f, g, m, sc, fy_new);
+    L.fy[k] = fy_new;
+    store_pops<St>(L.pc_out, L.n, k, f, g, true, seed, s * 16 + phase, (long long)L.node_off + k);
+}
+
+// Collision of the REF state into PC (the first collision after the state
+// was set from the host).
+template <class St, bool COARSE>
+__global__ void __launch_bounds__(OT) k_oct_collide(LvlPair<St> P, const OctScal<typename Fmt<St>::A>* __restrict__ tab,
+                                                    int S, const long long* __restrict__ step_dev, int lvl,
+                                                    uint32_t seed, int phase) {
+    using A = typename Fmt<St>::A;
+    constexpr bool SH = Fmt<St>::SHIFT;
+    const LvlIO<St>& L = P.b[blockIdx.y];
+    const int k = blockIdx.x * OT + threadIdx.x;
+    if (k >= L.n) return;
+    const int x = k % L.nx, y = k / L.nx;
+    if (!COARSE && (x == 0 || x == L.nx - 1 || y == 0 || y == L.ny - 1)) return;
+    long long s;
+    const LvlScal<A> sc = row_of<A>(tab, S, step_dev, 0, &s).l[lvl];
+    A f[Q], g[Q];
+    load_pops<St>(L.ref_in, L.n, k, f, g);
+    Macro<A, SH> m;
+    const A r0 = L.mac[k];
+    m.rho = SH ? A(1.0) + r0 : r0;
+    m.drho = SH ? r0 : r0 - A(1.0);
+    m.ux = L.mac[L.n + k];
+    m.uy = L.mac[2 * L.n + k];
+    m.t = L.mac[3 * L.n + k];
+    m.inv_rho = A(1.0) / m.rho;
+    A fy_new;
+    oct_collide<A, SH>(f, g, m, sc, fy_new);
+    L.fy[k] = fy_new;
+    store_pops<St>(L.pc_out, L.n, k, f, g, true, seed, s * 16 + phase, (long long)L.node_off + k);
+}
+
+// Moments of a node whose populations were just injected
+// (refresh_moments, src/octree/interface.rs:209-227, unguarded, and
+// refresh_moments_nodes, src/octree/solver.rs:1183-1206, guarded).
+template <class A, bool SHIFT, bool GUARD>
+__device__ __forceinline__ Macro<A, SHIFT> refresh(const A (&f)[Q], const A (&g)[Q]) {
+    Macro<A, SHIFT> m;
+    A rho = A(0.0), mx = A(0.0), my = A(0.0), t = A(0.0);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        rho = rho + f[i];
+        mx = mx + f[i] * A(CX(i));
+        my = my + f[i] * A(CY(i));
+        t = t + g[i];
+    }
+    if (SHIFT) {
+        m.drho = rho;
+        m.rho = A(1.0) + rho;
+    } else {
+        m.rho = rho;
+        m.drho = rho - A(1.0);
+    }
+    m.t = t;
+    if (GUARD && !(m.rho > A(2.220446049250313e-16))) {
+        m.ux = A(0.0);
+        m.uy = A(0.0);
+    } else {
+        m.ux = mx / m.rho;
+        m.uy = my / m.rho;
+    }
+    m.inv_rho = A(1.0) / m.rho;
+    return m;
+}
+
+// even/odd split of f^neq and its rescaling (split_odd_even, rescale_fneq,
+// rescale_fneq_inverse, src/octree/interface.rs:68-102).
+template <class A, bool SHIFT, bool INVERSE>
+__device__ __forceinline__ void rescale(const A (&fn)[Q], const Xi<A>& xi, A (&out)[Q]) {
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const A even = A(0.5) * (fn[i] + fn[OPP(i)]);
+        const A odd = A(0.5) * (fn[i] - fn[OPP(i)]);
+        if constexpr (!INVERSE)
+            out[i] = xi.even * even + xi.odd * odd;
+        else if constexpr (SHIFT)
+            out[i] = even * xi.inv_even + odd * xi.inv_odd;
+        else
+            out[i] = even / xi.even + odd / xi.odd;
+    }
+}
+
+// Weighted contribution of one stencil node to a coupling: c[0..3] = w *
+// (rho, ux, uy, T), c[4..12] = w * f^neq_i, c[13..21] = w * g^neq_i.
+constexpr int NC = 22;
+template <class St>
+__device__ __forceinline__ void stencil_term(const LvlIO<St>& L, int k, typename Fmt<St>::A w,
+                                             typename Fmt<St>::A (&c)[NC]) {
+    using A = typename Fmt<St>::A;
+    constexpr bool SH = Fmt<St>::SHIFT;
+    const A r0 = L.mac[k], u = L.mac[L.n + k], v = L.mac[2 * L.n + k], t = L.mac[3 * L.n + k];
+    A f[Q], g[Q];
+    load_pops<St>(L.ref_out, L.n, k, f, g);
+    c[0] = w * r0;
+    c[1] = w * u;
+    c[2] = w * v;
+    c[3] = w * t;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        c[4 + i] = w * (f[i] - feq_st<A, SH>(i, r0, u, v));
+        c[13 + i] = w * (g[i] - geq_full<A>(i, t, u, v, 2));
+    }
+}
+
+// Sum of the group's contributions in lane order (the reference's stencil
+// order, so that FP64 sums are bit-identical); every lane gets the sums.
+template <class A, int GW, int NS>
+__device__ __forceinline__ void group_sum(A (&c)[NC]) {
+    const int base = (threadIdx.x & 31) & ~(GW - 1);
+#pragma unroll
+    for (int m = 0; m < NC; ++m) {
+        A acc = __shfl_sync(0xffffffffu, c[m], base);
+#pragma unroll
+        for (int j = 1; j < NS; ++j) acc = acc + __shfl_sync(0xffffffffu, c[m], base + j);
+        c[m] = acc;
+    }
+}
+
+// coarse_to_fine (src/octree/interface.rs:137-170): every ghost node of the
+// finer level gets the bilinear moments of the coarser level plus the
+// interpolated, rescaled non-equilibrium parts; then its moments are
+// refreshed from the injected populations.  Four lanes per ghost, one per
+// stencil node.
+template <class StC, class StF>
+__global__ void __launch_bounds__(OT) k_oct_c2f(LvlPair<StC> C, LvlPair<StF> F,
+                                                const GhostE<typename Fmt<StF>::A>* __restrict__ tab, int n_ghost,
+                                                Xi<typename Fmt<StF>::A> xi, const long long* __restrict__ step_dev,
+                                                uint32_t seed, int phase) {
+    using A = typename Fmt<StF>::A;
+    constexpr bool SH = Fmt<StF>::SHIFT;
+    static_assert(Fmt<StC>::SHIFT == SH, "levels share one convention");
+    const int t = blockIdx.x * OT + threadIdx.x;
+    const int j = t >> 2, s = t & 3;
+    if ((t & ~31) >= 4 * n_ghost) return;  // whole warp past the end
+    const bool act = j < n_ghost;
+    const LvlIO<StC>& Lc = C.b[blockIdx.y];
+    const LvlIO<StF>& Lf = F.b[blockIdx.y];
+    const long long key = *step_dev * 16 + phase;
+    A c[NC];
+    int kf = 0;
+    if (act) {
+        const GhostE<A>& e = tab[blockIdx.y * n_ghost + j];
+        kf = e.kf;
+        stencil_term<StC>(Lc, e.kc[s], e.w[s], c);
+    } else {
+#pragma unroll
+        for (int m = 0; m < NC; ++m) c[m] = A(0.0);
+    }
+    group_sum<A, 4, 4>(c);
+    if (!act || s != 0) return;
+    const A rho = c[0], ux = c[1], uy = c[2], tt = c[3];
+    A fn[Q], fr[Q], f[Q], g[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) fn[i] = c[4 + i];
+    rescale<A, SH, false>(fn, xi, fr);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        f[i] = feq_st<A, SH>(i, rho, ux, uy) + fr[i];
+        g[i] = geq_full<A>(i, tt, ux, uy, 2) + xi.th * c[13 + i];
+    }
+    store_pops<StF>(Lf.ref_out, Lf.n, kf, f, g, true, seed, key, (long long)Lf.node_off + kf);
+    if constexpr (!std::is_same<StF, A>::value) load_pops<StF>(Lf.ref_out, Lf.n, kf, f, g);
+    const Macro<A, SH> m = refresh<A, SH, false>(f, g);
+    Lf.mac[kf] = SH ? m.drho : m.rho;
+    Lf.mac[Lf.n + kf] = m.ux;
+    Lf.mac[2 * Lf.n + kf] = m.uy;
+    Lf.mac[3 * Lf.n + kf] = m.t;
+}
+
+// fine_to_coarse (src/octree/interface.rs:175-206) + refresh of the
+// coincident node (src/octree/solver.rs:874-876, 936-942) + that node's next
+// collision into the coarser level's PC.  Sixteen lanes per coincident node,
+// nine of them on the 3 x 3 stencil.
+template <class StF, class StC>
+__global__ void __launch_bounds__(OT) k_oct_f2c(LvlPair<StF> F, LvlPair<StC> C, const CoinE* __restrict__ tab, int n0,
+                                                int n1, Xi<typename Fmt<StF>::A> xi,
+                                                const OctScal<typename Fmt<StF>::A>* __restrict__ stab, int S,
+                                                const long long* __restrict__ step_dev, int off, int lvl_c,
+                                                uint32_t seed, int phase) {
+    using A = typename Fmt<StF>::A;
+    constexpr bool SH = Fmt<StF>::SHIFT;
+    const int t = blockIdx.x * OT + threadIdx.x;
+    const int j = t >> 4, s = t & 15;
+    const int blk = blockIdx.y;
+    const int nb = blk == 0 ? n0 : n1;
+    if ((t & ~31) >= 16 * nb) return;  // whole warp past the end
+    const bool act_e = j < nb;
+    const LvlIO<StF>& Lf = F.b[blk];
+    const LvlIO<StC>& Lc = C.b[blk];
+    CoinE e{0, 0, 0};
+    if (act_e) e = tab[(blk == 0 ? 0 : n0) + j];
+    long long sidx;
+    const LvlScal<A> sc = row_of<A>(stab, S, step_dev, off, &sidx).l[lvl_c];
+    A c[NC];
+    if (act_e && s < 9) {
+        const int jb = s / 3, ja = s - 3 * jb;
+        const A ww[3] = {A(0.25), A(0.5), A(0.25)};
+        const int kf = (e.b + jb - 1) * Lf.nx + (e.a + ja - 1);
+        stencil_term<StF>(Lf, kf, ww[ja] * ww[jb], c);
+    } else {
+#pragma unroll
+        for (int m = 0; m < NC; ++m) c[m] = A(0.0);
+    }
+    group_sum<A, 16, 9>(c);
+    if (!act_e || s != 0) return;
+    const A rho = c[0], ux = c[1], uy = c[2], tt = c[3];
+    A fn[Q], fr[Q], f[Q], g[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) fn[i] = c[4 + i];
+    rescale<A, SH, true>(fn, xi, fr);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        f[i] = feq_st<A, SH>(i, rho, ux, uy) + fr[i];
+        if constexpr (SH)
+            g[i] = geq_full<A>(i, tt, ux, uy, 2) + c[13 + i] * xi.inv_th;
+        else
+            g[i] = geq_full<A>(i, tt, ux, uy, 2) + c[13 + i] / xi.th;
+    }
+    store_pops<StC>(Lc.ref_out, Lc.n, e.kc, f, g, true, seed, sidx * 16 + phase, (long long)Lc.node_off + e.kc);
+    if constexpr (!std::is_same<StC, A>::value) load_pops<StC>(Lc.ref_out, Lc.n, e.kc, f, g);
+    const Macro<A, SH> m = refresh<A, SH, true>(f, g);
+    Lc.mac[e.kc] = SH ? m.drho : m.rho;
+    Lc.mac[Lc.n + e.kc] = m.ux;
+    Lc.mac[2 * Lc.n + e.kc] = m.uy;
+    Lc.mac[3 * Lc.n + e.kc] = m.t;
+    A fy_new;
+    oct_collide<A, SH>(f, g, m, sc, fy_new);
+    Lc.fy[e.kc] = fy_new;
+    store_pops<StC>(Lc.pc_out, Lc.n, e.kc, f, g, true, seed, sidx * 16 + phase + 1, (long long)Lc.node_off + e.kc);
+}
+
+// ---------------------------------------------------------------------------
+// Diagnostics (FP64, deterministic: fixed CTA partition, sequential final sums).
+// ---------------------------------------------------------------------------
+template <class A>
+struct StatView {
+    const A* mac;
+    int n;
+};
+template <class A>
+struct StatViews {
+    StatView<A> v[5];
+};
+
+// Per CTA of view blockIdx.y: min / max of rho, max max(|ux|, |uy|) (max_u,
+// src/octree/cavity.rs:743-748), count of non-finite moments
+// (check_finite_levels, :751-789), sum of the rho plane.
+template <class A, bool SHIFT>
+__global__ void __launch_bounds__(256) k_oct_stats(StatViews<A> V, double* __restrict__ part) {
+    const StatView<A> W = V.v[blockIdx.y];
+    double mn = 1e300, mx = -1e300, mu = 0.0, nf = 0.0, sm = 0.0;
+    for (int k = blockIdx.x * 256 + threadIdx.x; k < W.n; k += gridDim.x * 256) {
+        const double r0 = double(W.mac[k]);
+        const double r = SHIFT ? 1.0 + r0 : r0;
+        const double u = double(W.mac[W.n + k]), v = double(W.mac[2 * W.n + k]), t = double(W.mac[3 * W.n + k]);
+        mn = fmin(mn, r);
+        mx = fmax(mx, r);
+        mu = fmax(mu, fmax(fabs(u), fabs(v)));
+        if (!(isfinite(r) && isfinite(u) && isfinite(v) && isfinite(t))) nf += 1.0;
+        sm += r0;
+    }
+    __shared__ double sh[OSTAT][256];
+    sh[0][threadIdx.x] = mn;
+    sh[1][threadIdx.x] = mx;
+    sh[2][threadIdx.x] = mu;
+    sh[3][threadIdx.x] = nf;
+    sh[4][threadIdx.x] = sm;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            const int o = threadIdx.x + h;
+            sh[0][threadIdx.x] = fmin(sh[0][threadIdx.x], sh[0][o]);
+            sh[1][threadIdx.x] = fmax(sh[1][threadIdx.x], sh[1][o]);
+            sh[2][threadIdx.x] = fmax(sh[2][threadIdx.x], sh[2][o]);
+            sh[3][threadIdx.x] += sh[3][o];
+            sh[4][threadIdx.x] += sh[4][o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double* p = part + (size_t(blockIdx.y) * gridDim.x + blockIdx.x) * OSTAT;
+        for (int q = 0; q < 5; ++q) p[q] = sh[q][0];
+        p[5] = 0.0;
+    }
+}
+
+// min / max of rho over the interface nodes (noise_stats, src/octree/
+// solver.rs:954-1003): ghosts of each finer level and coincident nodes of
+// each coarser level.  One CTA per (list, block).
+template <class A, bool SHIFT>
+__global__ void __launch_bounds__(256) k_oct_iface(const A* mac_f0, const A* mac_f1, const A* mac_c0, const A* mac_c1,
+                                                   const GhostE<A>* __restrict__ gh, int n_ghost,
+                                                   const CoinE* __restrict__ co, int n0, int n1,
+                                                   double* __restrict__ out) {
+    const int blk = blockIdx.x;
+    const A* mf = blk == 0 ? mac_f0 : mac_f1;
+    const A* mc = blk == 0 ? mac_c0 : mac_c1;
+    double mn = 1e300, mx = -1e300;
+    for (int j = threadIdx.x; j < n_ghost; j += 256) {
+        const double r0 = double(mf[gh[blk * n_ghost + j].kf]);
+        const double r = SHIFT ? 1.0 + r0 : r0;
+        mn = fmin(mn, r);
+        mx = fmax(mx, r);
+    }
+    const int nc = blk == 0 ? n0 : n1;
+    const CoinE* cb = co + (blk == 0 ? 0 : n0);
+    for (int j = threadIdx.x; j < nc; j += 256) {
+        const double r0 = double(mc[cb[j].kc]);
+        const double r = SHIFT ? 1.0 + r0 : r0;
+        mn = fmin(mn, r);
+        mx = fmax(mx, r);
+    }
+    __shared__ double s0[256], s1[256];
+    s0[threadIdx.x] = mn;
+    s1[threadIdx.x] = mx;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            s0[threadIdx.x] = fmin(s0[threadIdx.x], s0[threadIdx.x + h]);
+            s1[threadIdx.x] = fmax(s1[threadIdx.x], s1[threadIdx.x + h]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[2 * blk] = s0[0];
+        out[2 * blk + 1] = s1[0];
+    }
+}
+
+// Final reduction.  out: nu_hot, nu_hot_link0, nu_cold (nusselt_hot /
+// nusselt_hot_link0 / nusselt_cold, src/octree/cavity.rs:672-715, Lx
+// scale), nu_hot_fine (:728-741), max_u, mass (mean coarse rho), max_rho_dev,
+// max_rho_dev_ifaces, finite, y_plus (post.rs:182-199 formula on the finest
+// hot-wall level: wall column 1, first fluid column 2, rows 2..ny-3).
+template <class A, bool SHIFT>
+__global__ void k_oct_final(const A* __restrict__ mac0, int nx0, int ny0, const A* __restrict__ mac_h1, int nx1,
+                            int ny1, const A* __restrict__ mac_fin, int nxf, int nyf, double nu_fin,
+                            const double* __restrict__ part, int n_views, int n_ctas,
+                            const double* __restrict__ iface, int n_iface, double* __restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int n0 = nx0 * ny0;
+    const A* T0 = mac0 + 3 * (size_t)n0;
+    double sh = 0.0, s0 = 0.0, sc = 0.0;
+    for (int iy = 0; iy < ny0; ++iy) {
+        const double t0 = T0[iy * nx0], t1 = T0[iy * nx0 + 1], t2 = T0[iy * nx0 + 2];
+        const double tc2 = T0[iy * nx0 + nx0 - 2], tc3 = T0[iy * nx0 + nx0 - 3];
+        sh += fabs(t1 - t2);
+        s0 += fabs(t1 - t0);
+        sc += fabs(tc2 - tc3);
+    }
+    const double lx = double(nx0 - 1);
+    out[0] = sh / double(ny0) * lx / 1.0;
+    out[1] = s0 / double(ny0) * lx / 1.0;
+    out[2] = sc / double(ny0) * lx / 1.0;
+    const A* T1 = mac_h1 + 3 * (size_t)nx1 * ny1;
+    double sf = 0.0;
+    for (int b = 1; b < ny1 - 1; ++b) sf += fabs(double(T1[b * nx1 + 1]) - double(T1[b * nx1 + 2])) * 2.0;
+    out[3] = sf / double(ny1 - 2) * lx / 1.0;
+    double mn = 1e300, mx = -1e300, mu = 0.0, nf = 0.0, sum0 = 0.0;
+    for (int v = 0; v < n_views; ++v)
+        for (int c = 0; c < n_ctas; ++c) {
+            const double* p = part + (size_t(v) * n_ctas + c) * OSTAT;
+            mn = fmin(mn, p[0]);
+            mx = fmax(mx, p[1]);
+            mu = fmax(mu, p[2]);
+            nf += p[3];
+            if (v == 0) sum0 += p[4];
+        }
+    out[4] = mu;
+    const double rb = SHIFT ? 1.0 + sum0 / double(n0) : sum0 / double(n0);
+    out[5] = rb;
+    out[6] = fmax(mx - rb, rb - mn);
+    double imn = 1e300, imx = -1e300;
+    for (int j = 0; j < n_iface; ++j) {
+        imn = fmin(imn, iface[2 * j]);
+        imx = fmax(imx, iface[2 * j + 1]);
+    }
+    out[7] = fmax(imx - rb, rb - imn);
+    out[8] = nf == 0.0 ? 1.0 : 0.0;
+    const A* Uy = mac_fin + 2 * (size_t)nxf * nyf;
+    double sy = 0.0;
+    for (int b = 2; b < nyf - 2; ++b) {
+        const double tw = nu_fin * fabs(double(Uy[b * nxf + 2]) - double(Uy[b * nxf + 1]));
+        sy += 0.5 * sqrt(fmax(tw, 0.0)) / nu_fin;
+    }
+    out[9] = sy / double(nyf - 4);
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+// ---------------------------------------------------------------------------
+
+// The octree behind cav_octree_*; OctImpl<StC, StF> holds the buffers.
+struct Octree {
+    virtual ~Octree() = default;
+    virtual void setup(const cav_octree_params& p) = 0;
+    virtual void step(int64_t n) = 0;
+    virtual void get_level(int lvl, double* rho, double* ux, double* uy, double* t, double* f, double* g) = 0;
+    virtual void set_level(int lvl, const double* rho, const double* ux, const double* uy, const double* t,
+                           const double* f, const double* g) = 0;
+    virtual void diag(double* out10) = 0;
+    virtual void debug_phase(int phase) = 0;
+    virtual void sync() = 0;
+
+    cav_octree_params p{};
+    int levels = 2, nx0 = 0, ny0 = 0, nx1 = 0, ny1 = 0, nx2 = 0, ny2 = 0;
+    double nu = 0, alpha = 0, beta_c = 0, nu_start_mult = 1.0;
+    double tau_p[3] = {0, 0, 0};
+    double xiA[3] = {0, 0, 0}, xiB[3] = {0, 0, 0};
+    int64_t time_step = 0, spin_up = 0;
+    int n_ghost = 0, n_co0 = 0, n_co1 = 0, n_ghost2 = 0, n_co2_0 = 0, n_co2_1 = 0;
+    cudaStream_t stream = nullptr;
+    int64_t launches = 0;
+    std::string err;
+};
+
+// Host restatement of the grid tables (OctreeGrid::build, grid.rs:103-204,
+// bilinear_stencil :218-229), in FP64.
+struct HostGrid {
+    int nx0, ny0, bx0, by0, bx1, by1, nx1, ny1;
+    struct G {
+        int kf;
+        int kc[4];
+        double w[4];
+    };
+    std::vector<G> ghosts;
+    std::vector<CoinE> coin;
+    static void bilinear(double x, double y, int nx0, int ny0, int kc[4], double w[4]) {
+        long ix = (long)std::floor(x), iy = (long)std::floor(y);
+        ix = std::min<long>(std::max<long>(ix, 0), nx0 - 2);
+        iy = std::min<long>(std::max<long>(iy, 0), ny0 - 2);
+        const double fx = x - double(ix), fy = y - double(iy);
+        kc[0] = int(iy * nx0 + ix);
+        w[0] = (1.0 - fx) * (1.0 - fy);
+        kc[1] = int(iy * nx0 + ix + 1);
+        w[1] = fx * (1.0 - fy);
+        kc[2] = int((iy + 1) * nx0 + ix);
+        w[2] = (1.0 - fx) * fy;
+        kc[3] = int((iy + 1) * nx0 + ix + 1);
+        w[3] = fx * fy;
+    }
+    void build(int nx0_, int ny0_, int bx0_, int by0_, int bx1_, int by1_, bool wl, bool wr, bool wb, bool wt) {
+        nx0 = nx0_;
+        ny0 = ny0_;
+        bx0 = bx0_;
+        by0 = by0_;
+        bx1 = bx1_;
+        by1 = by1_;
+        nx1 = 2 * (bx1 - bx0) + 3;
+        ny1 = 2 * (by1 - by0) + 3;
+        ghosts.clear();
+        coin.clear();
+        for (int b = 0; b < ny1; ++b)
+            for (int a = 0; a < nx1; ++a)
+                if (a == 0 || b == 0 || a == nx1 - 1 || b == ny1 - 1) {
+                    G e;
+                    e.kf = b * nx1 + a;
+                    bilinear(double(bx0) - 0.5 + 0.5 * a, double(by0) - 0.5 + 0.5 * b, nx0, ny0, e.kc, e.w);
+                    ghosts.push_back(e);
+                }
+        for (int cy = by0; cy < by1; ++cy)
+            for (int cx = bx0; cx < bx1; ++cx) {
+                if (cx == 0 || cx + 1 == nx0 || cy == 0 || cy + 1 == ny0) continue;
+                if ((wl && cx == bx0) || (wr && cx + 1 == bx1) || (wb && cy == by0) || (wt && cy + 1 == by1)) continue;
+                coin.push_back(CoinE{cy * nx0 + cx, 2 * (cx - bx0) + 1, 2 * (cy - by0) + 1});
+            }
+    }
+};
+
+template <class StC, class StF>
+struct OctImpl final : Octree {
+    using A = typename Fmt<StC>::A;
+    static_assert(std::is_same<A, typename Fmt<StF>::A>::value, "one arithmetic type");
+    static constexpr bool SH = Fmt<StC>::SHIFT;
+
+    template <class St>
+    struct Lvl {
+        int nx = 0, ny = 0, n = 0;
+        St* ref[2] = {nullptr, nullptr};
+        St* pc[2] = {nullptr, nullptr};
+        A* mac = nullptr;
+        A* fy = nullptr;
+        int hot = 0, cold = 0, node_off = 0;
+        int cur = 0;  // REF and PC buffers flip together
+        LvlIO<St> io() const {
+            LvlIO<St> o;
+            o.ref_in = ref[cur];
+            o.ref_out = ref[cur ^ 1];
+            o.pc_in = pc[cur];
+            o.pc_out = pc[cur ^ 1];
+            o.mac = mac;
+            o.fy = fy;
+            o.nx = nx;
+            o.ny = ny;
+            o.n = n;
+            o.hot = hot;
+            o.cold = cold;
+            o.node_off = node_off;
+            return o;
+        }
+        // The current state: REF and PC written by the last step (the
+        // couplings read and write this one).
+        LvlIO<St> io_cur() const {
+            LvlIO<St> o = io();
+            o.ref_in = ref[cur];
+            o.ref_out = ref[cur];
+            o.pc_in = pc[cur];
+            o.pc_out = pc[cur];
+            return o;
+        }
+    };
+
+    Lvl<StC> L0;
+    Lvl<StF> L1[2], L2[2];
+    GhostE<A>* gh1 = nullptr;
+    GhostE<A>* gh2 = nullptr;
+    CoinE* co1 = nullptr;
+    CoinE* co2 = nullptr;
+    OctScal<A>* tab = nullptr;
+    int S = 0;
+    long long* step_dev = nullptr;
+    long long step_dev_val = -1;
+    double* part = nullptr;
+    double* iface = nullptr;
+    double* dout = nullptr;
+    uint32_t seed32 = 0;
+    bool pc_valid = false;
+    Xi<A> xa{}, xb{};
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    std::vector<void*> allocs;
+
+    ~OctImpl() override {
+        for (auto& gx : graph)
+            if (gx) cudaGraphExecDestroy(gx);
+        for (void* b : allocs) cudaFree(b);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    template <class T>
+    T* dalloc(size_t n) {
+        void* p = nullptr;
+        CK(cudaMalloc(&p, sizeof(T) * std::max<size_t>(n, 1)));
+        allocs.push_back(p);
+        CK(cudaMemsetAsync(p, 0, sizeof(T) * std::max<size_t>(n, 1), stream));
+        return static_cast<T*>(p);
+    }
+
+    template <class St>
+    void alloc_level(Lvl<St>& L, int nx, int ny, int hot, int cold, int node_off) {
+        L.nx = nx;
+        L.ny = ny;
+        L.n = nx * ny;
+        L.hot = hot;
+        L.cold = cold;
+        L.node_off = node_off;
+        for (int b = 0; b < 2; ++b) {
+            L.ref[b] = dalloc<St>(size_t(NPLANES) * L.n);
+            L.pc[b] = dalloc<St>(size_t(NPLANES) * L.n);
+        }
+        L.mac = dalloc<A>(size_t(4) * L.n);
+        L.fy = dalloc<A>(L.n);
+    }
+
+    static Xi<A> make_xi(const double* x) {
+        Xi<A> o;
+        o.even = A(x[0]);
+        o.odd = A(x[1]);
+        o.th = A(x[2]);
+        o.inv_even = A(1.0 / x[0]);
+        o.inv_odd = A(1.0 / x[1]);
+        o.inv_th = A(1.0 / x[2]);
+        return o;
+    }
+
+    // RelaxTimes::from_nu_alpha (lbm.rs:90-98) + collision coefficients.
+    static LvlScal<A> lvl_scal(double nu_l, double al_l, double beta) {
+        const double tp = 0.5 + 3.0 * nu_l;
+        const double tm = 0.5 + LAMBDA_TRT / (tp - 0.5);
+        const double tt = 0.5 + 3.0 * al_l;
+        LvlScal<A> c;
+        c.a_f = A(0.5 * (1.0 / tp + 1.0 / tm));
+        c.b_f = A(0.5 * (1.0 / tp - 1.0 / tm));
+        c.a_g = A(1.0 / tt);
+        c.c_m = A(1.0 - 0.5 / tm);
+        c.c_p = A(1.0 - 0.5 / tp);
+        c.om_p = A(1.0 / tp);
+        c.om_m = A(1.0 / tm);
+        c.om_g = A(1.0 / tt);
+        c.k_p = A(1.0 - 0.5 / tp);
+        c.k_m = A(1.0 - 0.5 / tm);
+        c.beta = A(beta);
+        return c;
+    }
+
+    // ramp_nu_alpha / ramp_beta_factor (src/octree/solver.rs:596-617) and the
+    // per-level tau / beta of step_cavity (:653-656, 718, 751-753).
+    OctScal<A> row(int64_t s) const {
+        double nu_eff = nu, al_eff = alpha, br = 1.0;
+        if (nu_start_mult != 1.0) {
+            const double m = 1.0 + (nu_start_mult - 1.0) * std::exp(-double(s) / 1000.0);
+            nu_eff = nu * m;
+            al_eff = alpha * m;
+            if (s < spin_up) br = double(s) / double(spin_up);
+        }
+        OctScal<A> r;
+        r.l[0] = lvl_scal(nu_eff, al_eff, beta_c * br);
+        r.l[1] = lvl_scal(2.0 * nu_eff, 2.0 * al_eff, (0.5 * beta_c) * br);
+        r.l[2] = lvl_scal(4.0 * nu_eff, 4.0 * al_eff, 0.25 * beta_c * br);
+        return r;
+    }
+
+    void setup(const cav_octree_params& pp) override {
+        p = pp;
+        if (p.bl_width < 2) throw ArgError{CAV_ERR_ARG, "bl_width >= 2 required"};
+        if (!(2 * p.bl_width < p.nx0)) throw ArgError{CAV_ERR_ARG, "2 * bl_width < nx0 required (coarse core)"};
+        if (p.levels != 2 && p.levels != 3) throw ArgError{CAV_ERR_ARG, "levels must be 2 or 3"};
+        if (p.ny0 < 4) throw ArgError{CAV_ERR_ARG, "ny0 >= 4 required"};
+        if ((long long)p.nx0 * p.ny0 * NPLANES >= (1ll << 31) || (long long)p.ny0 * 4 * (2 * p.bl_width + 3) * NPLANES >= (1ll << 31))
+            throw ArgError{CAV_ERR_ARG, "grid too large for 32-bit plane offsets"};
+        if (!(p.ra > 0 && p.pr > 0 && p.utarget > 0)) throw ArgError{CAV_ERR_ARG, "ra, pr, utarget must be > 0"};
+        levels = p.levels;
+        nx0 = p.nx0;
+        ny0 = p.ny0;
+        // CavitySolver::new, src/octree/solver.rs:298-336.
+        const double lz = double(ny0 - 1);
+        const double nu_cal = std::pow(p.utarget * std::sqrt(p.pr) * lz / (1.7 * std::sqrt(p.ra)), 2.0 / 3.0);
+        if (p.has_nu_override) {
+            if (!(p.nu_override > 0.0 && std::isfinite(p.nu_override)))
+                throw ArgError{CAV_ERR_ARG, "nu must be > 0 and finite"};
+            nu = p.nu_override;
+        } else {
+            nu = std::fmax(nu_cal, 0.002);
+        }
+        alpha = nu / p.pr;
+        beta_c = p.ra * nu * alpha / (lz * lz * lz);
+        nu_start_mult = std::max(p.nu_start_mult, 1.0);
+        spin_up = std::max<int64_t>(ny0 / 10, 2000);
+        for (int l = 0; l < 3; ++l) tau_p[l] = 0.5 + 3.0 * (double(1 << l) * nu);
+        auto xi_of = [&](int lc) {
+            // rescaling_factors_multilevel(tau(lc), tau(lc + 1), 2, odd_exact)
+            const double nc = lc == 0 ? nu : 2.0 * nu, ncf = lc == 0 ? 2.0 * nu : 4.0 * nu;
+            const double ac = lc == 0 ? alpha : 2.0 * alpha, acf = lc == 0 ? 2.0 * alpha : 4.0 * alpha;
+            const double tpc = 0.5 + 3.0 * nc, tpf = 0.5 + 3.0 * ncf;
+            const double tmc = 0.5 + LAMBDA_TRT / (tpc - 0.5), tmf = 0.5 + LAMBDA_TRT / (tpf - 0.5);
+            const double ttc = 0.5 + 3.0 * ac, ttf = 0.5 + 3.0 * acf;
+            const double dt = 1.0 / 2.0;
+            std::array<double, 3> x{dt * tpf / tpc, p.odd_exact ? dt * tmf / tmc : dt, dt * ttf / ttc};
+            return x;
+        };
+        const auto a = xi_of(0), b = xi_of(1);
+        for (int i = 0; i < 3; ++i) {
+            xiA[i] = a[i];
+            xiB[i] = b[i];
+        }
+        xa = make_xi(xiA);
+        xb = make_xi(xiB);
+        seed32 = uint32_t(p.seed) ^ uint32_t(p.seed >> 32) ^ 0x27d4eb2fu;
+
+        // grids (src/octree/solver.rs:356-431)
+        const int blw = p.bl_width;
+        HostGrid g1[2], g2[2];
+        const int spec[2][2] = {{0, blw}, {nx0 - 1 - blw, nx0 - 1}};
+        for (int b = 0; b < 2; ++b) g1[b].build(nx0, ny0, spec[b][0], 0, spec[b][1], ny0 - 1, false, false, false, false);
+        nx1 = g1[0].nx1;
+        ny1 = g1[0].ny1;
+        if (levels == 3) {
+            for (int b = 0; b < 2; ++b) {
+                const int sbx0 = b == 0 ? 1 : nx1 - 4, sbx1 = b == 0 ? 3 : nx1 - 2;
+                g2[b].build(nx1, ny1, sbx0, 1, sbx1, ny1 - 2, true, false, true, false);
+            }
+            nx2 = g2[0].nx1;
+            ny2 = g2[0].ny1;
+        }
+
+        CK(cudaSetDevice(p.device));
+        CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        alloc_level(L0, nx0, ny0, 1, 1, 0);
+        int off = nx0 * ny0;
+        for (int b = 0; b < 2; ++b) {
+            alloc_level(L1[b], nx1, ny1, b == 0, b == 1, off);
+            off += nx1 * ny1;
+        }
+        if (levels == 3)
+            for (int b = 0; b < 2; ++b) {
+                alloc_level(L2[b], nx2, ny2, b == 0, b == 1, off);
+                off += nx2 * ny2;
+            }
+
+        // tables
+        auto upload_ghosts = [&](HostGrid* g, GhostE<A>*& dst, int& ng) {
+            ng = int(g[0].ghosts.size());
+            std::vector<GhostE<A>> h(2 * size_t(ng));
+            for (int b = 0; b < 2; ++b)
+                for (int j = 0; j < ng; ++j) {
+                    const auto& e = g[b].ghosts[j];
+                    GhostE<A>& o = h[size_t(b) * ng + j];
+                    o.kf = e.kf;
+                    for (int s = 0; s < 4; ++s) {
+                        o.kc[s] = e.kc[s];
+                        o.w[s] = A(e.w[s]);
+                    }
+                }
+            dst = dalloc<GhostE<A>>(h.size());
+            CK(cudaMemcpyAsync(dst, h.data(), sizeof(GhostE<A>) * h.size(), cudaMemcpyHostToDevice, stream));
+            CK(cudaStreamSynchronize(stream));
+        };
+        auto upload_coin = [&](HostGrid* g, CoinE*& dst, int& c0, int& c1) {
+            c0 = int(g[0].coin.size());
+            c1 = int(g[1].coin.size());
+            std::vector<CoinE> h(g[0].coin);
+            h.insert(h.end(), g[1].coin.begin(), g[1].coin.end());
+            dst = dalloc<CoinE>(h.size());
+            CK(cudaMemcpyAsync(dst, h.data(), sizeof(CoinE) * h.size(), cudaMemcpyHostToDevice, stream));
+            CK(cudaStreamSynchronize(stream));
+        };
+        upload_ghosts(g1, gh1, n_ghost);
+        upload_coin(g1, co1, n_co0, n_co1);
+        if (levels == 3) {
+            upload_ghosts(g2, gh2, n_ghost2);
+            upload_coin(g2, co2, n_co2_0, n_co2_1);
+        }
+
+        // per-step table: rows until the ramps have converged bit for bit
+        std::vector<OctScal<A>> rows;
+        rows.push_back(row(0));
+        if (nu_start_mult != 1.0) {
+            for (int64_t s = 1;; ++s) {
+                const double m = 1.0 + (nu_start_mult - 1.0) * std::exp(-double(s) / 1000.0);
+                rows.push_back(row(s));
+                if (m == 1.0 && s >= spin_up) break;
+                if (s > 4000000) throw ArgError{CAV_ERR_ARG, "viscosity ramp does not converge"};
+            }
+        }
+        S = int(rows.size()) - 1;
+        tab = dalloc<OctScal<A>>(rows.size());
+        CK(cudaMemcpyAsync(tab, rows.data(), sizeof(OctScal<A>) * rows.size(), cudaMemcpyHostToDevice, stream));
+        step_dev = dalloc<long long>(1);
+        part = dalloc<double>(size_t(5) * OSTAT_CTAS * OSTAT);
+        iface = dalloc<double>(8);
+        dout = dalloc<double>(16);
+        CK(cudaStreamSynchronize(stream));
+        init_cavity();
+    }
+
+    // init_cavity, src/octree/solver.rs:504-578.
+    void init_cavity() {
+        Rng rng(p.seed);
+        const size_t n0 = size_t(nx0) * ny0;
+        std::vector<double> t0(n0);
+        for (int iy = 0; iy < ny0; ++iy)
+            for (int ix = 0; ix < nx0; ++ix) {
+                const double xf = double(ix) / double(nx0 - 1);
+                const double t_lin = T_HOT_C + (T_COLD_C - T_HOT_C) * xf;
+                const double pert = 1.0e-3 * (2.0 * rng.next_f64() - 1.0);
+                t0[size_t(iy) * nx0 + ix] = t_lin + pert;
+            }
+        upload_eq(L0, t0);
+        auto interp = [&](double x, double y) {
+            int kc[4];
+            double w[4];
+            HostGrid::bilinear(x, y, nx0, ny0, kc, w);
+            double t = 0.0;
+            for (int s = 0; s < 4; ++s) t += w[s] * t0[kc[s]];
+            return t;
+        };
+        const int blw = p.bl_width;
+        const int bx0s[2] = {0, nx0 - 1 - blw};
+        for (int b = 0; b < 2; ++b) {
+            std::vector<double> t1(size_t(nx1) * ny1);
+            for (int yb = 0; yb < ny1; ++yb)
+                for (int a = 0; a < nx1; ++a)
+                    t1[size_t(yb) * nx1 + a] = interp(double(bx0s[b]) - 0.5 + 0.5 * a, -0.5 + 0.5 * yb);
+            upload_eq(L1[b], t1);
+            if (levels == 3) {
+                const int sbx0 = b == 0 ? 1 : nx1 - 4;
+                std::vector<double> t2(size_t(nx2) * ny2);
+                for (int b2 = 0; b2 < ny2; ++b2)
+                    for (int a2 = 0; a2 < nx2; ++a2) {
+                        const double x = double(bx0s[b]) - 0.5 + 0.5 * (double(sbx0) - 0.5 + 0.5 * a2);
+                        const double y = 0.0 - 0.5 + 0.5 * (1.0 - 0.5 + 0.5 * b2);
+                        t2[size_t(b2) * nx2 + a2] = interp(x, y);
+                    }
+                upload_eq(L2[b], t2);
+            }
+        }
+        time_step = 0;
+        pc_valid = false;
+    }
+
+    // f = feq(1, 0, 0), g = geq(T, 0, 0), rho = 1, u = 0, fy = 0.
+    template <class St>
+    void upload_eq(Lvl<St>& L, const std::vector<double>& t) {
+        const size_t n = size_t(L.n);
+        std::vector<double> f(n * Q), g(n * Q), r(n, 1.0), z(n, 0.0);
+        for (size_t k = 0; k < n; ++k)
+            for (int i = 0; i < Q; ++i) {
+                f[k * Q + i] = feq_full<double>(i, 1.0, 0.0, 0.0);
+                g[k * Q + i] = geq_full<double>(i, t[k], 0.0, 0.0, 2);
+            }
+        upload_state(L, r.data(), z.data(), z.data(), t.data(), f.data(), g.data());
+        CK(cudaMemsetAsync(L.fy, 0, sizeof(A) * n, stream));
+        CK(cudaStreamSynchronize(stream));
+    }
+
+    template <class St>
+    void upload_state(Lvl<St>& L, const double* r, const double* u, const double* v, const double* t, const double* f,
+                      const double* g) {
+        const size_t n = size_t(L.n);
+        if (f || g) {
+            std::vector<St> hp(NPLANES * n);
+            CK(cudaMemcpyAsync(hp.data(), L.ref[L.cur], sizeof(St) * hp.size(), cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+            for (size_t k = 0; k < n; ++k)
+                for (int i = 0; i < Q; ++i) {
+                    if (f) hp[size_t(i) * n + k] = Fmt<St>::store(A(f[k * Q + i] - (SH ? WD(i) : 0.0)), i, RN_BITS);
+                    if (g) hp[size_t(Q + i) * n + k] = Fmt<St>::store(A(g[k * Q + i]), Q + i, RN_BITS);
+                }
+            CK(cudaMemcpyAsync(L.ref[L.cur], hp.data(), sizeof(St) * hp.size(), cudaMemcpyHostToDevice, stream));
+        }
+        std::vector<A> hm(4 * n);
+        CK(cudaMemcpyAsync(hm.data(), L.mac, sizeof(A) * hm.size(), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        for (size_t k = 0; k < n; ++k) {
+            if (r) hm[k] = A(SH ? r[k] - 1.0 : r[k]);
+            if (u) hm[n + k] = A(u[k]);
+            if (v) hm[2 * n + k] = A(v[k]);
+            if (t) hm[3 * n + k] = A(t[k]);
+        }
+        CK(cudaMemcpyAsync(L.mac, hm.data(), sizeof(A) * hm.size(), cudaMemcpyHostToDevice, stream));
+        CK(cudaStreamSynchronize(stream));
+        pc_valid = false;
+    }
+
+    template <class St>
+    void download_state(const Lvl<St>& L, double* r, double* u, double* v, double* t, double* f, double* g) {
+        const size_t n = size_t(L.n);
+        if (f || g) {
+            std::vector<St> hp(NPLANES * n);
+            CK(cudaMemcpyAsync(hp.data(), L.ref[L.cur], sizeof(St) * hp.size(), cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+            for (size_t k = 0; k < n; ++k)
+                for (int i = 0; i < Q; ++i) {
+                    if (f) f[k * Q + i] = double(Fmt<St>::load(hp[size_t(i) * n + k], i)) + (SH ? WD(i) : 0.0);
+                    if (g) g[k * Q + i] = double(Fmt<St>::load(hp[size_t(Q + i) * n + k], Q + i));
+                }
+        }
+        std::vector<A> hm(4 * n);
+        CK(cudaMemcpyAsync(hm.data(), L.mac, sizeof(A) * hm.size(), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        for (size_t k = 0; k < n; ++k) {
+            if (r) r[k] = SH ? 1.0 + double(hm[k]) : double(hm[k]);
+            if (u) u[k] = double(hm[n + k]);
+            if (v) v[k] = double(hm[2 * n + k]);
+            if (t) t[k] = double(hm[3 * n + k]);
+        }
+    }
+
+    void check_launch() {
+        ++launches;
+        CK(cudaGetLastError());
+    }
+
+    template <class St>
+    static LvlPair<St> pair(const Lvl<St>& a, const Lvl<St>& b) {
+        LvlPair<St> q;
+        q.b[0] = a.io();
+        q.b[1] = b.io();
+        return q;
+    }
+    template <class St>
+    static LvlPair<St> pair_cur(const Lvl<St>& a, const Lvl<St>& b) {
+        LvlPair<St> q;
+        q.b[0] = a.io_cur();
+        q.b[1] = b.io_cur();
+        return q;
+    }
+    static dim3 grid_of(int n, int nb) { return dim3((n + OT - 1) / OT, nb); }
+
+    void set_step_dev() {
+        if (step_dev_val != time_step) {
+            k_set_step<<<1, 1, 0, stream>>>(step_dev, time_step);
+            check_launch();
+            step_dev_val = time_step;
+        }
+    }
+
+    // The first collision of every level from the REF state.
+    void collide_all() {
+        set_step_dev();
+        {
+            LvlPair<StC> q = pair_cur(L0, L0);
+            k_oct_collide<StC, true><<<grid_of(L0.n, 1), OT, 0, stream>>>(q, tab, S, step_dev, 0, seed32, 10);
+            check_launch();
+        }
+        {
+            LvlPair<StF> q = pair_cur(L1[0], L1[1]);
+            k_oct_collide<StF, false><<<grid_of(L1[0].n, 2), OT, 0, stream>>>(q, tab, S, step_dev, 1, seed32, 11);
+            check_launch();
+        }
+        if (levels == 3) {
+            LvlPair<StF> q = pair_cur(L2[0], L2[1]);
+            k_oct_collide<StF, false><<<grid_of(L2[0].n, 2), OT, 0, stream>>>(q, tab, S, step_dev, 2, seed32, 12);
+            check_launch();
+        }
+        pc_valid = true;
+    }
+
+    void c2f_L1() {
+        LvlPair<StC> c = pair_cur(L0, L0);
+        LvlPair<StF> f = pair_cur(L1[0], L1[1]);
+        k_oct_c2f<StC, StF><<<grid_of(4 * n_ghost, 2), OT, 0, stream>>>(c, f, gh1, n_ghost, xa, step_dev, seed32, 2);
+        check_launch();
+    }
+    void c2f_L2() {
+        LvlPair<StF> c = pair_cur(L1[0], L1[1]);
+        LvlPair<StF> f = pair_cur(L2[0], L2[1]);
+        k_oct_c2f<StF, StF><<<grid_of(4 * n_ghost2, 2), OT, 0, stream>>>(c, f, gh2, n_ghost2, xb, step_dev, seed32, 4);
+        check_launch();
+    }
+    void f2c_L2(int off) {
+        LvlPair<StF> f = pair_cur(L2[0], L2[1]);
+        LvlPair<StF> c = pair_cur(L1[0], L1[1]);
+        k_oct_f2c<StF, StF><<<grid_of(16 * std::max(n_co2_0, n_co2_1), 2), OT, 0, stream>>>(
+            f, c, co2, n_co2_0, n_co2_1, xb, tab, S, step_dev, off, 1, seed32, 7);
+        check_launch();
+    }
+    void f2c_L1(int off) {
+        LvlPair<StF> f = pair_cur(L1[0], L1[1]);
+        LvlPair<StC> c = pair_cur(L0, L0);
+        k_oct_f2c<StF, StC><<<grid_of(16 * std::max(n_co0, n_co1), 2), OT, 0, stream>>>(
+            f, c, co1, n_co0, n_co1, xa, tab, S, step_dev, off, 0, seed32, 13);
+        check_launch();
+    }
+    void step_L0() {
+        LvlPair<StC> q = pair(L0, L0);
+        k_oct_step<StC, true><<<grid_of(L0.n, 1), OT, 0, stream>>>(q, tab, S, step_dev, 1, 0, seed32, 1);
+        check_launch();
+        L0.cur ^= 1;
+    }
+    void step_L1(int off, int phase) {
+        LvlPair<StF> q = pair(L1[0], L1[1]);
+        k_oct_step<StF, false><<<grid_of(L1[0].n, 2), OT, 0, stream>>>(q, tab, S, step_dev, off, 1, seed32, phase);
+        check_launch();
+        L1[0].cur ^= 1;
+        L1[1].cur ^= 1;
+    }
+    void step_L2(int off, int phase) {
+        LvlPair<StF> q = pair(L2[0], L2[1]);
+        k_oct_step<StF, false><<<grid_of(L2[0].n, 2), OT, 0, stream>>>(q, tab, S, step_dev, off, 2, seed32, phase);
+        check_launch();
+        L2[0].cur ^= 1;
+        L2[1].cur ^= 1;
+    }
+
+    // One step_cavity (src/octree/solver.rs:647-947), all launches on `stream`,
+    // with the step index taken from *step_dev (advanced at the end).
+    void launch_coarse_step() {
+        step_L0();
+        c2f_L1();
+        step_L1(0, 3);
+        if (levels == 3) {
+            c2f_L2();
+            step_L2(0, 5);
+            step_L2(1, 6);
+            f2c_L2(0);
+        }
+        step_L1(1, 9);
+        f2c_L1(1);
+        k_add_step<<<1, 1, 0, stream>>>(step_dev, 1);
+        check_launch();
+    }
+
+    cudaGraphExec_t get_graph() {
+        cudaGraphExec_t& gx = graph[L0.cur];
+        if (gx) return gx;
+        const int c0 = L0.cur, c1 = L1[0].cur, c2 = L2[0].cur;
+        const int64_t l0 = launches;
+        CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        for (int j = 0; j < OCT_GRAPH_STEPS; ++j) launch_coarse_step();
+        cudaGraph_t gr;
+        CK(cudaStreamEndCapture(stream, &gr));
+        L0.cur = c0;
+        L1[0].cur = L1[1].cur = c1;
+        L2[0].cur = L2[1].cur = c2;
+        launches = l0;
+        CK(cudaGraphInstantiate(&gx, gr, 0));
+        cudaGraphDestroy(gr);
+        return gx;
+    }
+
+    int per_step_launches() const { return levels == 3 ? 10 : 6; }
+
+    void step(int64_t n) override {
+        if (n <= 0) return;
+        if (!pc_valid) collide_all();
+        set_step_dev();
+        while (n > 0) {
+            if (n >= OCT_GRAPH_STEPS) {
+                cudaGraphExec_t gx = get_graph();
+                CK(cudaGraphLaunch(gx, stream));
+                launches += int64_t(OCT_GRAPH_STEPS) * per_step_launches();
+                time_step += OCT_GRAPH_STEPS;
+                n -= OCT_GRAPH_STEPS;
+            } else {
+                launch_coarse_step();
+                time_step += 1;
+                n -= 1;
+            }
+            step_dev_val = time_step;
+        }
+        CK(cudaGetLastError());
+    }
+
+    void get_level(int lvl, double* r, double* u, double* v, double* t, double* f, double* g) override {
+        CK(cudaStreamSynchronize(stream));
+        if (lvl == 0) return download_state(L0, r, u, v, t, f, g);
+        if (lvl == 1 || lvl == 2) return download_state(L1[lvl - 1], r, u, v, t, f, g);
+        if (levels == 3 && (lvl == 3 || lvl == 4)) return download_state(L2[lvl - 3], r, u, v, t, f, g);
+        throw ArgError{CAV_ERR_ARG, "no such level"};
+    }
+
+    void set_level(int lvl, const double* r, const double* u, const double* v, const double* t, const double* f,
+                   const double* g) override {
+        CK(cudaStreamSynchronize(stream));
+        if (lvl == 0) return upload_state(L0, r, u, v, t, f, g);
+        if (lvl == 1 || lvl == 2) return upload_state(L1[lvl - 1], r, u, v, t, f, g);
+        if (levels == 3 && (lvl == 3 || lvl == 4)) return upload_state(L2[lvl - 3], r, u, v, t, f, g);
+        throw ArgError{CAV_ERR_ARG, "no such level"};
+    }
+
+    // Single couplings on the current state (for the interface tests):
+    // 0 = coarse_to_fine L0 -> L1, 1 = fine_to_coarse L1 -> L0 (+ refresh),
+    // 2 = coarse_to_fine L1 -> L2, 3 = fine_to_coarse L2 -> L1 (+ refresh).
+    void debug_phase(int phase) override {
+        set_step_dev();
+        if (phase == 0) c2f_L1();
+        else if (phase == 1) f2c_L1(0);
+        else if (levels == 3 && phase == 2) c2f_L2();
+        else if (levels == 3 && phase == 3) f2c_L2(0);
+        else throw ArgError{CAV_ERR_ARG, "no such coupling phase"};
+        pc_valid = false;
+        CK(cudaStreamSynchronize(stream));
+    }
+
+    void diag(double* out) override {
+        StatViews<A> V{};
+        int nv = 0;
+        V.v[nv++] = StatView<A>{L0.mac, L0.n};
+        for (int b = 0; b < 2; ++b) V.v[nv++] = StatView<A>{L1[b].mac, L1[b].n};
+        if (levels == 3)
+            for (int b = 0; b < 2; ++b) V.v[nv++] = StatView<A>{L2[b].mac, L2[b].n};
+        k_oct_stats<A, SH><<<dim3(OSTAT_CTAS, nv), 256, 0, stream>>>(V, part);
+        check_launch();
+        k_oct_iface<A, SH><<<2, 256, 0, stream>>>(L1[0].mac, L1[1].mac, L0.mac, L0.mac, gh1, n_ghost, co1, n_co0,
+                                                 n_co1, iface);
+        check_launch();
+        int n_if = 2;
+        if (levels == 3) {
+            k_oct_iface<A, SH><<<2, 256, 0, stream>>>(L2[0].mac, L2[1].mac, L1[0].mac, L1[1].mac, gh2, n_ghost2, co2,
+                                                     n_co2_0, n_co2_1, iface + 4);
+            check_launch();
+            n_if = 4;
+        }
+        const bool l3 = levels == 3;
+        const A* mf = l3 ? L2[0].mac : L1[0].mac;
+        const int nxf = l3 ? nx2 : nx1, nyf = l3 ? ny2 : ny1;
+        const double nu_f = (l3 ? 4.0 : 2.0) * nu;
+        k_oct_final<A, SH><<<1, 32, 0, stream>>>(L0.mac, nx0, ny0, L1[0].mac, nx1, ny1, mf, nxf, nyf, nu_f, part, nv,
+                                                 OSTAT_CTAS, iface, n_if, dout);
+        check_launch();
+        CK(cudaMemcpyAsync(out, dout, sizeof(double) * 10, cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+    }
+
+    void sync() override { CK(cudaStreamSynchronize(stream)); }
+};
+
+}  // namespace oct
+}  // namespace cav

@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <type_traits>
 #include <cmath>
 #include <cstdio>

@@ -1,0 +1,152 @@
+"""Python mirror of the reference's block-refined ``octree::solver::CavitySolver``
+(``src/octree/solver.rs:284-1206``) over the ``cav_octree_*`` C ABI.
+
+Same constructor arguments as ``CavitySolver::new(nx0, ny0, bl_width, ra,
+pr, utarget, seed, jobs, odd_exact, levels, nu_start_mult, nu_override)``,
+``step_cavity``, ``noise_stats``, ``max_u_all``, ``check_guards`` and the
+Nusselt estimators of ``src/octree/cavity.rs:672-741``.  The level fields
+the reference tests read (``sim.coarse.rho``, ``block.fine.temp`` ...) come
+back through ``level()``.  All computation runs in the CUDA library.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+
+COARSE, HOT_L1, COLD_L1, HOT_L2, COLD_L2 = range(5)
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(L._dp)
+
+
+class OctreeSolver:
+    def __init__(self, nx0, ny0, bl_width, ra, pr, utarget, seed, jobs=1, odd_exact=False, levels=2,
+                 nu_start_mult=1.0, nu_override=None, *, precision="f64", device=0):
+        lib = L.load()
+        p = L.CavOctreeParams()
+        L.check_octree(lib.cav_octree_default_params(ctypes.byref(p)))
+        p.nx0, p.ny0, p.bl_width = nx0, ny0, bl_width
+        p.ra, p.pr, p.utarget, p.seed, p.jobs = ra, pr, utarget, seed, jobs
+        p.odd_exact, p.levels, p.nu_start_mult = int(bool(odd_exact)), levels, nu_start_mult
+        p.has_nu_override = 0 if nu_override is None else 1
+        p.nu_override = 0.0 if nu_override is None else float(nu_override)
+        p.precision = L.OCT_PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        p.device = device
+        h = ctypes.c_void_p()
+        L.check_octree(lib.cav_octree_create(ctypes.byref(p), ctypes.byref(h)))
+        self._h = h
+        self.precision = precision
+        self.levels = levels
+        self.nx0, self.ny0 = nx0, ny0
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            L.load().cav_octree_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc):
+        L.check_octree(rc, self._h)
+
+    def step_cavity(self, n: int = 1):
+        """``n`` calls of ``step_cavity`` (src/octree/solver.rs:647-947)."""
+        self._ck(L.load().cav_octree_step(self._h, int(n)))
+
+    def info(self):
+        i = L.CavOctreeInfo()
+        self._ck(L.load().cav_octree_get_info(self._h, ctypes.byref(i)))
+        out = {}
+        for k, _ in L.CavOctreeInfo._fields_:
+            v = getattr(i, k)
+            out[k] = list(v) if isinstance(v, ctypes.Array) else v
+        return out
+
+    def n_nodes_total(self):
+        """``n_nodes_total`` (src/octree/solver.rs:475-486)."""
+        return self.info()["n_nodes_total"]
+
+    def level(self, lvl, pops=False):
+        """Fields of level ``lvl`` (0 coarse, 1/2 hot/cold L1, 3/4 hot/cold L2)."""
+        i = self.info()
+        nx, ny = i["nx"][lvl], i["ny"][lvl]
+        n = nx * ny
+        out = {k: np.empty(n) for k in ("rho", "ux", "uy", "temp")}
+        f = np.empty((n, 9)) if pops else None
+        g = np.empty((n, 9)) if pops else None
+        self._ck(L.load().cav_octree_get_level(self._h, lvl, _dp(out["rho"]), _dp(out["ux"]),
+                                               _dp(out["uy"]), _dp(out["temp"]), _dp(f), _dp(g)))
+        if pops:
+            out["f"], out["g"] = f, g
+        out["nx"], out["ny"] = nx, ny
+        return out
+
+    def set_level(self, lvl, rho=None, ux=None, uy=None, temp=None, f=None, g=None):
+        def c(a, shape=None):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            return a
+        arrs = [c(a) for a in (rho, ux, uy, temp, f, g)]
+        self._ck(L.load().cav_octree_set_level(self._h, lvl, *[_dp(a) for a in arrs]))
+
+    def couple(self, which):
+        """One coupling: 0 coarse_to_fine L0->L1, 1 fine_to_coarse L1->L0,
+        2 / 3 the same between L1 and L2 (src/octree/interface.rs:137-206)."""
+        self._ck(L.load().cav_octree_couple(self._h, int(which)))
+
+    def diag(self):
+        d = L.CavOctreeDiag()
+        self._ck(L.load().cav_octree_diag(self._h, ctypes.byref(d)))
+        return {k: getattr(d, k) for k, _ in L.CavOctreeDiag._fields_}
+
+    def noise_stats(self):
+        """``noise_stats`` (src/octree/solver.rs:954-1003)."""
+        d = self.diag()
+        return {"max_rho_dev": d["max_rho_dev"], "max_rho_dev_ifaces": d["max_rho_dev_ifaces"],
+                "masse": d["mass"]}
+
+    def max_u_all(self):
+        return self.diag()["max_u"]
+
+    def nusselt_hot(self):
+        return self.diag()["nu_hot"]
+
+    def nusselt_cold(self):
+        return self.diag()["nu_cold"]
+
+    def nusselt_hot_link0(self):
+        return self.diag()["nu_hot_link0"]
+
+    def nusselt_hot_fine(self):
+        return self.diag()["nu_hot_fine"]
+
+    def check_guards(self, max_u_abort=0.10):
+        """``check_guards`` (src/octree/solver.rs:1019-1038): 0 when all pass."""
+        return L.load().cav_octree_check_guards(self._h, max_u_abort)
+
+    def sync(self):
+        self._ck(L.load().cav_octree_sync(self._h))
+
+    def stream_handle(self):
+        s = ctypes.c_void_p()
+        self._ck(L.load().cav_octree_get_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    def launch_count(self):
+        n = ctypes.c_int64()
+        self._ck(L.load().cav_octree_launch_count(self._h, ctypes.byref(n)))
+        return n.value
+
+    @property
+    def time_step(self):
+        return self.info()["time_step"]

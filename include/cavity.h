@@ -239,6 +239,91 @@ int cav_batch_sync(cav_batch* b);
 int cav_batch_get_stream(cav_batch* b, void** stream);
 int cav_batch_launch_count(cav_batch* b, int64_t* n);
 
+/* ---- block-refined (octree) cavity: src/octree/ ------------------------- */
+/* Replaces octree::solver::CavitySolver (src/octree/solver.rs:284-1206) with
+ * the dynamic SGS model off (the default, src/cli.rs:117):
+ *   cav_octree_create   CavitySolver::new (solver.rs:284-471), init_cavity
+ *                       (:504-578)
+ *   cav_octree_step     n x step_cavity (:647-947)
+ *   cav_octree_diag     nusselt_hot / nusselt_hot_link0 / nusselt_cold /
+ *                       nusselt_hot_fine (src/octree/cavity.rs:672-741),
+ *                       max_u_all (solver.rs:1005-1016), noise_stats
+ *                       (:954-1003), check_finite_levels (cavity.rs:751)
+ *   cav_octree_check_guards  check_guards (solver.rs:1019-1038)
+ *   cav_octree_get_level     the LbmLevel fields (src/octree/lbm.rs:19-53)
+ * Levels are numbered 0 = coarse L0, 1 / 2 = hot / cold L1 blocks,
+ * 3 / 4 = hot / cold L2 strips (levels = 3).  Populations cross the ABI as
+ * the reference's AoS [k][9] FP64, k = b * nx + a. */
+enum {
+    CAV_OCT_F64 = 0,     /* FP64 everywhere (bit-identical to the FP64 oracle) */
+    CAV_OCT_F32 = 1,     /* FP32 arithmetic and storage                        */
+    CAV_OCT_F32_F16 = 2, /* FP32 arithmetic, FP32 L0, binary16 (stochastic
+                            rounding) L1 / L2 populations                      */
+    CAV_OCT_F32_F16G = 3 /* as CAV_OCT_F32_F16 with the L1 / L2 g populations
+                            in 16-bit fixed point (CAV_PREC_F16GSR's format)   */
+};
+typedef struct cav_octree_params {
+    int32_t nx0, ny0;      /* coarse grid                                       */
+    int32_t bl_width;      /* L1 block width in coarse cells (--bl-width)       */
+    double ra, pr, utarget;
+    uint64_t seed;
+    int32_t jobs;          /* accepted for signature parity; unused             */
+    int32_t odd_exact;     /* xi_odd = tau-_f / tau-_c / 2 instead of 1/2       */
+    int32_t levels;        /* 2 or 3                                            */
+    double nu_start_mult;  /* viscosity ramp start multiplier (>= 1)            */
+    int32_t has_nu_override;
+    double nu_override;
+    int32_t precision;     /* CAV_OCT_*                                         */
+    int32_t device;
+} cav_octree_params;
+typedef struct cav_octree_info {
+    double nu, alpha, beta_eff_coarse;
+    double tau_plus[3];                       /* L0, L1, L2                     */
+    double xi_even, xi_odd, xi_thermal;       /* interface L0 / L1              */
+    double xi_even_sub, xi_odd_sub, xi_thermal_sub; /* interface L1 / L2        */
+    int64_t time_step, spin_up_steps, n_nodes_total;
+    int32_t levels, precision;
+    int32_t nx[5], ny[5];                     /* per level (0 when absent)      */
+    int32_t n_ghosts, n_coincident;           /* L1 blocks, summed over both    */
+    int32_t n_ghosts_sub, n_coincident_sub;   /* L2 strips, summed over both    */
+} cav_octree_info;
+typedef struct cav_octree_diag_out {
+    double nu_hot, nu_hot_link0, nu_cold; /* coarse, 2nd / 1st link, x Lx      */
+    double nu_hot_fine;                   /* hot L1 block, x lx_coarse         */
+    double max_u;                         /* all levels, max(|ux|, |uy|)       */
+    double mass;                          /* mean coarse rho                   */
+    double max_rho_dev, max_rho_dev_ifaces;
+    double finite;                        /* 1.0 when every field is finite    */
+    double y_plus_fine;                   /* post.rs:182-199 formula on the
+                                             finest hot-wall level (the
+                                             reference octree has no y+)       */
+} cav_octree_diag_out;
+typedef struct cav_octree cav_octree;
+int cav_octree_default_params(cav_octree_params* p);
+int cav_octree_create(const cav_octree_params* p, cav_octree** out);
+int cav_octree_destroy(cav_octree* h);
+const char* cav_octree_last_error(const cav_octree* h);
+int cav_octree_step(cav_octree* h, int64_t n_coarse_steps);
+int cav_octree_get_info(cav_octree* h, cav_octree_info* out);
+/* Any output pointer may be NULL.  rho, ux, uy, t: [nx*ny]; f, g: [nx*ny][9]. */
+int cav_octree_get_level(cav_octree* h, int32_t level, double* rho, double* ux, double* uy, double* t,
+                         double* f, double* g);
+/* Overwrites the given parts of a level's state (NULL = keep); the next step
+ * starts with the collision of that state, as the reference's would. */
+int cav_octree_set_level(cav_octree* h, int32_t level, const double* rho, const double* ux,
+                         const double* uy, const double* t, const double* f, const double* g);
+/* One coupling on the current state: 0 = coarse_to_fine L0 -> L1,
+ * 1 = fine_to_coarse L1 -> L0 + moment refresh, 2 / 3 = the same between L1
+ * and L2 (src/octree/interface.rs:137-206). */
+int cav_octree_couple(cav_octree* h, int32_t which);
+int cav_octree_diag(cav_octree* h, cav_octree_diag_out* out);
+/* check_guards: CAV_OK, CAV_ERR_MAXU (max_u > max_u_abort) or
+ * CAV_ERR_DIVERGED (a non-finite field). */
+int cav_octree_check_guards(cav_octree* h, double max_u_abort);
+int cav_octree_sync(cav_octree* h);
+int cav_octree_get_stream(cav_octree* h, void** stream);
+int cav_octree_launch_count(cav_octree* h, int64_t* n);
+
 /* ---- diagnostics without device allocation ------------------------------ */
 /* No counterpart in the reference.  The diagnostics of cav_diag computed on a
  * cavity state that lives in the caller's own device memory, for callers that

@@ -96,6 +96,18 @@ def lib():
         L.orc_avg_means.argtypes = [vp, dp, dp, dp, dp, dp]
         L.orc_nusselt_from_mean.restype = ctypes.c_double
         L.orc_nusselt_from_mean.argtypes = [vp, dp, ctypes.c_int32]
+        i32, d = ctypes.c_int32, ctypes.c_double
+        L.orc_oct_create.restype = vp
+        L.orc_oct_create.argtypes = [i32, i32, i32, d, d, d, ctypes.c_uint64, i32, i32, d, i32, d,
+                                     ctypes.POINTER(i32)]
+        L.orc_oct_destroy.argtypes = [vp]
+        L.orc_oct_step.argtypes = [vp, i64]
+        L.orc_oct_level_dims.restype = i32
+        L.orc_oct_level_dims.argtypes = [vp, i32, ctypes.POINTER(i32), ctypes.POINTER(i32)]
+        L.orc_oct_get_level.restype = i32
+        L.orc_oct_get_level.argtypes = [vp, i32, dp, dp, dp, dp, dp, dp]
+        L.orc_oct_info.argtypes = [vp, dp]
+        L.orc_oct_diag.argtypes = [vp, dp]
         _lib = L
     return _lib
 
@@ -317,3 +329,67 @@ class OracleAverager:
         out = [np.empty(self._n) for _ in range(5)]
         cnt = lib().orc_avg_means(self._a, *[_dp(a) for a in out])
         return cnt, out
+
+
+OCT_INFO_KEYS = ("nu", "alpha", "beta_eff_coarse", "tau_plus_l0", "tau_plus_l1", "tau_plus_l2",
+                 "xi_even", "xi_odd", "xi_thermal", "xi_even_sub", "time_step", "n_coincident",
+                 "n_ghosts")
+OCT_DIAG_KEYS = ("nu_hot", "nu_hot_link0", "nu_cold", "nu_hot_fine", "max_u", "mass",
+                 "max_rho_dev", "max_rho_dev_ifaces", "finite")
+
+
+class OracleOctree:
+    """CPU FP64 restatement of the block-refined ``octree::solver::CavitySolver``
+    (src/octree/solver.rs:284-947): ``CavitySolver::new(nx0, ny0, bl_width,
+    ra, pr, utarget, seed, jobs, odd_exact, levels, nu_start_mult,
+    nu_override)`` and ``step_cavity``.  Levels: 0 coarse, 1/2 the hot/cold
+    L1 blocks, 3/4 the hot/cold L2 strips (levels = 3)."""
+
+    def __init__(self, nx0, ny0, bl_width, ra, pr, utarget, seed, jobs=1, odd_exact=False, levels=2,
+                 nu_start_mult=1.0, nu_override=None):
+        err = ctypes.c_int32(0)
+        self._h = lib().orc_oct_create(nx0, ny0, bl_width, ra, pr, utarget, seed, int(odd_exact), levels,
+                                       nu_start_mult, 0 if nu_override is None else 1,
+                                       0.0 if nu_override is None else float(nu_override),
+                                       ctypes.byref(err))
+        if not self._h:
+            raise OracleError(f"orc_oct_create failed with code {err.value}")
+        self.levels = levels
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().orc_oct_destroy(h)
+            self._h = None
+
+    def step_cavity(self, n: int = 1):
+        lib().orc_oct_step(self._h, int(n))
+
+    def level_dims(self, level):
+        nx, ny = ctypes.c_int32(), ctypes.c_int32()
+        if lib().orc_oct_level_dims(self._h, level, ctypes.byref(nx), ctypes.byref(ny)):
+            raise OracleError(f"no level {level}")
+        return nx.value, ny.value
+
+    def level(self, level, pops=False):
+        nx, ny = self.level_dims(level)
+        n = nx * ny
+        out = {k: np.empty(n) for k in ("rho", "ux", "uy", "temp")}
+        f = np.empty((n, 9)) if pops else None
+        g = np.empty((n, 9)) if pops else None
+        lib().orc_oct_get_level(self._h, level, _dp(out["rho"]), _dp(out["ux"]), _dp(out["uy"]),
+                                _dp(out["temp"]), _dp(f), _dp(g))
+        if pops:
+            out["f"], out["g"] = f, g
+        out["nx"], out["ny"] = nx, ny
+        return out
+
+    def info(self):
+        o = np.empty(len(OCT_INFO_KEYS))
+        lib().orc_oct_info(self._h, _dp(o))
+        return dict(zip(OCT_INFO_KEYS, o.tolist()))
+
+    def diag(self):
+        o = np.empty(len(OCT_DIAG_KEYS))
+        lib().orc_oct_diag(self._h, _dp(o))
+        return dict(zip(OCT_DIAG_KEYS, o.tolist()))

@@ -78,6 +78,21 @@ double orc_nusselt_from_mean(void* h, const double* t_mean, int32_t hot);
 int orc_tl_nusselt(const orc_params* p, int64_t n_steps, int64_t ws, const double* dtheta, double dcs,
                    double* J, double* dJ);
 
+/* Block-refined (octree) cavity, src/octree/solver.rs (fixed Cs, no dynamic
+ * SGS).  levels 2 or 3; odd_exact selects the tau- ratio for the odd
+ * rescaling.  *err = 1 on invalid arguments (CavitySolver::new asserts). */
+void* orc_oct_create(int32_t nx0, int32_t ny0, int32_t bl_width, double ra, double pr, double utarget,
+                     uint64_t seed, int32_t odd_exact, int32_t levels, double nu_start_mult, int32_t has_nu,
+                     double nu, int32_t* err);
+void orc_oct_destroy(void* h);
+void orc_oct_step(void* h, int64_t n);
+/* level 0 coarse, 1/2 hot/cold L1 blocks, 3/4 hot/cold L2 strips. */
+int32_t orc_oct_level_dims(void* h, int32_t level, int32_t* nx, int32_t* ny);
+int32_t orc_oct_get_level(void* h, int32_t level, double* rho, double* ux, double* uy, double* t, double* f,
+                          double* g);
+void orc_oct_info(void* h, double* out13);
+void orc_oct_diag(void* h, double* out9);
+
 #ifdef __cplusplus
 }
 #endif
