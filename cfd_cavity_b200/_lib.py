@@ -91,6 +91,7 @@ class CavOctreeParams(ctypes.Structure):
         ("levels", ctypes.c_int32), ("nu_start_mult", ctypes.c_double),
         ("has_nu_override", ctypes.c_int32), ("nu_override", ctypes.c_double),
         ("precision", ctypes.c_int32), ("device", ctypes.c_int32),
+        ("cs", ctypes.c_double), ("pr_t", ctypes.c_double),
     ]
 
 
@@ -183,6 +184,8 @@ def load(path: str | None = None):
         "cav_octree_get_level": (i32, [vp, i32, _dp, _dp, _dp, _dp, _dp, _dp]),
         "cav_octree_set_level": (i32, [vp, i32, _dp, _dp, _dp, _dp, _dp, _dp]),
         "cav_octree_couple": (i32, [vp, i32]),
+        "cav_octree_restart_level": (i32, [vp, i32, _dp, _dp, _dp, _dp]),
+        "cav_octree_set_time_step": (i32, [vp, i64]),
         "cav_octree_diag": (i32, [vp, ctypes.POINTER(CavOctreeDiag)]),
         "cav_octree_check_guards": (i32, [vp, ctypes.c_double]),
         "cav_octree_sync": (i32, [vp]),

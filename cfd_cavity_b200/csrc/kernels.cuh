@@ -53,6 +53,14 @@ __device__ __forceinline__ void store_node(St* __restrict__ dst, const Geom& G, 
     }
 }
 
+// Programmatic dependent launch: a kernel launched with the programmatic
+// stream-serialisation attribute may start while its predecessor finishes;
+// it must not touch global memory before pdl_wait() (which returns once the
+// predecessor grid has completed and its writes are visible; a no-op without
+// the attribute).  pdl_trigger() lets the successor launch early.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 static __global__ void k_set_step(long long* p, long long v) { *p = v; }
 static __global__ void k_add_step(long long* p, long long d) { *p += d; }
 
@@ -185,6 +193,8 @@ __global__ void __launch_bounds__(256) k_fused(const St* __restrict__ src, St* _
                                                typename Fmt<St>::A* __restrict__ nut, double* __restrict__ acc_hot,
                                                double* __restrict__ acc_cold, Geom G,
                                                StepScalars<typename Fmt<St>::A> c) {
+    pdl_wait();
+    pdl_trigger();
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iy = blockIdx.y * blockDim.y + threadIdx.y;
     if (ix >= G.nx || iy >= G.ny) return;

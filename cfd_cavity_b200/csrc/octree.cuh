@@ -48,6 +48,9 @@ struct LvlScal {
     A a_f, b_f, a_g, c_m, c_p;           // reference (FP64) form
     A om_p, om_m, om_g, k_p, k_m;        // pairwise (FP32) form
     A beta;
+    // fixed-Cs Smagorinsky on the level (an extension: the reference octree
+    // has none; cs = 0 is the reference)
+    A cs, nu, alpha, tau_s, inv_tau_s, pr_t, inv_pr_t;
 };
 template <class A>
 struct OctScal {
@@ -107,6 +110,24 @@ __device__ __forceinline__ const OctScal<A>& row_of(const OctScal<A>* tab, int S
 template <class A, bool SHIFT>
 __device__ __forceinline__ void oct_collide(A (&f)[Q], A (&g)[Q], const Macro<A, SHIFT>& m, const LvlScal<A>& c,
                                             A& fy_out) {
+    if (c.cs != A(0.0)) {
+        // with the Smagorinsky extension: the uniform solver's collision
+        // (collide_node, src/uniform/solver.rs:1054-1185) with the level's
+        // molecular nu / alpha and lattice spacing 1
+        StepScalars<A> u{};
+        u.tau_s = c.tau_s;
+        u.beta = c.beta;
+        u.nu = c.nu;
+        u.alpha = c.alpha;
+        u.cs = c.cs;
+        u.pr_t = c.pr_t;
+        u.inv_tau_s = c.inv_tau_s;
+        u.inv_pr_t = c.inv_pr_t;
+        u.geq_order = 2;
+        A nut;
+        collide_node<A, SHIFT>(f, g, m, u, fy_out, nut);
+        return;
+    }
     if constexpr (!SHIFT) {
         const double r = m.rho, u = m.ux, v = m.uy, temp = m.t;
         const double fyv = r * c.beta * 1.0 * (temp - 0.0);
@@ -723,6 +744,8 @@ struct Octree {
                            const double* f, const double* g) = 0;
     virtual void diag(double* out10) = 0;
     virtual void debug_phase(int phase) = 0;
+    virtual void restart_level(int lvl, const double* rho, const double* ux, const double* uy, const double* t) = 0;
+    virtual void set_time_step(int64_t t) = 0;
     virtual void sync() = 0;
 
     cav_octree_params p{};
@@ -896,7 +919,7 @@ struct OctImpl final : Octree {
     }
 
     // RelaxTimes::from_nu_alpha (lbm.rs:90-98) + collision coefficients.
-    static LvlScal<A> lvl_scal(double nu_l, double al_l, double beta) {
+    LvlScal<A> lvl_scal(double nu_l, double al_l, double beta) const {
         const double tp = 0.5 + 3.0 * nu_l;
         const double tm = 0.5 + LAMBDA_TRT / (tp - 0.5);
         const double tt = 0.5 + 3.0 * al_l;
@@ -912,6 +935,14 @@ struct OctImpl final : Octree {
         c.k_p = A(1.0 - 0.5 / tp);
         c.k_m = A(1.0 - 0.5 / tm);
         c.beta = A(beta);
+        const double ts = 0.5 + 3.0 * std::fmax(nu_l, 0.002 / 3.0);
+        c.cs = A(p.cs);
+        c.nu = A(nu_l);
+        c.alpha = A(al_l);
+        c.tau_s = A(ts);
+        c.inv_tau_s = A(1.0 / ts);
+        c.pr_t = A(p.pr_t);
+        c.inv_pr_t = A(1.0 / p.pr_t);
         return c;
     }
 
@@ -941,6 +972,7 @@ struct OctImpl final : Octree {
         if ((long long)p.nx0 * p.ny0 * NPLANES >= (1ll << 31) || (long long)p.ny0 * 4 * (2 * p.bl_width + 3) * NPLANES >= (1ll << 31))
             throw ArgError{CAV_ERR_ARG, "grid too large for 32-bit plane offsets"};
         if (!(p.ra > 0 && p.pr > 0 && p.utarget > 0)) throw ArgError{CAV_ERR_ARG, "ra, pr, utarget must be > 0"};
+        if (!(p.cs >= 0.0 && p.cs < 1.0) || !(p.pr_t > 0.0)) throw ArgError{CAV_ERR_ARG, "cs in [0, 1), pr_t > 0"};
         levels = p.levels;
         nx0 = p.nx0;
         ny0 = p.ny0;
@@ -1349,6 +1381,51 @@ struct OctImpl final : Octree {
         if (lvl == 1 || lvl == 2) return upload_state(L1[lvl - 1], r, u, v, t, f, g);
         if (levels == 3 && (lvl == 3 || lvl == 4)) return upload_state(L2[lvl - 3], r, u, v, t, f, g);
         throw ArgError{CAV_ERR_ARG, "no such level"};
+    }
+
+    // set_from_snapshot's per-level injection (src/octree/solver.rs:1113-1153):
+    // fields as given, f = feq(rho, u), g = geq(T, u), then the level's
+    // no-slip on the stored velocity (the populations keep the given u).
+    void restart_level(int lvl, const double* r, const double* u, const double* v, const double* t) override {
+        CK(cudaStreamSynchronize(stream));
+        int nx, ny, hot = 0, cold = 0;
+        bool coarse = lvl == 0;
+        if (lvl == 0) {
+            nx = nx0;
+            ny = ny0;
+        } else if (lvl == 1 || lvl == 2) {
+            nx = nx1;
+            ny = ny1;
+            hot = lvl == 1;
+            cold = lvl == 2;
+        } else if (levels == 3 && (lvl == 3 || lvl == 4)) {
+            nx = nx2;
+            ny = ny2;
+            hot = lvl == 3;
+            cold = lvl == 4;
+        } else {
+            throw ArgError{CAV_ERR_ARG, "no such level"};
+        }
+        const size_t n = size_t(nx) * ny;
+        std::vector<double> f(n * Q), g(n * Q), uu(u, u + n), vv(v, v + n);
+        for (size_t k = 0; k < n; ++k)
+            for (int i = 0; i < Q; ++i) {
+                f[k * Q + i] = feq_full<double>(i, r[k], u[k], v[k]);
+                g[k * Q + i] = geq_full<double>(i, t[k], u[k], v[k], 2);
+            }
+        for (int b = 0; b < ny; ++b)
+            for (int a = 0; a < nx; ++a) {
+                const bool wall = coarse ? (a == 0 || a == nx - 1 || b == 0 || b == ny - 1)
+                                         : ((hot && a == 1) || (cold && a == nx - 2) || b == 1 || b == ny - 2);
+                if (wall) uu[size_t(b) * nx + a] = vv[size_t(b) * nx + a] = 0.0;
+            }
+        set_level(lvl, r, uu.data(), vv.data(), t, f.data(), g.data());
+    }
+
+    void set_time_step(int64_t t) override {
+        if (t < 0) throw ArgError{CAV_ERR_ARG, "negative time step"};
+        time_step = t;
+        pc_valid = false;
     }
 
     // Single couplings on the current state (for the interface tests):

@@ -62,6 +62,8 @@ int cav_octree_default_params(cav_octree_params* p) {
     p->nu_start_mult = 1.0;
     p->precision = CAV_OCT_F64;
     p->device = 0;
+    p->cs = 0.0;
+    p->pr_t = 0.9;
     return CAV_OK;
 }
 
@@ -166,6 +168,22 @@ int cav_octree_set_level(cav_octree* h, int32_t level, const double* rho, const 
                          const double* t, const double* f, const double* g) {
     return oguarded(h, [&](Octree& o) {
         o.set_level(level, rho, ux, uy, t, f, g);
+        return CAV_OK;
+    });
+}
+
+int cav_octree_restart_level(cav_octree* h, int32_t level, const double* rho, const double* ux, const double* uy,
+                             const double* t) {
+    if (!rho || !ux || !uy || !t) return ofail(h, CAV_ERR_ARG, "null field");
+    return oguarded(h, [&](Octree& o) {
+        o.restart_level(level, rho, ux, uy, t);
+        return CAV_OK;
+    });
+}
+
+int cav_octree_set_time_step(cav_octree* h, int64_t t) {
+    return oguarded(h, [&](Octree& o) {
+        o.set_time_step(t);
         return CAV_OK;
     });
 }

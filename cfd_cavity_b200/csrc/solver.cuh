@@ -345,6 +345,24 @@ struct Impl final : Solver {
     }
 
     // ---- the step loop -----------------------------------------------------------
+    // k_fused with programmatic dependent launch: successive fused steps
+    // overlap the next launch with the tail of the previous one.
+    template <bool WN, bool ACC>
+    void launch_fused_pdl(const StepScalars<A>& c) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = grd;
+        cfg.blockDim = blk;
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CK(cudaLaunchKernelEx(&cfg, k_fused<St, WN, ACC, false>, (const St*)pop[cur], pop[cur ^ 1], fy, nut,
+                              acc_hot, acc_cold, G, c));
+    }
+
     void launch_fused(int64_t s, bool write_nut, bool acc, const long long* sdev = nullptr, int64_t off = 0) {
         StepScalars<A> c = scalars(s);
         if (sdev) {
@@ -353,18 +371,14 @@ struct Impl final : Solver {
         }
         if (write_nut) {
             if (acc)
-                k_fused<St, true, true, false><<<grd, blk, 0, stream>>>(pop[cur], pop[cur ^ 1], fy, nut, acc_hot,
-                                                                         acc_cold, G, c);
+                launch_fused_pdl<true, true>(c);
             else
-                k_fused<St, true, false, false><<<grd, blk, 0, stream>>>(pop[cur], pop[cur ^ 1], fy, nut, acc_hot,
-                                                                          acc_cold, G, c);
+                launch_fused_pdl<true, false>(c);
         } else {
             if (acc)
-                k_fused<St, false, true, false><<<grd, blk, 0, stream>>>(pop[cur], pop[cur ^ 1], fy, nut, acc_hot,
-                                                                          acc_cold, G, c);
+                launch_fused_pdl<false, true>(c);
             else
-                k_fused<St, false, false, false><<<grd, blk, 0, stream>>>(pop[cur], pop[cur ^ 1], fy, nut, acc_hot,
-                                                                           acc_cold, G, c);
+                launch_fused_pdl<false, false>(c);
         }
         check_launch();
         cur ^= 1;

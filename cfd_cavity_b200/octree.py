@@ -25,7 +25,8 @@ def _dp(a):
 
 class OctreeSolver:
     def __init__(self, nx0, ny0, bl_width, ra, pr, utarget, seed, jobs=1, odd_exact=False, levels=2,
-                 nu_start_mult=1.0, nu_override=None, *, precision="f64", device=0):
+                 nu_start_mult=1.0, nu_override=None, *, precision="f64", device=0, cs=0.0,
+                 pr_t=0.9):
         lib = L.load()
         p = L.CavOctreeParams()
         L.check_octree(lib.cav_octree_default_params(ctypes.byref(p)))
@@ -36,6 +37,7 @@ class OctreeSolver:
         p.nu_override = 0.0 if nu_override is None else float(nu_override)
         p.precision = L.OCT_PRECISIONS[precision] if isinstance(precision, str) else int(precision)
         p.device = device
+        p.cs, p.pr_t = cs, pr_t
         h = ctypes.c_void_p()
         L.check_octree(lib.cav_octree_create(ctypes.byref(p), ctypes.byref(h)))
         self._h = h
@@ -98,6 +100,23 @@ class OctreeSolver:
             return a
         arrs = [c(a) for a in (rho, ux, uy, temp, f, g)]
         self._ck(L.load().cav_octree_set_level(self._h, lvl, *[_dp(a) for a in arrs]))
+
+    def set_time_step(self, t):
+        self._ck(L.load().cav_octree_set_time_step(self._h, int(t)))
+
+    def restart_from(self, other: "OctreeSolver"):
+        """``set_from_snapshot`` (src/octree/solver.rs:1080-1168) from another
+        solver with the same layout: every level restarts at the equilibrium
+        of the other's fields, then the time step (and the ramps) restart at 0."""
+        n = 3 if self.levels == 2 else 5
+        if other.levels != self.levels or other.info()["nx"] != self.info()["nx"] \
+                or other.info()["ny"] != self.info()["ny"]:
+            raise ValueError("restart needs the same level layout")
+        for lvl in range(n):
+            d = other.level(lvl)
+            self._ck(L.load().cav_octree_restart_level(self._h, lvl, _dp(d["rho"]), _dp(d["ux"]),
+                                                       _dp(d["uy"]), _dp(d["temp"])))
+        self.set_time_step(0)
 
     def couple(self, which):
         """One coupling: 0 coarse_to_fine L0->L1, 1 fine_to_coarse L1->L0,

@@ -275,6 +275,11 @@ typedef struct cav_octree_params {
     double nu_override;
     int32_t precision;     /* CAV_OCT_*                                         */
     int32_t device;
+    /* Extension (no counterpart in the reference octree, which has no fixed
+     * Smagorinsky model): cs > 0 adds nu_t = cs^2 |S| on every level, with
+     * the uniform solver's collision and the level's lattice spacing.
+     * cs = 0 (default) is the reference. */
+    double cs, pr_t;
 } cav_octree_params;
 typedef struct cav_octree_info {
     double nu, alpha, beta_eff_coarse;
@@ -312,6 +317,14 @@ int cav_octree_get_level(cav_octree* h, int32_t level, double* rho, double* ux, 
  * starts with the collision of that state, as the reference's would. */
 int cav_octree_set_level(cav_octree* h, int32_t level, const double* rho, const double* ux,
                          const double* uy, const double* t, const double* f, const double* g);
+/* Restart injection of one level (set_from_snapshot, src/octree/solver.rs:
+ * 1080-1168, same grid): the level's fields become rho, ux, uy, t [nx*ny],
+ * its populations feq / geq of them, then its no-slip is applied to the
+ * stored velocity.  Call it for every level, then cav_octree_set_time_step(h,
+ * 0) as the reference does (the ramps restart). */
+int cav_octree_restart_level(cav_octree* h, int32_t level, const double* rho, const double* ux,
+                             const double* uy, const double* t);
+int cav_octree_set_time_step(cav_octree* h, int64_t t);
 /* One coupling on the current state: 0 = coarse_to_fine L0 -> L1,
  * 1 = fine_to_coarse L1 -> L0 + moment refresh, 2 / 3 = the same between L1
  * and L2 (src/octree/interface.rs:137-206). */

@@ -108,6 +108,9 @@ def lib():
         L.orc_oct_get_level.argtypes = [vp, i32, dp, dp, dp, dp, dp, dp]
         L.orc_oct_info.argtypes = [vp, dp]
         L.orc_oct_diag.argtypes = [vp, dp]
+        L.orc_oct_restart_level.restype = i32
+        L.orc_oct_restart_level.argtypes = [vp, i32, dp, dp, dp, dp]
+        L.orc_oct_set_time_step.argtypes = [vp, i64]
         _lib = L
     return _lib
 
@@ -383,6 +386,15 @@ class OracleOctree:
             out["f"], out["g"] = f, g
         out["nx"], out["ny"] = nx, ny
         return out
+
+    def restart_from(self, other):
+        """set_from_snapshot (src/octree/solver.rs:1080-1168) from another
+        octree of the same layout, then time_step = 0."""
+        for lvl in range(3 if self.levels == 2 else 5):
+            d = other.level(lvl)
+            lib().orc_oct_restart_level(self._h, lvl, _dp(d["rho"]), _dp(d["ux"]), _dp(d["uy"]),
+                                        _dp(d["temp"]))
+        lib().orc_oct_set_time_step(self._h, 0)
 
     def info(self):
         o = np.empty(len(OCT_INFO_KEYS))

@@ -91,6 +91,9 @@ int32_t orc_oct_level_dims(void* h, int32_t level, int32_t* nx, int32_t* ny);
 int32_t orc_oct_get_level(void* h, int32_t level, double* rho, double* ux, double* uy, double* t, double* f,
                           double* g);
 void orc_oct_info(void* h, double* out13);
+int32_t orc_oct_restart_level(void* h, int32_t level, const double* rho, const double* ux, const double* uy,
+                              const double* t);
+void orc_oct_set_time_step(void* h, int64_t t);
 void orc_oct_diag(void* h, double* out9);
 
 #ifdef __cplusplus

@@ -653,6 +653,33 @@ int32_t orc_oct_get_level(void* h, int32_t level, double* rho, double* ux, doubl
     return 0;
 }
 
+// set_from_snapshot's injection for one level (src/octree/solver.rs:1113-1153)
+// followed by that level's no-slip; orc_oct_set_time_step(h, 0) completes a restart.
+int32_t orc_oct_restart_level(void* h, int32_t level, const double* rho, const double* ux, const double* uy,
+                              const double* t) {
+    Octree* o = static_cast<Octree*>(h);
+    orc::oct::Level* l = o->level(level);
+    if (!l) return 1;
+    const size_t n = size_t(l->nx) * l->ny;
+    for (size_t k = 0; k < n; ++k) {
+        l->rho[k] = rho[k];
+        l->ux[k] = ux[k];
+        l->uy[k] = uy[k];
+        l->temp[k] = t[k];
+        for (int i = 0; i < orc::Q; ++i) {
+            l->f[k][i] = orc::feq<double>(i, rho[k], ux[k], uy[k]);
+            l->g[k][i] = orc::geq<double>(i, t[k], ux[k], uy[k], o->geq_order);
+        }
+    }
+    if (level == 0)
+        orc::oct::noslip(*l);
+    else
+        orc::oct::noslip_block(*l, level == 1 || level == 3, level == 2 || level == 4);
+    return 0;
+}
+
+void orc_oct_set_time_step(void* h, int64_t t) { static_cast<Octree*>(h)->time_step = t; }
+
 // out: nu (L0 lattice), alpha, beta_c, tau+ L0, tau+ L1, tau+ L2, xi_even A,
 // xi_odd A, xi_th A, xi_even B, time_step, coincident L0 count, ghost count.
 void orc_oct_info(void* h, double* out) {

@@ -119,3 +119,23 @@ def test_sweep_configs_follow_the_benchmark_ranges():
     assert {(c["nx"], c["ny"]) for c in cfg} == {(64, 256), (96, 384), (128, 512)}
     assert all(1e6 <= c["ra"] <= 1e8 and 0.08 <= c["cs"] <= 0.12 for c in cfg)
     assert cfg == sweep_configs(64, seed=2024)
+
+
+def test_octree_default_params_and_argument_checks():
+    """cav_octree_*: defaults (256x1024 base, the reference CLI's octree
+    options, src/cli.rs:94-130) and CavitySolver::new's assertions
+    (src/octree/solver.rs:298-303) as CAV_ERR_ARG before any CUDA call."""
+    lib = L.load()
+    p = L.CavOctreeParams()
+    assert lib.cav_octree_default_params(ctypes.byref(p)) == 0
+    assert (p.nx0, p.ny0, p.bl_width, p.levels, p.odd_exact) == (256, 1024, 16, 2, 0)
+    assert (p.ra, p.pr, p.utarget, p.seed, p.nu_start_mult) == (1e6, 0.71, 0.02, 42, 1.0)
+    assert (p.cs, p.pr_t, p.precision) == (0.0, 0.9, L.CAV_OCT_F64)
+    for field, bad in (("bl_width", 1), ("bl_width", 128), ("levels", 4), ("precision", 9), ("ny0", 3)):
+        q = L.CavOctreeParams()
+        lib.cav_octree_default_params(ctypes.byref(q))
+        setattr(q, field, bad)
+        h = ctypes.c_void_p()
+        assert lib.cav_octree_create(ctypes.byref(q), ctypes.byref(h)) == L.CAV_ERR_ARG, field
+        assert not h.value
+        assert lib.cav_octree_last_error(None)

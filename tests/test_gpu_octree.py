@@ -70,6 +70,29 @@ def test_fp64_bit_identical_variants(levels, odd_exact, nu_start_mult):
     assert gpu.time_step == 37
 
 
+def test_fp64_restart_bit_identical_to_oracle():
+    """set_from_snapshot (src/octree/solver.rs:1080-1168): a Ra = 1e7 octree
+    restarted from the fields of a Ra = 1e6 run of the same layout, then
+    stepped; every level bit-identical to the oracle doing the same."""
+    a_args = (32, 64, 4, 1.0e6, 0.71, 0.02, 42)
+    b_args = (32, 64, 4, 1.0e7, 0.71, 0.02, 9)
+    ga = OctreeSolver(*a_args, levels=3, precision="f64")
+    oa = oracle.OracleOctree(*a_args, levels=3)
+    ga.step_cavity(30)
+    oa.step_cavity(30)
+    gb = OctreeSolver(*b_args, levels=3, precision="f64")
+    ob = oracle.OracleOctree(*b_args, levels=3)
+    gb.step_cavity(5)
+    ob.step_cavity(5)
+    gb.restart_from(ga)
+    ob.restart_from(oa)
+    assert gb.time_step == 0
+    assert_levels_equal(gb, ob, 3)
+    gb.step_cavity(20)
+    ob.step_cavity(20)
+    assert_levels_equal(gb, ob, 3)
+
+
 def test_reference_octree_kats_on_gpu():
     """src/octree/tests.rs:397-580 on the GPU path (FP64 and FP32)."""
     for prec in ("f64", "f32", "f32_f16"):
