@@ -73,10 +73,8 @@ static __global__ void k_add_step(long long* p, long long d) { *p += d; }
 //  the domain, so the reference's "keep g at out-of-domain sources" value
 //  is always overwritten and never needed here.
 template <class St>
-__device__ __forceinline__ void pull_node(const St* __restrict__ src, const Geom& G, int ix, int iy,
-                                          const StepScalars<typename Fmt<St>::A>& c,
-                                          typename Fmt<St>::A (&f)[Q], typename Fmt<St>::A (&g)[Q]) {
-    using A = typename Fmt<St>::A;
+__device__ __forceinline__ void pull_f(const St* __restrict__ src, const Geom& G, int ix, int iy,
+                                       typename Fmt<St>::A (&f)[Q]) {
     // 32-bit element offsets: 18 * plane < 2^31 is checked at allocation.
     const int P = int(G.plane), W = G.pitch;
     const int k = iy * W + ix;
@@ -88,6 +86,14 @@ __device__ __forceinline__ void pull_node(const St* __restrict__ src, const Geom
         const int idx = ok ? i * P + k - cx - cy * W : OPP(i) * P + k;  // else bounce-back
         f[i] = Fmt<St>::load(src[idx], i);
     }
+}
+
+template <class St>
+__device__ __forceinline__ void pull_g(const St* __restrict__ src, const Geom& G, int ix, int iy,
+                                       const StepScalars<typename Fmt<St>::A>& c, typename Fmt<St>::A (&g)[Q]) {
+    using A = typename Fmt<St>::A;
+    const int P = int(G.plane), W = G.pitch;
+    const int k = iy * W + ix;
     const int gy = iy == 0 ? 1 : (iy == G.ny - 1 ? G.ny - 2 : iy);
     const bool wall_col = (ix == 0) || (ix == G.nx - 1);
     const A tw = ix == 0 ? c.t_hot[gy] : c.t_cold;
@@ -99,6 +105,14 @@ __device__ __forceinline__ void pull_node(const St* __restrict__ src, const Geom
         const A v = Fmt<St>::load(src[idx], Q + i);
         g[i] = wall_col ? geq_rest<A>(i, tw, c.geq_order) : v;
     }
+}
+
+template <class St>
+__device__ __forceinline__ void pull_node(const St* __restrict__ src, const Geom& G, int ix, int iy,
+                                          const StepScalars<typename Fmt<St>::A>& c,
+                                          typename Fmt<St>::A (&f)[Q], typename Fmt<St>::A (&g)[Q]) {
+    pull_f<St>(src, G, ix, iy, f);
+    pull_g<St>(src, G, ix, iy, c, g);
 }
 
 // Temperature of node (ix, iy) of the streamed state, gathered from a PC

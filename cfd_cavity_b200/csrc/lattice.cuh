@@ -276,17 +276,23 @@ struct Macro {
     A rho, drho, ux, uy, t, inv_rho;
 };
 
+template <class A>
+__device__ __forceinline__ A sum_g(const A (&g)[Q]) {
+    A tn = g[0];
+#pragma unroll
+    for (int j = 1; j < Q; ++j) tn = tn + g[j];
+    return tn;
+}
+
+// rho and u of the node (t left 0): the f part of macro_node.
 template <class A, bool SHIFT>
-__device__ __forceinline__ Macro<A, SHIFT> macro_node(const A (&f)[Q], const A (&g)[Q], A fy_prev, bool wall) {
+__device__ __forceinline__ Macro<A, SHIFT> macro_f(const A (&f)[Q], A fy_prev, bool wall) {
     Macro<A, SHIFT> m;
     A s = f[0];
 #pragma unroll
     for (int j = 1; j < Q; ++j) s = s + f[j];
     A un = ((((f[1] + f[3]) - f[4]) - f[5]) - f[7]) + f[8];
     A vn = ((((f[2] + f[3]) + f[4]) - f[6]) - f[7]) - f[8];
-    A tn = g[0];
-#pragma unroll
-    for (int j = 1; j < Q; ++j) tn = tn + g[j];
     A r;
     m.inv_rho = A(0.0);
     if (SHIFT) {
@@ -309,7 +315,14 @@ __device__ __forceinline__ Macro<A, SHIFT> macro_node(const A (&f)[Q], const A (
     m.rho = r;
     m.ux = wall ? A(0.0) : un;
     m.uy = wall ? A(0.0) : vn;
-    m.t = tn;
+    m.t = A(0.0);
+    return m;
+}
+
+template <class A, bool SHIFT>
+__device__ __forceinline__ Macro<A, SHIFT> macro_node(const A (&f)[Q], const A (&g)[Q], A fy_prev, bool wall) {
+    Macro<A, SHIFT> m = macro_f<A, SHIFT>(f, fy_prev, wall);
+    m.t = sum_g<A>(g);
     return m;
 }
 
@@ -320,27 +333,27 @@ __device__ __forceinline__ Macro<A, SHIFT> macro_node(const A (&f)[Q], const A (
 // FP64 follows the reference expression by expression; the FP32 variant
 // works on f_i - w_i and replaces divisions by constants with products.
 // ---------------------------------------------------------------------------
+// The collision in three parts: collide_f_pre (everything of f that does
+// not need T: non-equilibrium parts, pi_neq, nu_t, relaxation rates),
+// collide_f_post (the f update, with the Guo force rho beta T) and collide_g
+// (BGK of g, needs T, u and nu_t).  collide_node runs the three.
+template <class A>
+struct CollF {
+    A d[Q];                // FP64: f - feq
+    A d0, dS[5], dD[5];    // FP32: rest part, symmetric / antisymmetric pair parts
+    A nut, w1, w2, k1, k2; // FP64 a_f, b_f, k-, k+;  FP32 om+, om-, k+, k-
+};
+
 template <class A, bool SHIFT>
-__device__ __forceinline__ void collide_node(A (&f)[Q], A (&g)[Q], const Macro<A, SHIFT>& m,
-                                             const StepScalars<A>& c, A& fy_out, A& nut_out) {
-    const A r = m.rho, u = m.ux, v = m.uy, temp = m.t;
+__device__ __forceinline__ CollF<A> collide_f_pre(const A (&f)[Q], const Macro<A, SHIFT>& m, const StepScalars<A>& c) {
+    CollF<A> o;
+    const A r = m.rho, u = m.ux, v = m.uy;
     if constexpr (!SHIFT) {
         // ---- FP64: expression order of the reference ----------------------
         const double cs2 = CS2;
-        double fyv = r * c.beta * 1.0 * (temp - 0.0);
-        fy_out = fyv;
-        double f_eq[Q], g_eq[Q];
 #pragma unroll
-        for (int i = 0; i < Q; ++i) {
-            f_eq[i] = feq_full<double>(i, r, u, v);
-            g_eq[i] = geq_full<double>(i, temp, u, v, c.geq_order);
-        }
-        double d_f[Q], d_g[Q];
-#pragma unroll
-        for (int i = 0; i < Q; ++i) {
-            d_f[i] = f[i] - f_eq[i];
-            d_g[i] = g[i] - g_eq[i];
-        }
+        for (int i = 0; i < Q; ++i) o.d[i] = f[i] - feq_full<double>(i, r, u, v);
+        const double* d_f = o.d;
         // pi_neq, solver.rs:1096-1106 (terms with c = 0 add +-0).
         double pxx = ((((d_f[1] + d_f[3]) + d_f[4]) + d_f[5]) + d_f[7]) + d_f[8];
         double pxy = ((d_f[3] - d_f[4]) + d_f[7]) - d_f[8];
@@ -349,29 +362,13 @@ __device__ __forceinline__ void collide_node(A (&f)[Q], A (&g)[Q], const Macro<A
         double rho_m = r > 1e-12 ? r : 1e-12;
         double s_mag = sqrt(pi2) / (2.0 * cs2 * c.tau_s * rho_m);
         double nut = c.cs * c.cs * s_mag;
-        nut_out = nut;
+        o.nut = nut;
         double tau_plus = 0.5 + 3.0 * (c.nu + nut);
         double tau_minus = 0.5 + LAMBDA_TRT / (tau_plus - 0.5);
-        double alpha_t = nut / c.pr_t;
-        double tau_t_plus = 0.5 + 3.0 * (c.alpha + alpha_t);
-        double tau_t_minus = tau_t_plus;
-        double a_f = 0.5 * (1.0 / tau_plus + 1.0 / tau_minus);
-        double b_f = 0.5 * (1.0 / tau_plus - 1.0 / tau_minus);
-        double a_g = 0.5 * (1.0 / tau_t_plus + 1.0 / tau_t_minus);
-        double b_g = 0.5 * (1.0 / tau_t_plus - 1.0 / tau_t_minus);
-        double k_minus = 1.0 - 0.5 / tau_minus;
-        double k_plus = 1.0 - 0.5 / tau_plus;
-#pragma unroll
-        for (int i = 0; i < Q; ++i) {
-            const double cx = CX(i), cy = CY(i);
-            double ei_u = cx * u + cy * v;
-            double s_i = WD(i) * ((cy - v) / cs2 + ei_u * cy / (cs2 * cs2)) * fyv;
-            double s_minus = WD(i) * (cy / cs2) * fyv;
-            double s_plus = s_i - s_minus;
-            f[i] = f[i] + (-a_f * d_f[i] - b_f * d_f[OPP(i)] + k_minus * s_minus + k_plus * s_plus);
-        }
-#pragma unroll
-        for (int i = 0; i < Q; ++i) g[i] = g[i] + (-a_g * d_g[i] - b_g * d_g[OPP(i)]);
+        o.w1 = 0.5 * (1.0 / tau_plus + 1.0 / tau_minus);
+        o.w2 = 0.5 * (1.0 / tau_plus - 1.0 / tau_minus);
+        o.k1 = 1.0 - 0.5 / tau_minus;
+        o.k2 = 1.0 - 0.5 / tau_plus;
     } else {
         // ---- FP32 on h_i = f_i - w_i, pairwise (i, opp(i)) form --------------
         // For each pair p = (i, i+4), i = 1..4, split populations and
@@ -382,48 +379,92 @@ __device__ __forceinline__ void collide_node(A (&f)[Q], A (&g)[Q], const Macro<A
         //   E = -w+ (d_p + d_opp)/2 + k+ S+_p,  O = -w- (d_p - d_opp)/2 + k- S-_p,
         // and pi_neq only needs the symmetric parts.  Same arithmetic as the
         // reference up to rounding (FP32), a third of the operations.
-        const float fyv = r * c.beta * temp;
-        fy_out = fyv;
         const float u2 = u * u + v * v;
         const float inv_r = m.inv_rho;
-        // rest population
         const float feq0 = float(WD(0)) * (m.drho - 1.5f * r * u2);
-        const float d0 = f[0] - feq0;
-        float dS[5], dD[5], feS[5], feA[5];
+        o.d0 = f[0] - feq0;
 #pragma unroll
         for (int p = 1; p <= 4; ++p) {
             const float cx = CX(p), cy = CY(p);
             const float eu = cx * u + cy * v;
-            feS[p] = float(WD(p)) * (m.drho + r * (4.5f * eu * eu - 1.5f * u2));
-            feA[p] = float(WD(p)) * (r * 3.0f * eu);
-            dS[p] = (f[p] + f[p + 4]) - 2.0f * feS[p];
-            dD[p] = (f[p] - f[p + 4]) - 2.0f * feA[p];
+            const float feS = float(WD(p)) * (m.drho + r * (4.5f * eu * eu - 1.5f * u2));
+            const float feA = float(WD(p)) * (r * 3.0f * eu);
+            o.dS[p] = (f[p] + f[p + 4]) - 2.0f * feS;
+            o.dD[p] = (f[p] - f[p + 4]) - 2.0f * feA;
         }
         // pi_neq (solver.rs:1096-1106) from the symmetric parts.
-        const float pxx = dS[1] + dS[3] + dS[4];
-        const float pxy = dS[3] - dS[4];
-        const float pyy = dS[2] + dS[3] + dS[4];
+        const float pxx = o.dS[1] + o.dS[3] + o.dS[4];
+        const float pxy = o.dS[3] - o.dS[4];
+        const float pyy = o.dS[2] + o.dS[3] + o.dS[4];
         const float pi2 = pxx * pxx + 2.0f * pxy * pxy + pyy * pyy;
         // |S| = sqrt(pi:pi) / (2 cs^2 tau rho) = sqrt(pi:pi) * (1.5 / tau) / rho
         const float s_mag = __fsqrt_rn(pi2) * (1.5f * c.inv_tau_s) * inv_r;
         const float nut = c.cs * c.cs * s_mag;
-        nut_out = nut;
+        o.nut = nut;
         const float e = 3.0f * (c.nu + nut);             // tau+ - 1/2
-        const float om_p = __fdividef(1.0f, 0.5f + e);   // 1/tau+
-        const float om_m = __fdividef(e, 0.5f * e + float(LAMBDA_TRT));  // 1/tau-, tau- = 1/2 + Lambda/e
-        const float om_g = __fdividef(1.0f, 0.5f + 3.0f * (c.alpha + nut * c.inv_pr_t));  // BGK g
-        const float k_p = 1.0f - 0.5f * om_p, k_m = 1.0f - 0.5f * om_m;
+        o.w1 = __fdividef(1.0f, 0.5f + e);                // 1/tau+
+        o.w2 = __fdividef(e, 0.5f * e + float(LAMBDA_TRT));  // 1/tau-, tau- = 1/2 + Lambda/e
+        o.k1 = 1.0f - 0.5f * o.w1;
+        o.k2 = 1.0f - 0.5f * o.w2;
+    }
+    return o;
+}
+
+// The f update with the Guo force fy = rho beta (T - 0) (solver.rs:1084,
+// 1159-1179); returns fy.
+template <class A, bool SHIFT>
+__device__ __forceinline__ A collide_f_post(A (&f)[Q], const CollF<A>& o, const Macro<A, SHIFT>& m,
+                                            const StepScalars<A>& c, A temp) {
+    const A r = m.rho, u = m.ux, v = m.uy;
+    if constexpr (!SHIFT) {
+        const double cs2 = CS2;
+        const double fyv = r * c.beta * 1.0 * (temp - 0.0);
+        const double* d_f = o.d;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const double cx = CX(i), cy = CY(i);
+            double ei_u = cx * u + cy * v;
+            double s_i = WD(i) * ((cy - v) / cs2 + ei_u * cy / (cs2 * cs2)) * fyv;
+            double s_minus = WD(i) * (cy / cs2) * fyv;
+            double s_plus = s_i - s_minus;
+            f[i] = f[i] + (-o.w1 * d_f[i] - o.w2 * d_f[OPP(i)] + o.k1 * s_minus + o.k2 * s_plus);
+        }
+        return fyv;
+    } else {
+        const float fyv = r * c.beta * temp;
+        const float om_p = o.w1, om_m = o.w2, k_p = o.k1, k_m = o.k2;
         // Guo source: S+_p = w_p (-3 u_y + 9 (e.u) c_y) fy, S-_p = w_p 3 c_y fy.
-        f[0] = f[0] - om_p * d0 + k_p * float(WD(0)) * (-3.0f * v) * fyv;
+        f[0] = f[0] - om_p * o.d0 + k_p * float(WD(0)) * (-3.0f * v) * fyv;
 #pragma unroll
         for (int p = 1; p <= 4; ++p) {
             const float cx = CX(p), cy = CY(p);
             const float eu = cx * u + cy * v;
-            const float E = -0.5f * om_p * dS[p] + k_p * float(WD(p)) * (-3.0f * v + 9.0f * eu * cy) * fyv;
-            const float O = -0.5f * om_m * dD[p] + k_m * float(WD(p)) * (3.0f * cy) * fyv;
+            const float E = -0.5f * om_p * o.dS[p] + k_p * float(WD(p)) * (-3.0f * v + 9.0f * eu * cy) * fyv;
+            const float O = -0.5f * om_m * o.dD[p] + k_m * float(WD(p)) * (3.0f * cy) * fyv;
             f[p] = f[p] + (E + O);
             f[p + 4] = f[p + 4] + (E - O);
         }
+        return fyv;
+    }
+}
+
+// BGK collision of g (solver.rs:1136-1144, 1181-1184).
+template <class A, bool SHIFT>
+__device__ __forceinline__ void collide_g(A (&g)[Q], A temp, A u, A v, A nut, const StepScalars<A>& c) {
+    if constexpr (!SHIFT) {
+        double d_g[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) d_g[i] = g[i] - geq_full<double>(i, temp, u, v, c.geq_order);
+        double alpha_t = nut / c.pr_t;
+        double tau_t_plus = 0.5 + 3.0 * (c.alpha + alpha_t);
+        double tau_t_minus = tau_t_plus;
+        double a_g = 0.5 * (1.0 / tau_t_plus + 1.0 / tau_t_minus);
+        double b_g = 0.5 * (1.0 / tau_t_plus - 1.0 / tau_t_minus);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) g[i] = g[i] + (-a_g * d_g[i] - b_g * d_g[OPP(i)]);
+    } else {
+        const float u2 = u * u + v * v;
+        const float om_g = __fdividef(1.0f, 0.5f + 3.0f * (c.alpha + nut * c.inv_pr_t));  // BGK g
         // g: BGK towards geq (quadratic or linear in u).
         const float one_m = 1.0f - om_g;
         const float q2 = c.geq_order == 1 ? 0.0f : 1.0f;
@@ -438,6 +479,22 @@ __device__ __forceinline__ void collide_node(A (&f)[Q], A (&g)[Q], const Macro<A
             g[p + 4] = one_m * g[p + 4] + (gS - gA);
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Collision of one node: TRT + Smagorinsky + Guo forcing for f, BGK for g
+// (collide_node, src/uniform/solver.rs:1054-1185, fixed-Cs branch).
+// f and g are updated in place; returns fy and nu_t.
+// FP64 follows the reference expression by expression; the FP32 variant
+// works on f_i - w_i and replaces divisions by constants with products.
+// ---------------------------------------------------------------------------
+template <class A, bool SHIFT>
+__device__ __forceinline__ void collide_node(A (&f)[Q], A (&g)[Q], const Macro<A, SHIFT>& m,
+                                             const StepScalars<A>& c, A& fy_out, A& nut_out) {
+    const CollF<A> o = collide_f_pre<A, SHIFT>(f, m, c);
+    nut_out = o.nut;
+    fy_out = collide_f_post<A, SHIFT>(f, o, m, c, m.t);
+    collide_g<A, SHIFT>(g, m.t, m.ux, m.uy, o.nut, c);
 }
 
 // Wall-node equilibrium of g (apply_thermal_boundary_conditions,

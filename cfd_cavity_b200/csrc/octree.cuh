@@ -240,24 +240,48 @@ __device__ __forceinline__ void load_pops(const St* __restrict__ src, int n, int
 // wall_top = true): interior nodes only; a source in a wall-side ghost line
 // bounces back, a source in an interface ghost column is pulled from REF
 // (the injected value), any other source from PC.
+// The per-node neighbour classes are computed once (Src), so that each of
+// the 18 loads costs a select and an address; all loads are in flight
+// together.
 // ---------------------------------------------------------------------------
-template <class St, bool COARSE>
-__device__ __forceinline__ typename Fmt<St>::A pull_one(const LvlIO<St>& L, int x, int y, int q_plane, int i) {
-    // Branch-free: the source index, plane and buffer are selected, so the
-    // 9 (18) loads of a node are all in flight together.
-    const int sx = x - CX(i), sy = y - CY(i);
-    const int k = y * L.nx + x;
-    bool bb;
-    const St* base = L.pc_in;
+struct Src {
+    int k, nx;
+    bool bb_xm, bb_xp, bb_ym, bb_yp;  // source x-1 / x+1 / y-1 / y+1 bounces back
+    bool gh_xm, gh_xp;                // source x-1 / x+1 is an interface ghost (REF)
+};
+
+template <bool COARSE, class St>
+__device__ __forceinline__ Src src_of(const LvlIO<St>& L, int x, int y) {
+    Src r;
+    r.k = y * L.nx + x;
+    r.nx = L.nx;
     if constexpr (COARSE) {
-        bb = sx < 0 || sx >= L.nx || sy < 0 || sy >= L.ny;
+        r.bb_xm = x == 0;
+        r.bb_xp = x == L.nx - 1;
+        r.bb_ym = y == 0;
+        r.bb_yp = y == L.ny - 1;
+        r.gh_xm = r.gh_xp = false;
     } else {
-        bb = (sx == 0 && L.hot) || (sx == L.nx - 1 && L.cold) || sy == 0 || sy == L.ny - 1;
-        const bool ghost = !bb && (sx == 0 || sx == L.nx - 1);
-        base = ghost ? L.ref_in : L.pc_in;
+        r.bb_ym = y - 1 == 0;
+        r.bb_yp = y + 1 == L.ny - 1;
+        const bool xm_edge = x - 1 == 0, xp_edge = x + 1 == L.nx - 1;
+        r.bb_xm = xm_edge && L.hot;
+        r.bb_xp = xp_edge && L.cold;
+        r.gh_xm = xm_edge && !L.hot;
+        r.gh_xp = xp_edge && !L.cold;
     }
+    return r;
+}
+
+// Population q_plane (plane i of f, or Q + i of g) streamed into the node.
+template <class St>
+__device__ __forceinline__ typename Fmt<St>::A pull_one(const LvlIO<St>& L, const Src& r, int q_plane, int i) {
+    const int cx = CX(i), cy = CY(i);
+    const bool bb = (cx > 0 && r.bb_xm) || (cx < 0 && r.bb_xp) || (cy > 0 && r.bb_ym) || (cy < 0 && r.bb_yp);
+    const bool ghost = !bb && ((cx > 0 && r.gh_xm) || (cx < 0 && r.gh_xp));
+    const St* base = ghost ? L.ref_in : L.pc_in;
     const int qs = (bb && q_plane < Q) ? OPP(i) : q_plane;
-    const int ks = bb ? k : sy * L.nx + sx;
+    const int ks = bb ? r.k : r.k - cx - cy * r.nx;
     return Fmt<St>::load(base[qs * L.n + ks], qs);
 }
 
@@ -271,7 +295,7 @@ __device__ __forceinline__ typename Fmt<St>::A pull_one(const LvlIO<St>& L, int 
 // column clamped to 1..nx-2 and y'' the row clamped to 2..ny-3, or the wall
 // equilibrium when x' is a wall column.
 template <class St, bool COARSE>
-__device__ __forceinline__ void bc_g(const LvlIO<St>& L, int x, int y, typename Fmt<St>::A (&g)[Q]) {
+__device__ __forceinline__ void bc_g(const LvlIO<St>& L, int x, int y, const Src& own, typename Fmt<St>::A (&g)[Q]) {
     using A = typename Fmt<St>::A;
     int xs, ys;
     bool wall;
@@ -292,9 +316,16 @@ __device__ __forceinline__ void bc_g(const LvlIO<St>& L, int x, int y, typename 
 #pragma unroll
         for (int i = 0; i < Q; ++i) g[i] = geq_full<A>(i, tw, A(0.0), A(0.0), 2);
     } else {
+        const Src r = (xs == x && ys == y) ? own : src_of<COARSE>(L, xs, ys);
 #pragma unroll
-        for (int i = 0; i < Q; ++i) g[i] = pull_one<St, COARSE>(L, xs, ys, Q + i, i);
+        for (int i = 0; i < Q; ++i) g[i] = pull_one<St>(L, r, Q + i, i);
     }
+}
+
+// Row and column of node k of a level with nx columns (exact for k < 2^22).
+__device__ __forceinline__ void split_k(int k, int nx, float inv_nx, int& x, int& y) {
+    y = int((float(k) + 0.5f) * inv_nx);
+    x = k - y * nx;
 }
 
 // One (sub-)step of a level: pull + BC + macroscopic (update_macroscopic_guo,
@@ -303,27 +334,31 @@ __device__ __forceinline__ void bc_g(const LvlIO<St>& L, int x, int y, typename 
 template <class St, bool COARSE>
 __global__ void __launch_bounds__(OT) k_oct_step(LvlPair<St> P, const OctScal<typename Fmt<St>::A>* __restrict__ tab,
                                                  int S, const long long* __restrict__ step_dev, int off, int lvl,
-                                                 uint32_t seed, int phase) {
+                                                 uint32_t seed, int phase, float inv_nx) {
+    pdl_wait();
+    pdl_trigger();
     using A = typename Fmt<St>::A;
     constexpr bool SH = Fmt<St>::SHIFT;
-    const LvlIO<St>& L = P.b[blockIdx.y];
+    const LvlIO<St> L = P.b[blockIdx.y];
     const int k = blockIdx.x * OT + threadIdx.x;
     if (k >= L.n) return;
     // the step index and the collision constants first: the stores below
     // may alias them as far as the compiler knows
     long long s;
     const LvlScal<A> sc = row_of<A>(tab, S, step_dev, off, &s).l[lvl];
-    const int x = k % L.nx, y = k / L.nx;
+    int x, y;
+    split_k(k, L.nx, inv_nx, x, y);
     const bool ghost = !COARSE && (x == 0 || x == L.nx - 1 || y == 0 || y == L.ny - 1);
+    const Src own = src_of<COARSE>(L, x, y);
     A f[Q], g[Q];
     if (ghost) {
 #pragma unroll
         for (int i = 0; i < Q; ++i) f[i] = Fmt<St>::load(L.ref_in[i * L.n + k], i);
     } else {
 #pragma unroll
-        for (int i = 0; i < Q; ++i) f[i] = pull_one<St, COARSE>(L, x, y, i, i);
+        for (int i = 0; i < Q; ++i) f[i] = pull_one<St>(L, own, i, i);
     }
-    bc_g<St, COARSE>(L, x, y, g);
+    bc_g<St, COARSE>(L, x, y, own, g);
     bool wall;
     if constexpr (COARSE)
         wall = x == 0 || x == L.nx - 1 || y == 0 || y == L.ny - 1;
@@ -349,9 +384,11 @@ template <class St, bool COARSE>
 __global__ void __launch_bounds__(OT) k_oct_collide(LvlPair<St> P, const OctScal<typename Fmt<St>::A>* __restrict__ tab,
                                                     int S, const long long* __restrict__ step_dev, int lvl,
                                                     uint32_t seed, int phase) {
+    pdl_wait();
+    pdl_trigger();
     using A = typename Fmt<St>::A;
     constexpr bool SH = Fmt<St>::SHIFT;
-    const LvlIO<St>& L = P.b[blockIdx.y];
+    const LvlIO<St> L = P.b[blockIdx.y];
     const int k = blockIdx.x * OT + threadIdx.x;
     if (k >= L.n) return;
     const int x = k % L.nx, y = k / L.nx;
@@ -470,6 +507,8 @@ __global__ void __launch_bounds__(OT) k_oct_c2f(LvlPair<StC> C, LvlPair<StF> F,
                                                 const GhostE<typename Fmt<StF>::A>* __restrict__ tab, int n_ghost,
                                                 Xi<typename Fmt<StF>::A> xi, const long long* __restrict__ step_dev,
                                                 uint32_t seed, int phase) {
+    pdl_wait();
+    pdl_trigger();
     using A = typename Fmt<StF>::A;
     constexpr bool SH = Fmt<StF>::SHIFT;
     static_assert(Fmt<StC>::SHIFT == SH, "levels share one convention");
@@ -477,8 +516,8 @@ __global__ void __launch_bounds__(OT) k_oct_c2f(LvlPair<StC> C, LvlPair<StF> F,
     const int j = t >> 2, s = t & 3;
     if ((t & ~31) >= 4 * n_ghost) return;  // whole warp past the end
     const bool act = j < n_ghost;
-    const LvlIO<StC>& Lc = C.b[blockIdx.y];
-    const LvlIO<StF>& Lf = F.b[blockIdx.y];
+    const LvlIO<StC> Lc = C.b[blockIdx.y];
+    const LvlIO<StF> Lf = F.b[blockIdx.y];
     const long long key = *step_dev * 16 + phase;
     A c[NC];
     int kf = 0;
@@ -521,6 +560,8 @@ __global__ void __launch_bounds__(OT) k_oct_f2c(LvlPair<StF> F, LvlPair<StC> C, 
                                                 const OctScal<typename Fmt<StF>::A>* __restrict__ stab, int S,
                                                 const long long* __restrict__ step_dev, int off, int lvl_c,
                                                 uint32_t seed, int phase) {
+    pdl_wait();
+    pdl_trigger();
     using A = typename Fmt<StF>::A;
     constexpr bool SH = Fmt<StF>::SHIFT;
     const int t = blockIdx.x * OT + threadIdx.x;
@@ -529,8 +570,8 @@ __global__ void __launch_bounds__(OT) k_oct_f2c(LvlPair<StF> F, LvlPair<StC> C, 
     const int nb = blk == 0 ? n0 : n1;
     if ((t & ~31) >= 16 * nb) return;  // whole warp past the end
     const bool act_e = j < nb;
-    const LvlIO<StF>& Lf = F.b[blk];
-    const LvlIO<StC>& Lc = C.b[blk];
+    const LvlIO<StF> Lf = F.b[blk];
+    const LvlIO<StC> Lc = C.b[blk];
     CoinE e{0, 0, 0};
     if (act_e) e = tab[(blk == 0 ? 0 : n0) + j];
     long long sidx;
@@ -969,8 +1010,9 @@ struct OctImpl final : Octree {
         if (!(2 * p.bl_width < p.nx0)) throw ArgError{CAV_ERR_ARG, "2 * bl_width < nx0 required (coarse core)"};
         if (p.levels != 2 && p.levels != 3) throw ArgError{CAV_ERR_ARG, "levels must be 2 or 3"};
         if (p.ny0 < 4) throw ArgError{CAV_ERR_ARG, "ny0 >= 4 required"};
-        if ((long long)p.nx0 * p.ny0 * NPLANES >= (1ll << 31) || (long long)p.ny0 * 4 * (2 * p.bl_width + 3) * NPLANES >= (1ll << 31))
-            throw ArgError{CAV_ERR_ARG, "grid too large for 32-bit plane offsets"};
+        // node kernels split k into (x, y) in FP32 (exact below 2^22 nodes)
+        if ((long long)p.nx0 * p.ny0 >= (1ll << 22) || (long long)p.ny0 * 4 * (2 * p.bl_width + 3) >= (1ll << 22))
+            throw ArgError{CAV_ERR_ARG, "grid too large: every level must stay below 2^22 nodes"};
         if (!(p.ra > 0 && p.pr > 0 && p.utarget > 0)) throw ArgError{CAV_ERR_ARG, "ra, pr, utarget must be > 0"};
         if (!(p.cs >= 0.0 && p.cs < 1.0) || !(p.pr_t > 0.0)) throw ArgError{CAV_ERR_ARG, "cs in [0, 1), pr_t > 0"};
         levels = p.levels;
@@ -1231,6 +1273,24 @@ struct OctImpl final : Octree {
     }
     static dim3 grid_of(int n, int nb) { return dim3((n + OT - 1) / OT, nb); }
 
+    // Launch with programmatic dependent launch (the kernels start with
+    // pdl_wait(), so a launch overlaps only the tail of its predecessor).
+    template <typename... KArgs, typename... Args>
+    void launch(void (*kern)(KArgs...), dim3 grid, Args... args) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = grid;
+        cfg.blockDim = dim3(OT);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CK(cudaLaunchKernelEx(&cfg, kern, args...));
+        check_launch();
+    }
+
     void set_step_dev() {
         if (step_dev_val != time_step) {
             k_set_step<<<1, 1, 0, stream>>>(step_dev, time_step);
@@ -1244,18 +1304,18 @@ struct OctImpl final : Octree {
         set_step_dev();
         {
             LvlPair<StC> q = pair_cur(L0, L0);
-            k_oct_collide<StC, true><<<grid_of(L0.n, 1), OT, 0, stream>>>(q, tab, S, step_dev, 0, seed32, 10);
-            check_launch();
+            launch(k_oct_collide<StC, true>, grid_of(L0.n, 1), q, (const OctScal<A>*)tab, S,
+                   (const long long*)step_dev, 0, seed32, 10);
         }
         {
             LvlPair<StF> q = pair_cur(L1[0], L1[1]);
-            k_oct_collide<StF, false><<<grid_of(L1[0].n, 2), OT, 0, stream>>>(q, tab, S, step_dev, 1, seed32, 11);
-            check_launch();
+            launch(k_oct_collide<StF, false>, grid_of(L1[0].n, 2), q, (const OctScal<A>*)tab, S,
+                   (const long long*)step_dev, 1, seed32, 11);
         }
         if (levels == 3) {
             LvlPair<StF> q = pair_cur(L2[0], L2[1]);
-            k_oct_collide<StF, false><<<grid_of(L2[0].n, 2), OT, 0, stream>>>(q, tab, S, step_dev, 2, seed32, 12);
-            check_launch();
+            launch(k_oct_collide<StF, false>, grid_of(L2[0].n, 2), q, (const OctScal<A>*)tab, S,
+                   (const long long*)step_dev, 2, seed32, 12);
         }
         pc_valid = true;
     }
@@ -1263,46 +1323,44 @@ struct OctImpl final : Octree {
     void c2f_L1() {
         LvlPair<StC> c = pair_cur(L0, L0);
         LvlPair<StF> f = pair_cur(L1[0], L1[1]);
-        k_oct_c2f<StC, StF><<<grid_of(4 * n_ghost, 2), OT, 0, stream>>>(c, f, gh1, n_ghost, xa, step_dev, seed32, 2);
-        check_launch();
+        launch(k_oct_c2f<StC, StF>, grid_of(4 * n_ghost, 2), c, f, (const GhostE<A>*)gh1, n_ghost, xa,
+               (const long long*)step_dev, seed32, 2);
     }
     void c2f_L2() {
         LvlPair<StF> c = pair_cur(L1[0], L1[1]);
         LvlPair<StF> f = pair_cur(L2[0], L2[1]);
-        k_oct_c2f<StF, StF><<<grid_of(4 * n_ghost2, 2), OT, 0, stream>>>(c, f, gh2, n_ghost2, xb, step_dev, seed32, 4);
-        check_launch();
+        launch(k_oct_c2f<StF, StF>, grid_of(4 * n_ghost2, 2), c, f, (const GhostE<A>*)gh2, n_ghost2, xb,
+               (const long long*)step_dev, seed32, 4);
     }
     void f2c_L2(int off) {
         LvlPair<StF> f = pair_cur(L2[0], L2[1]);
         LvlPair<StF> c = pair_cur(L1[0], L1[1]);
-        k_oct_f2c<StF, StF><<<grid_of(16 * std::max(n_co2_0, n_co2_1), 2), OT, 0, stream>>>(
-            f, c, co2, n_co2_0, n_co2_1, xb, tab, S, step_dev, off, 1, seed32, 7);
-        check_launch();
+        launch(k_oct_f2c<StF, StF>, grid_of(16 * std::max(n_co2_0, n_co2_1), 2), f, c, (const CoinE*)co2, n_co2_0,
+               n_co2_1, xb, (const OctScal<A>*)tab, S, (const long long*)step_dev, off, 1, seed32, 7);
     }
     void f2c_L1(int off) {
         LvlPair<StF> f = pair_cur(L1[0], L1[1]);
         LvlPair<StC> c = pair_cur(L0, L0);
-        k_oct_f2c<StF, StC><<<grid_of(16 * std::max(n_co0, n_co1), 2), OT, 0, stream>>>(
-            f, c, co1, n_co0, n_co1, xa, tab, S, step_dev, off, 0, seed32, 13);
-        check_launch();
+        launch(k_oct_f2c<StF, StC>, grid_of(16 * std::max(n_co0, n_co1), 2), f, c, (const CoinE*)co1, n_co0, n_co1,
+               xa, (const OctScal<A>*)tab, S, (const long long*)step_dev, off, 0, seed32, 13);
     }
     void step_L0() {
         LvlPair<StC> q = pair(L0, L0);
-        k_oct_step<StC, true><<<grid_of(L0.n, 1), OT, 0, stream>>>(q, tab, S, step_dev, 1, 0, seed32, 1);
-        check_launch();
+        launch(k_oct_step<StC, true>, grid_of(L0.n, 1), q, (const OctScal<A>*)tab, S, (const long long*)step_dev, 1,
+               0, seed32, 1, 1.0f / float(L0.nx));
         L0.cur ^= 1;
     }
     void step_L1(int off, int phase) {
         LvlPair<StF> q = pair(L1[0], L1[1]);
-        k_oct_step<StF, false><<<grid_of(L1[0].n, 2), OT, 0, stream>>>(q, tab, S, step_dev, off, 1, seed32, phase);
-        check_launch();
+        launch(k_oct_step<StF, false>, grid_of(L1[0].n, 2), q, (const OctScal<A>*)tab, S,
+               (const long long*)step_dev, off, 1, seed32, phase, 1.0f / float(L1[0].nx));
         L1[0].cur ^= 1;
         L1[1].cur ^= 1;
     }
     void step_L2(int off, int phase) {
         LvlPair<StF> q = pair(L2[0], L2[1]);
-        k_oct_step<StF, false><<<grid_of(L2[0].n, 2), OT, 0, stream>>>(q, tab, S, step_dev, off, 2, seed32, phase);
-        check_launch();
+        launch(k_oct_step<StF, false>, grid_of(L2[0].n, 2), q, (const OctScal<A>*)tab, S,
+               (const long long*)step_dev, off, 2, seed32, phase, 1.0f / float(L2[0].nx));
         L2[0].cur ^= 1;
         L2[1].cur ^= 1;
     }
