@@ -274,6 +274,32 @@ def octree_c5(dev, chain=(30_000, 30_000, 60_000), window=40_000, sample_every=1
     return out
 
 
+def octree_only(coarse_steps):
+    """C5 octree timing alone: a few warm-up coarse steps, then
+    `coarse_steps` timed with CUDA events on the octree's stream."""
+    import torch
+
+    from cfd_cavity_b200.octree import OctreeSolver
+
+    s = OctreeSolver(256, 1024, 16, 1e10, 0.71, 0.02, 42, levels=3, precision="f32_f16")
+    s.step_cavity(3)
+    st = torch.cuda.ExternalStream(s.stream_handle(), device=0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(st):
+        e0.record(st)
+    s.step_cavity(coarse_steps)
+    with torch.cuda.stream(st):
+        e1.record(st)
+    e1.synchronize()
+    d = s.diag()
+    print(json.dumps({"workload": "octree 256x1024 bl16 levels 3 Ra=1e10 f32_f16",
+                      "coarse_steps": coarse_steps,
+                      "us_per_coarse_step": e0.elapsed_time(e1) * 1e3 / coarse_steps,
+                      "finite": d["finite"]}), flush=True)
+    s.close()
+    return 0
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -318,8 +344,13 @@ def main():
     ap.add_argument("--chunk", type=int, default=CHUNK)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched-sweep and FP32 extras")
+    ap.add_argument("--octree-only", type=int, default=0, metavar="COARSE_STEPS",
+                    help="only time COARSE_STEPS octree coarse steps of the 256x1024 levels-3 cavity "
+                         "(FP32 / binary16) and print their device time (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.octree_only:
+        return octree_only(args.octree_only)
     world, rank, local, dist = dist_setup(args)
     if args.impl == "reference":
         rc = run_reference(args, world, rank, dist)

@@ -712,34 +712,56 @@ __global__ void __launch_bounds__(256) k_oct_iface(const A* mac_f0, const A* mac
     }
 }
 
+// Per-row terms of the Nusselt and y+ estimators, one thread per row, into
+// rows[5][R] (summed in row order by k_oct_final).
+template <class A>
+__global__ void __launch_bounds__(256) k_oct_rows(const A* __restrict__ mac0, int nx0, int ny0,
+                                                  const A* __restrict__ mac_h1, int nx1, int ny1,
+                                                  const A* __restrict__ mac_fin, int nxf, int nyf, double nu_fin,
+                                                  double* __restrict__ rows, int R) {
+    const int r = blockIdx.x * 256 + threadIdx.x;
+    if (r < ny0) {
+        const A* T0 = mac0 + 3 * (size_t)nx0 * ny0;
+        const double t0 = T0[r * nx0], t1 = T0[r * nx0 + 1], t2 = T0[r * nx0 + 2];
+        const double tc2 = T0[r * nx0 + nx0 - 2], tc3 = T0[r * nx0 + nx0 - 3];
+        rows[r] = fabs(t1 - t2);
+        rows[R + r] = fabs(t1 - t0);
+        rows[2 * R + r] = fabs(tc2 - tc3);
+    }
+    if (r >= 1 && r < ny1 - 1) {
+        const A* T1 = mac_h1 + 3 * (size_t)nx1 * ny1;
+        rows[3 * R + r] = fabs(double(T1[r * nx1 + 1]) - double(T1[r * nx1 + 2])) * 2.0;
+    }
+    if (r >= 2 && r < nyf - 2) {
+        const A* Uy = mac_fin + 2 * (size_t)nxf * nyf;
+        const double tw = nu_fin * fabs(double(Uy[r * nxf + 2]) - double(Uy[r * nxf + 1]));
+        rows[4 * R + r] = 0.5 * sqrt(fmax(tw, 0.0)) / nu_fin;
+    }
+}
+
 // Final reduction.  out: nu_hot, nu_hot_link0, nu_cold (nusselt_hot /
 // nusselt_hot_link0 / nusselt_cold, src/octree/cavity.rs:672-715, Lx
 // scale), nu_hot_fine (:728-741), max_u, mass (mean coarse rho), max_rho_dev,
 // max_rho_dev_ifaces, finite, y_plus (post.rs:182-199 formula on the finest
 // hot-wall level: wall column 1, first fluid column 2, rows 2..ny-3).
-template <class A, bool SHIFT>
-__global__ void k_oct_final(const A* __restrict__ mac0, int nx0, int ny0, const A* __restrict__ mac_h1, int nx1,
-                            int ny1, const A* __restrict__ mac_fin, int nxf, int nyf, double nu_fin,
+// Row sums in row order, as the reference.
+template <bool SHIFT>
+__global__ void k_oct_final(const double* __restrict__ rows, int R, int nx0, int ny0, int ny1, int nyf, int n0,
                             const double* __restrict__ part, int n_views, int n_ctas,
                             const double* __restrict__ iface, int n_iface, double* __restrict__ out) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const int n0 = nx0 * ny0;
-    const A* T0 = mac0 + 3 * (size_t)n0;
     double sh = 0.0, s0 = 0.0, sc = 0.0;
     for (int iy = 0; iy < ny0; ++iy) {
-        const double t0 = T0[iy * nx0], t1 = T0[iy * nx0 + 1], t2 = T0[iy * nx0 + 2];
-        const double tc2 = T0[iy * nx0 + nx0 - 2], tc3 = T0[iy * nx0 + nx0 - 3];
-        sh += fabs(t1 - t2);
-        s0 += fabs(t1 - t0);
-        sc += fabs(tc2 - tc3);
+        sh += rows[iy];
+        s0 += rows[R + iy];
+        sc += rows[2 * R + iy];
     }
     const double lx = double(nx0 - 1);
     out[0] = sh / double(ny0) * lx / 1.0;
     out[1] = s0 / double(ny0) * lx / 1.0;
     out[2] = sc / double(ny0) * lx / 1.0;
-    const A* T1 = mac_h1 + 3 * (size_t)nx1 * ny1;
     double sf = 0.0;
-    for (int b = 1; b < ny1 - 1; ++b) sf += fabs(double(T1[b * nx1 + 1]) - double(T1[b * nx1 + 2])) * 2.0;
+    for (int b = 1; b < ny1 - 1; ++b) sf += rows[3 * R + b];
     out[3] = sf / double(ny1 - 2) * lx / 1.0;
     double mn = 1e300, mx = -1e300, mu = 0.0, nf = 0.0, sum0 = 0.0;
     for (int v = 0; v < n_views; ++v)
@@ -762,12 +784,8 @@ __global__ void k_oct_final(const A* __restrict__ mac0, int nx0, int ny0, const 
     }
     out[7] = fmax(imx - rb, rb - imn);
     out[8] = nf == 0.0 ? 1.0 : 0.0;
-    const A* Uy = mac_fin + 2 * (size_t)nxf * nyf;
     double sy = 0.0;
-    for (int b = 2; b < nyf - 2; ++b) {
-        const double tw = nu_fin * fabs(double(Uy[b * nxf + 2]) - double(Uy[b * nxf + 1]));
-        sy += 0.5 * sqrt(fmax(tw, 0.0)) / nu_fin;
-    }
+    for (int b = 2; b < nyf - 2; ++b) sy += rows[4 * R + b];
     out[9] = sy / double(nyf - 4);
 }
 
@@ -910,6 +928,7 @@ struct OctImpl final : Octree {
     double* part = nullptr;
     double* iface = nullptr;
     double* dout = nullptr;
+    double* rowbuf = nullptr;
     uint32_t seed32 = 0;
     bool pc_valid = false;
     Xi<A> xa{}, xb{};
@@ -1135,6 +1154,7 @@ struct OctImpl final : Octree {
         part = dalloc<double>(size_t(5) * OSTAT_CTAS * OSTAT);
         iface = dalloc<double>(8);
         dout = dalloc<double>(16);
+        rowbuf = dalloc<double>(size_t(5) * std::max(std::max(ny0, ny1), levels == 3 ? ny2 : 0));
         CK(cudaStreamSynchronize(stream));
         init_cavity();
     }
@@ -1523,8 +1543,12 @@ struct OctImpl final : Octree {
         const A* mf = l3 ? L2[0].mac : L1[0].mac;
         const int nxf = l3 ? nx2 : nx1, nyf = l3 ? ny2 : ny1;
         const double nu_f = (l3 ? 4.0 : 2.0) * nu;
-        k_oct_final<A, SH><<<1, 32, 0, stream>>>(L0.mac, nx0, ny0, L1[0].mac, nx1, ny1, mf, nxf, nyf, nu_f, part, nv,
-                                                 OSTAT_CTAS, iface, n_if, dout);
+        const int R = std::max(std::max(ny0, ny1), nyf);
+        k_oct_rows<A><<<(R + 255) / 256, 256, 0, stream>>>(L0.mac, nx0, ny0, L1[0].mac, nx1, ny1, mf, nxf, nyf, nu_f,
+                                                          rowbuf, R);
+        check_launch();
+        k_oct_final<SH><<<1, 32, 0, stream>>>(rowbuf, R, nx0, ny0, ny1, nyf, nx0 * ny0, part, nv, OSTAT_CTAS, iface, n_if,
+                                              dout);
         check_launch();
         CK(cudaMemcpyAsync(out, dout, sizeof(double) * 10, cudaMemcpyDeviceToHost, stream));
         CK(cudaStreamSynchronize(stream));
