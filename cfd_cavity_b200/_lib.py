@@ -159,6 +159,8 @@ def load(path: str | None = None):
         "cav_sync": (i32, [vp]),
         "cav_get_stream": (i32, [vp, ctypes.POINTER(vp)]),
         "cav_launch_count": (i32, [vp, ctypes.POINTER(i64)]),
+        "cav_set_dynamic_sgs": (i32, [vp, i32, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
+        "cav_dynamic_sgs_stats": (i32, [vp, _dp]),
         "cav_adjoint_run": (i32, [vp, ctypes.POINTER(CavAdjointSpec), _dp,
                                   ctypes.POINTER(CavAdjointResult)]),
         "cav_batch_create": (i32, [pp, i32, ctypes.POINTER(vp)]),

@@ -298,6 +298,15 @@ int cav_get_stream(cav_handle* h, void** stream) {
     return guarded(h, [&](Solver& s) { *stream = (void*)s.stream; });
 }
 
+int cav_set_dynamic_sgs(cav_handle* h, int32_t on, double smag_alpha, double nu_sm_min, double eta_test) {
+    return guarded(h, [&](Solver& s) { s.set_dynamic_sgs(on != 0, smag_alpha, nu_sm_min, eta_test); });
+}
+
+int cav_dynamic_sgs_stats(cav_handle* h, double* out4) {
+    if (!out4) return fail(h, CAV_ERR_ARG, "null output");
+    return guarded(h, [&](Solver& s) { s.dynamic_stats(out4); });
+}
+
 int cav_launch_count(cav_handle* h, int64_t* n) {
     if (!n) return fail(h, CAV_ERR_ARG, "null output");
     return guarded(h, [&](Solver& s) { *n = s.launches; });

@@ -226,7 +226,9 @@ __global__ void __launch_bounds__(256) k_collide_ref(const St* __restrict__ src,
                                                      const typename Fmt<St>::A* __restrict__ tt,
                                                      typename Fmt<St>::A* __restrict__ fy,
                                                      typename Fmt<St>::A* __restrict__ nut, Geom G,
-                                                     StepScalars<typename Fmt<St>::A> c) {
+                                                     StepScalars<typename Fmt<St>::A> c,
+                                                     const typename Fmt<St>::A* __restrict__ nut_pre = nullptr,
+                                                     const typename Fmt<St>::A* __restrict__ at_pre = nullptr) {
     using A = typename Fmt<St>::A;
     constexpr bool SH = Fmt<St>::SHIFT;
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
@@ -247,7 +249,7 @@ __global__ void __launch_bounds__(256) k_collide_ref(const St* __restrict__ src,
     m.uy = uy[k];
     m.t = tt[k];
     A fyv, nutv;
-    collide_node<A, SH>(f, g, m, c, fyv, nutv);
+    collide_node<A, SH>(f, g, m, c, fyv, nutv, nut_pre ? nut_pre + k : nullptr, at_pre ? at_pre + k : nullptr);
     fy[k] = fyv;
     nut[k] = nutv;
     store_node<St>(dst, G, iy, ix, f, g, c);

@@ -344,8 +344,11 @@ struct CollF {
     A nut, w1, w2, k1, k2; // FP64 a_f, b_f, k-, k+;  FP32 om+, om-, k+, k-
 };
 
+// nut_ovr: nu_t given per node (the dynamic subgrid model, solver.rs:1118-1121)
+// instead of Cs^2 |S|.
 template <class A, bool SHIFT>
-__device__ __forceinline__ CollF<A> collide_f_pre(const A (&f)[Q], const Macro<A, SHIFT>& m, const StepScalars<A>& c) {
+__device__ __forceinline__ CollF<A> collide_f_pre(const A (&f)[Q], const Macro<A, SHIFT>& m, const StepScalars<A>& c,
+                                                  const A* nut_ovr = nullptr) {
     CollF<A> o;
     const A r = m.rho, u = m.ux, v = m.uy;
     if constexpr (!SHIFT) {
@@ -361,7 +364,7 @@ __device__ __forceinline__ CollF<A> collide_f_pre(const A (&f)[Q], const Macro<A
         double pi2 = pxx * pxx + 2.0 * pxy * pxy + pyy * pyy;
         double rho_m = r > 1e-12 ? r : 1e-12;
         double s_mag = sqrt(pi2) / (2.0 * cs2 * c.tau_s * rho_m);
-        double nut = c.cs * c.cs * s_mag;
+        double nut = nut_ovr ? double(*nut_ovr) : c.cs * c.cs * s_mag;
         o.nut = nut;
         double tau_plus = 0.5 + 3.0 * (c.nu + nut);
         double tau_minus = 0.5 + LAMBDA_TRT / (tau_plus - 0.5);
@@ -399,7 +402,7 @@ __device__ __forceinline__ CollF<A> collide_f_pre(const A (&f)[Q], const Macro<A
         const float pi2 = pxx * pxx + 2.0f * pxy * pxy + pyy * pyy;
         // |S| = sqrt(pi:pi) / (2 cs^2 tau rho) = sqrt(pi:pi) * (1.5 / tau) / rho
         const float s_mag = __fsqrt_rn(pi2) * (1.5f * c.inv_tau_s) * inv_r;
-        const float nut = c.cs * c.cs * s_mag;
+        const float nut = nut_ovr ? float(*nut_ovr) : c.cs * c.cs * s_mag;
         o.nut = nut;
         const float e = 3.0f * (c.nu + nut);             // tau+ - 1/2
         o.w1 = __fdividef(1.0f, 0.5f + e);                // 1/tau+
@@ -448,14 +451,16 @@ __device__ __forceinline__ A collide_f_post(A (&f)[Q], const CollF<A>& o, const 
     }
 }
 
-// BGK collision of g (solver.rs:1136-1144, 1181-1184).
+// BGK collision of g (solver.rs:1136-1144, 1181-1184); at_ovr: alpha_t given
+// per node (dynamic subgrid model) instead of nu_t / Pr_t.
 template <class A, bool SHIFT>
-__device__ __forceinline__ void collide_g(A (&g)[Q], A temp, A u, A v, A nut, const StepScalars<A>& c) {
+__device__ __forceinline__ void collide_g(A (&g)[Q], A temp, A u, A v, A nut, const StepScalars<A>& c,
+                                          const A* at_ovr = nullptr) {
     if constexpr (!SHIFT) {
         double d_g[Q];
 #pragma unroll
         for (int i = 0; i < Q; ++i) d_g[i] = g[i] - geq_full<double>(i, temp, u, v, c.geq_order);
-        double alpha_t = nut / c.pr_t;
+        double alpha_t = at_ovr ? double(*at_ovr) : nut / c.pr_t;
         double tau_t_plus = 0.5 + 3.0 * (c.alpha + alpha_t);
         double tau_t_minus = tau_t_plus;
         double a_g = 0.5 * (1.0 / tau_t_plus + 1.0 / tau_t_minus);
@@ -464,7 +469,8 @@ __device__ __forceinline__ void collide_g(A (&g)[Q], A temp, A u, A v, A nut, co
         for (int i = 0; i < Q; ++i) g[i] = g[i] + (-a_g * d_g[i] - b_g * d_g[OPP(i)]);
     } else {
         const float u2 = u * u + v * v;
-        const float om_g = __fdividef(1.0f, 0.5f + 3.0f * (c.alpha + nut * c.inv_pr_t));  // BGK g
+        const float alpha_t = at_ovr ? float(*at_ovr) : nut * c.inv_pr_t;
+        const float om_g = __fdividef(1.0f, 0.5f + 3.0f * (c.alpha + alpha_t));  // BGK g
         // g: BGK towards geq (quadratic or linear in u).
         const float one_m = 1.0f - om_g;
         const float q2 = c.geq_order == 1 ? 0.0f : 1.0f;
@@ -490,11 +496,12 @@ __device__ __forceinline__ void collide_g(A (&g)[Q], A temp, A u, A v, A nut, co
 // ---------------------------------------------------------------------------
 template <class A, bool SHIFT>
 __device__ __forceinline__ void collide_node(A (&f)[Q], A (&g)[Q], const Macro<A, SHIFT>& m,
-                                             const StepScalars<A>& c, A& fy_out, A& nut_out) {
-    const CollF<A> o = collide_f_pre<A, SHIFT>(f, m, c);
+                                             const StepScalars<A>& c, A& fy_out, A& nut_out,
+                                             const A* nut_ovr = nullptr, const A* at_ovr = nullptr) {
+    const CollF<A> o = collide_f_pre<A, SHIFT>(f, m, c, nut_ovr);
     nut_out = o.nut;
     fy_out = collide_f_post<A, SHIFT>(f, o, m, c, m.t);
-    collide_g<A, SHIFT>(g, m.t, m.ux, m.uy, o.nut, c);
+    collide_g<A, SHIFT>(g, m.t, m.ux, m.uy, o.nut, c, at_ovr);
 }
 
 // Wall-node equilibrium of g (apply_thermal_boundary_conditions,

@@ -203,10 +203,13 @@ __device__ __forceinline__ A feq_st(int i, A rho0, A ux, A uy) {
     }
 }
 
-template <class St>
-__device__ __forceinline__ void store_pops(St* __restrict__ dst, int n, int k, const typename Fmt<St>::A (&f)[Q],
-                                          const typename Fmt<St>::A (&g)[Q], bool sr, uint32_t seed, long long key,
-                                          long long node) {
+// Stores the 18 populations of node k (stochastic rounding when `sr` and
+// the format rounds stochastically).  With BACK, f and g are replaced by the
+// stored (rounded) values, computed in registers rather than re-read.
+template <class St, bool BACK = false>
+__device__ __forceinline__ void store_pops(St* __restrict__ dst, int n, int k, typename Fmt<St>::A (&f)[Q],
+                                           typename Fmt<St>::A (&g)[Q], bool sr, uint32_t seed, long long key,
+                                           long long node) {
     if constexpr (Fmt<St>::SR) {
         if (sr) {
             NodeRng rng(seed, key, node);
@@ -215,13 +218,21 @@ __device__ __forceinline__ void store_pops(St* __restrict__ dst, int n, int k, c
             for (int q = 0; q < NPLANES; ++q) {
                 if ((q & 1) == 0) r = rng.next();
                 const uint32_t bits = (q & 1) == 0 ? (r & 0xffff0000u) : (r << 16);
-                dst[q * n + k] = Fmt<St>::store_sr(q < Q ? f[q] : g[q - Q], q, bits);
+                typename Fmt<St>::A& x = q < Q ? f[q] : g[q - Q];
+                const St v = Fmt<St>::store_sr(x, q, bits);
+                dst[q * n + k] = v;
+                if (BACK) x = Fmt<St>::load(v, q);
             }
             return;
         }
     }
 #pragma unroll
-    for (int q = 0; q < NPLANES; ++q) dst[q * n + k] = Fmt<St>::store(q < Q ? f[q] : g[q - Q], q, RN_BITS);
+    for (int q = 0; q < NPLANES; ++q) {
+        typename Fmt<St>::A& x = q < Q ? f[q] : g[q - Q];
+        const St v = Fmt<St>::store(x, q, RN_BITS);
+        dst[q * n + k] = v;
+        if (BACK) x = Fmt<St>::load(v, q);
+    }
 }
 
 template <class St>
@@ -541,8 +552,7 @@ __global__ void __launch_bounds__(OT) k_oct_c2f(LvlPair<StC> C, LvlPair<StF> F,
         f[i] = feq_st<A, SH>(i, rho, ux, uy) + fr[i];
         g[i] = geq_full<A>(i, tt, ux, uy, 2) + xi.th * c[13 + i];
     }
-    store_pops<StF>(Lf.ref_out, Lf.n, kf, f, g, true, seed, key, (long long)Lf.node_off + kf);
-    if constexpr (!std::is_same<StF, A>::value) load_pops<StF>(Lf.ref_out, Lf.n, kf, f, g);
+    store_pops<StF, true>(Lf.ref_out, Lf.n, kf, f, g, true, seed, key, (long long)Lf.node_off + kf);
     const Macro<A, SH> m = refresh<A, SH, false>(f, g);
     Lf.mac[kf] = SH ? m.drho : m.rho;
     Lf.mac[Lf.n + kf] = m.ux;
@@ -552,8 +562,9 @@ __global__ void __launch_bounds__(OT) k_oct_c2f(LvlPair<StC> C, LvlPair<StF> F,
 
 // fine_to_coarse (src/octree/interface.rs:175-206) + refresh of the
 // coincident node (src/octree/solver.rs:874-876, 936-942) + that node's next
-// collision into the coarser level's PC.  Sixteen lanes per coincident node,
-// nine of them on the 3 x 3 stencil.
+// collision into the coarser level's PC.  Four lanes per coincident node
+// (eight nodes per warp): lane l takes the stencil nodes l, l + 4 (and 8 for
+// lane 0) in three rounds, and the round sums are added in stencil order.
 template <class StF, class StC>
 __global__ void __launch_bounds__(OT) k_oct_f2c(LvlPair<StF> F, LvlPair<StC> C, const CoinE* __restrict__ tab, int n0,
                                                 int n1, Xi<typename Fmt<StF>::A> xi,
@@ -565,10 +576,10 @@ __global__ void __launch_bounds__(OT) k_oct_f2c(LvlPair<StF> F, LvlPair<StC> C, 
     using A = typename Fmt<StF>::A;
     constexpr bool SH = Fmt<StF>::SHIFT;
     const int t = blockIdx.x * OT + threadIdx.x;
-    const int j = t >> 4, s = t & 15;
+    const int j = t >> 2, l = t & 3;
     const int blk = blockIdx.y;
     const int nb = blk == 0 ? n0 : n1;
-    if ((t & ~31) >= 16 * nb) return;  // whole warp past the end
+    if ((t & ~31) >= 4 * nb) return;  // whole warp past the end
     const bool act_e = j < nb;
     const LvlIO<StF> Lf = F.b[blk];
     const LvlIO<StC> Lc = C.b[blk];
@@ -576,18 +587,34 @@ __global__ void __launch_bounds__(OT) k_oct_f2c(LvlPair<StF> F, LvlPair<StC> C, 
     if (act_e) e = tab[(blk == 0 ? 0 : n0) + j];
     long long sidx;
     const LvlScal<A> sc = row_of<A>(stab, S, step_dev, off, &sidx).l[lvl_c];
+    const int base = (threadIdx.x & 31) & ~3;
+    const A ww[3] = {A(0.25), A(0.5), A(0.25)};
     A c[NC];
-    if (act_e && s < 9) {
-        const int jb = s / 3, ja = s - 3 * jb;
-        const A ww[3] = {A(0.25), A(0.5), A(0.25)};
-        const int kf = (e.b + jb - 1) * Lf.nx + (e.a + ja - 1);
-        stencil_term<StF>(Lf, kf, ww[ja] * ww[jb], c);
-    } else {
 #pragma unroll
-        for (int m = 0; m < NC; ++m) c[m] = A(0.0);
+    for (int m = 0; m < NC; ++m) c[m] = A(0.0);
+#pragma unroll
+    for (int round = 0; round < 3; ++round) {
+        const int st = 4 * round + l;  // this lane's stencil node in this round
+        A term[NC];
+        if (act_e && st < 9) {
+            const int jb = st / 3, ja = st - 3 * jb;
+            const int kf = (e.b + jb - 1) * Lf.nx + (e.a + ja - 1);
+            stencil_term<StF>(Lf, kf, ww[ja] * ww[jb], term);
+        } else {
+#pragma unroll
+            for (int m = 0; m < NC; ++m) term[m] = A(0.0);
+        }
+        const int nl = round < 2 ? 4 : 1;  // stencil nodes 0..3, 4..7, 8
+#pragma unroll
+        for (int m = 0; m < NC; ++m)
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (q < nl) {
+                    const A v = __shfl_sync(0xffffffffu, term[m], base + q);
+                    c[m] = (round == 0 && q == 0) ? v : c[m] + v;
+                }
     }
-    group_sum<A, 16, 9>(c);
-    if (!act_e || s != 0) return;
+    if (!act_e || l != 0) return;
     const A rho = c[0], ux = c[1], uy = c[2], tt = c[3];
     A fn[Q], fr[Q], f[Q], g[Q];
 #pragma unroll
@@ -601,8 +628,7 @@ __global__ void __launch_bounds__(OT) k_oct_f2c(LvlPair<StF> F, LvlPair<StC> C, 
         else
             g[i] = geq_full<A>(i, tt, ux, uy, 2) + c[13 + i] / xi.th;
     }
-    store_pops<StC>(Lc.ref_out, Lc.n, e.kc, f, g, true, seed, sidx * 16 + phase, (long long)Lc.node_off + e.kc);
-    if constexpr (!std::is_same<StC, A>::value) load_pops<StC>(Lc.ref_out, Lc.n, e.kc, f, g);
+    store_pops<StC, true>(Lc.ref_out, Lc.n, e.kc, f, g, true, seed, sidx * 16 + phase, (long long)Lc.node_off + e.kc);
     const Macro<A, SH> m = refresh<A, SH, true>(f, g);
     Lc.mac[e.kc] = SH ? m.drho : m.rho;
     Lc.mac[Lc.n + e.kc] = m.ux;
@@ -745,23 +771,39 @@ __global__ void __launch_bounds__(256) k_oct_rows(const A* __restrict__ mac0, in
 // max_rho_dev_ifaces, finite, y_plus (post.rs:182-199 formula on the finest
 // hot-wall level: wall column 1, first fluid column 2, rows 2..ny-3).
 // Row sums in row order, as the reference.
+// Sum of a[lo..hi) in index order, computed by a whole warp: coalesced
+// loads of 32 values, then every lane adds them one by one.
+__device__ __forceinline__ double warp_ordered_sum(const double* __restrict__ a, int lo, int hi) {
+    const int lane = threadIdx.x & 31;
+    double s = 0.0;
+    bool first = true;
+    for (int b = lo; b < hi; b += 32) {
+        const double v = b + lane < hi ? a[b + lane] : 0.0;
+        const int nv = hi - b < 32 ? hi - b : 32;
+        for (int j = 0; j < nv; ++j) {
+            const double x = __shfl_sync(0xffffffffu, v, j);
+            s = first ? x : s + x;
+            first = false;
+        }
+    }
+    return s;
+}
+
 template <bool SHIFT>
 __global__ void k_oct_final(const double* __restrict__ rows, int R, int nx0, int ny0, int ny1, int nyf, int n0,
                             const double* __restrict__ part, int n_views, int n_ctas,
                             const double* __restrict__ iface, int n_iface, double* __restrict__ out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double sh = 0.0, s0 = 0.0, sc = 0.0;
-    for (int iy = 0; iy < ny0; ++iy) {
-        sh += rows[iy];
-        s0 += rows[R + iy];
-        sc += rows[2 * R + iy];
-    }
+    // one warp; FP64 row sums in row order (bit-identical to the reference's loops)
+    const double sh = warp_ordered_sum(rows, 0, ny0);
+    const double s0 = warp_ordered_sum(rows + R, 0, ny0);
+    const double sc = warp_ordered_sum(rows + 2 * R, 0, ny0);
+    const double sf = warp_ordered_sum(rows + 3 * R, 1, ny1 - 1);
+    const double sy = warp_ordered_sum(rows + 4 * R, 2, nyf - 2);
+    if (threadIdx.x != 0) return;
     const double lx = double(nx0 - 1);
     out[0] = sh / double(ny0) * lx / 1.0;
     out[1] = s0 / double(ny0) * lx / 1.0;
     out[2] = sc / double(ny0) * lx / 1.0;
-    double sf = 0.0;
-    for (int b = 1; b < ny1 - 1; ++b) sf += rows[3 * R + b];
     out[3] = sf / double(ny1 - 2) * lx / 1.0;
     double mn = 1e300, mx = -1e300, mu = 0.0, nf = 0.0, sum0 = 0.0;
     for (int v = 0; v < n_views; ++v)
@@ -784,8 +826,6 @@ __global__ void k_oct_final(const double* __restrict__ rows, int R, int nx0, int
     }
     out[7] = fmax(imx - rb, rb - imn);
     out[8] = nf == 0.0 ? 1.0 : 0.0;
-    double sy = 0.0;
-    for (int b = 2; b < nyf - 2; ++b) sy += rows[4 * R + b];
     out[9] = sy / double(nyf - 4);
 }
 
@@ -1355,13 +1395,13 @@ struct OctImpl final : Octree {
     void f2c_L2(int off) {
         LvlPair<StF> f = pair_cur(L2[0], L2[1]);
         LvlPair<StF> c = pair_cur(L1[0], L1[1]);
-        launch(k_oct_f2c<StF, StF>, grid_of(16 * std::max(n_co2_0, n_co2_1), 2), f, c, (const CoinE*)co2, n_co2_0,
+        launch(k_oct_f2c<StF, StF>, grid_of(4 * std::max(n_co2_0, n_co2_1), 2), f, c, (const CoinE*)co2, n_co2_0,
                n_co2_1, xb, (const OctScal<A>*)tab, S, (const long long*)step_dev, off, 1, seed32, 7);
     }
     void f2c_L1(int off) {
         LvlPair<StF> f = pair_cur(L1[0], L1[1]);
         LvlPair<StC> c = pair_cur(L0, L0);
-        launch(k_oct_f2c<StF, StC>, grid_of(16 * std::max(n_co0, n_co1), 2), f, c, (const CoinE*)co1, n_co0, n_co1,
+        launch(k_oct_f2c<StF, StC>, grid_of(4 * std::max(n_co0, n_co1), 2), f, c, (const CoinE*)co1, n_co0, n_co1,
                xa, (const OctScal<A>*)tab, S, (const long long*)step_dev, off, 0, seed32, 13);
     }
     void step_L0() {

@@ -35,6 +35,7 @@
 #include "adjoint.cuh"
 #include "diag.cuh"
 #include "kernels.cuh"
+#include "sgs.cuh"
 
 namespace cav {
 
@@ -127,6 +128,12 @@ struct Solver {
     // sweep; see Impl::adjoint_run.  out[0] = J, out[1] = dJ/dCs,
     // out[2] = forward ms, out[3] = reverse ms, out[4] = checkpoints.
     virtual void adjoint_run(int64_t n_steps, int64_t ws, int ck_every, double* grad_theta, double* out) = 0;
+    // set_dynamic_sgs (src/uniform/solver.rs:215-220) and the model's
+    // coefficient statistics (cs_dyn_mean, cs_dyn_max, kappa_dyn_mean,
+    // kappa_dyn_max) of the last step.
+    virtual void set_dynamic_sgs(bool on, double smag_alpha, double nu_sm_min, double eta_test) = 0;
+    virtual void dynamic_stats(double* out4) = 0;
+    bool dyn = false;
 
     cav_params p{};
     Units U{};
@@ -162,13 +169,19 @@ struct Impl final : Solver {
     bool ref_cached = false; // PC form with a materialized REF copy in pop[cur ^ 1]
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     dim3 blk{BX, BY}, grd{};
+    // dynamic subgrid model
+    double dyn_alpha = 0.5, dyn_min = -0.1, dyn_eta = 2.0;
+    double* sgs_w = nullptr;       // S_NPLANES FP64 work planes
+    A *nut_pre = nullptr, *at_pre = nullptr;
+    double* sgs_out = nullptr;     // 4 statistics
+    bool sgs_valid = false;        // the work planes hold the last step's coefficients
 
     ~Impl() override {
         for (auto& row : graph)
             for (auto& gx : row)
                 if (gx) cudaGraphExecDestroy(gx);
         void* bufs[] = {pop[0], pop[1], rho, ux, uy, tt, fy, nut, t_hot_d, acc_hot, acc_cold,
-                        partials, diag_out, sums, aos, step_dev};
+                        partials, diag_out, sums, aos, step_dev, sgs_w, nut_pre, at_pre, sgs_out};
         for (void* b : bufs)
             if (b) cudaFree(b);
         if (stream && own_stream) cudaStreamDestroy(stream);
@@ -402,8 +415,85 @@ struct Impl final : Solver {
         return gx;
     }
 
+    void set_dynamic_sgs(bool on, double smag_alpha, double nu_sm_min, double eta_test) override {
+        if (!(smag_alpha >= 0.0 && smag_alpha <= 1.0) || !(eta_test >= 1.0) || !std::isfinite(nu_sm_min))
+            throw ArgError{CAV_ERR_ARG, "dynamic SGS: smag_alpha in [0, 1], eta_test >= 1, finite nu_sm_min"};
+        dyn = on;
+        dyn_alpha = smag_alpha;
+        dyn_min = nu_sm_min;
+        dyn_eta = eta_test;
+        if (on && !sgs_w) {
+            CK(cudaMalloc(&sgs_w, sizeof(double) * S_NPLANES * field_elems()));
+            CK(cudaMemsetAsync(sgs_w, 0, sizeof(double) * S_NPLANES * field_elems(), stream));
+            CK(cudaMalloc(&nut_pre, sizeof(A) * field_elems()));
+            CK(cudaMalloc(&at_pre, sizeof(A) * field_elems()));
+            CK(cudaMalloc(&sgs_out, sizeof(double) * 4));
+        }
+        sgs_valid = false;
+    }
+
+    void dynamic_stats(double* out4) override {
+        if (!sgs_valid) {
+            for (int i = 0; i < 4; ++i) out4[i] = 0.0;
+            return;
+        }
+        k_sgs_stats<<<1, 256, 0, stream>>>(sgs_w, G, sgs_out);
+        check_launch();
+        CK(cudaMemcpyAsync(out4, sgs_out, sizeof(double) * 4, cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+    }
+
+    // One step with the dynamic model, in the reference's order
+    // (src/uniform/solver.rs:279-291): compute_dynamic_sgs on the REF state,
+    // collide with the per-node nu_t / alpha_t, then stream + BC + macro +
+    // no-slip back to a REF state.
+    void dyn_step() {
+        to_ref_form();
+        double nu_eff = U.nu;
+        if (time_step < spin_up) {
+            const double x = double(time_step) / double(spin_up);
+            const double nu_start = U.nu * nu_start_mult;
+            nu_eff = nu_start * std::pow(U.nu / nu_start, x);
+        }
+        SgsParams sp;
+        const double eta = std::max(dyn_eta, 1.0);
+        sp.width = std::max((int)std::llround(eta), 1);
+        sp.dtest = eta * 1.0;
+        sp.alpha_exp = dyn_alpha;
+        sp.tau_s = 0.5 + 3.0 * std::fmax(nu_eff, 0.002 / 3.0);
+        sp.nu_mol = U.nu;
+        sp.alpha_mol = U.alpha;
+        sp.nu_sm_min = dyn_min;
+        k_sgs_a<A><<<grd, blk, 0, stream>>>(ux, uy, tt, sgs_w, G, sp);
+        check_launch();
+        k_sgs_b<St><<<grd, blk, 0, stream>>>(pop[cur], rho, ux, uy, tt, sgs_w, G, sp);
+        check_launch();
+        k_sgs_c<<<grd, blk, 0, stream>>>(sgs_w, G, sp);
+        check_launch();
+        k_sgs_d<A><<<grd, blk, 0, stream>>>(sgs_w, nut_pre, at_pre, G, sp);
+        check_launch();
+        sgs_valid = true;
+        k_collide_ref<St><<<grd, blk, 0, stream>>>(pop[cur], pop[cur ^ 1], rho, ux, uy, tt, fy, nut, G,
+                                                   scalars(time_step), nut_pre, at_pre);
+        check_launch();
+        cur ^= 1;
+        pc_form = true;
+        ref_cached = false;
+        to_ref_form();
+        time_step += 1;
+        if (acc_on) {
+            k_acc_nu_ref<A><<<(p.ny + 127) / 128, 128, 0, stream>>>(tt, acc_hot, acc_cold, G);
+            check_launch();
+            n_acc += 1;
+        }
+    }
+
     void step(int64_t n) override {
         if (n <= 0) return;
+        if (dyn) {
+            for (int64_t j = 0; j < n; ++j) dyn_step();
+            return;
+        }
         bool first = true;
         const int64_t n_total = n;
         while (n > 0) {
@@ -620,6 +710,7 @@ struct Impl final : Solver {
         if constexpr (!(std::is_same<St, float>::value || std::is_same<St, double>::value)) {
             throw ArgError{CAV_ERR_ARG, "the adjoint needs FP32 or FP64 storage"};
         } else {
+            if (dyn) throw ArgError{CAV_ERR_STATE, "the adjoint needs the fixed-Cs model (dynamic SGS is on)"};
             if (pc_form || time_step != 0)
                 throw ArgError{CAV_ERR_STATE, "adjoint_run starts from step 0 (after create or init_from_fields)"};
             if (N < 2 || ws < 1 || ws > N || C < 2) throw ArgError{CAV_ERR_ARG, "bad adjoint spec"};

@@ -207,6 +207,18 @@ class CavitySolver:
         """``total_f_mass`` (src/uniform/solver.rs:1018-1020)."""
         return self.diag()["total_f_mass"]
 
+    # -- dynamic mixed-scale subgrid model ---------------------------------------
+    def set_dynamic_sgs(self, dynamic_smag, smag_alpha=0.5, nu_sm_min=-0.1, eta_test=2.0):
+        """``set_dynamic_sgs`` (src/uniform/solver.rs:215-220)."""
+        self._ck(L.load().cav_set_dynamic_sgs(self._h, 1 if dynamic_smag else 0, smag_alpha, nu_sm_min,
+                                              eta_test))
+
+    def dynamic_stats(self):
+        """cs_dyn_mean, cs_dyn_max, kappa_dyn_mean, kappa_dyn_max of the last step."""
+        o = np.empty(4)
+        self._ck(L.load().cav_dynamic_sgs_stats(self._h, _dp(o)))
+        return dict(zip(("cs_dyn_mean", "cs_dyn_max", "kappa_dyn_mean", "kappa_dyn_max"), o.tolist()))
+
     # -- adjoint -----------------------------------------------------------------
     def adjoint_nusselt(self, n_steps, window_start, checkpoint_every=500):
         """Gradients of J = mean over s in [window_start, n_steps] of the hot-wall

@@ -183,6 +183,19 @@ int cav_get_stream(cav_handle* h, void** stream);
  * every kernel they contain; no counterpart in the reference). */
 int cav_launch_count(cav_handle* h, int64_t* n);
 
+/* ---- dynamic mixed-scale subgrid model (--dynamic-smag) ------------------ */
+/* set_dynamic_sgs (src/uniform/solver.rs:215-220): on = 1 computes nu_t and
+ * alpha_t per node before every collision with the dynamic mixed-scale model
+ * (compute_dynamic_sgs, :562-828) instead of Cs^2 |S| and nu_t / Pr_t.
+ * Reference defaults: smag_alpha 0.5, nu_sm_min -0.1, eta_test 2.0
+ * (src/cli.rs:118-120).  A step then runs the model's four kernels, the
+ * collision and the streaming as separate launches (no graph replay). */
+int cav_set_dynamic_sgs(cav_handle* h, int32_t on, double smag_alpha, double nu_sm_min, double eta_test);
+/* out4 = cs_dyn_mean, cs_dyn_max, kappa_dyn_mean, kappa_dyn_max of the last
+ * evaluation (the driver's progress line, src/main.rs:181-182); zeros before
+ * the first dynamic step. */
+int cav_dynamic_sgs_stats(cav_handle* h, double* out4);
+
 /* ---- adjoint: gradients of the time-averaged hot-wall Nusselt number ------ */
 /* No counterpart in the reference (it has no gradients).  Objective
  * J = mean over s in [window_start, n_steps] of nusselt_hot (post.rs:68-78)

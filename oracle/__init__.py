@@ -96,6 +96,14 @@ def lib():
         L.orc_avg_means.argtypes = [vp, dp, dp, dp, dp, dp]
         L.orc_nusselt_from_mean.restype = ctypes.c_double
         L.orc_nusselt_from_mean.argtypes = [vp, dp, ctypes.c_int32]
+        L.orc_set_dynamic_sgs.argtypes = [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_double]
+        L.orc_compute_dynamic_sgs.argtypes = [vp]
+        L.orc_dynamic_stats.argtypes = [vp, dp, dp, dp]
+        L.orc_lilly_coefficient.restype = ctypes.c_double
+        L.orc_lilly_coefficient.argtypes = [ctypes.c_double, ctypes.c_double]
+        L.orc_mixed_factor.restype = ctypes.c_double
+        L.orc_mixed_factor.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double]
         i32, d = ctypes.c_int32, ctypes.c_double
         L.orc_oct_create.restype = vp
         L.orc_oct_create.argtypes = [i32, i32, i32, d, d, d, ctypes.c_uint64, i32, i32, d, i32, d,
@@ -117,6 +125,14 @@ def lib():
 
 def _dp(a):
     return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def lilly_coefficient(num, den):
+    return lib().orc_lilly_coefficient(num, den)
+
+
+def mixed_factor(a, b, alpha):
+    return lib().orc_mixed_factor(a, b, alpha)
 
 
 def feq(i, rho, ux, uy):
@@ -306,6 +322,22 @@ class OracleSolver:
 
     def nusselt_cold(self):
         return self.nusselt()[1]
+
+    def set_dynamic_sgs(self, on, smag_alpha=0.5, nu_sm_min=-0.1, eta_test=2.0):
+        """set_dynamic_sgs (src/uniform/solver.rs:215-220)."""
+        lib().orc_set_dynamic_sgs(self._h, int(bool(on)), smag_alpha, nu_sm_min, eta_test)
+
+    def compute_dynamic_sgs(self):
+        lib().orc_compute_dynamic_sgs(self._h)
+
+    def dynamic_stats(self):
+        """(cs_dyn_mean, cs_dyn_max, kappa_dyn_mean, kappa_dyn_max, nu_t_pre, alpha_t_pre)."""
+        n = self._nx * self._ny
+        o, a, b = np.empty(4), np.empty(n), np.empty(n)
+        a[:] = np.nan
+        b[:] = np.nan
+        lib().orc_dynamic_stats(self._h, _dp(o), _dp(a), _dp(b))
+        return (*o.tolist(), a, b)
 
     def nusselt_from_mean(self, t_mean, hot=True):
         t = np.ascontiguousarray(t_mean, dtype=np.float64)

@@ -139,6 +139,40 @@ void orc_destroy(void* h) { delete H(h); }
 void orc_step(void* h, int64_t n) {
     for (int64_t i = 0; i < n; ++i) H(h)->s.step();
 }
+// set_dynamic_sgs, src/uniform/solver.rs:215-220.
+void orc_set_dynamic_sgs(void* h, int32_t on, double smag_alpha, double nu_sm_min, double eta_test) {
+    auto& s = H(h)->s;
+    s.dynamic_smag = on != 0;
+    s.smag_alpha = smag_alpha;
+    s.nu_sm_min = nu_sm_min;
+    s.eta_test = eta_test;
+    if (!s.dynamic_smag) {
+        s.nu_t_pre.clear();
+        s.alpha_t_pre.clear();
+    }
+}
+
+// compute_dynamic_sgs alone (src/uniform/solver.rs:562-828) on the current state.
+void orc_compute_dynamic_sgs(void* h) { H(h)->s.compute_dynamic_sgs(); }
+
+// out4 = cs_dyn_mean, cs_dyn_max, kappa_dyn_mean, kappa_dyn_max; the per-node
+// nu_t_pre / alpha_t_pre when the model has run (NULL to skip).
+void orc_dynamic_stats(void* h, double* out4, double* nu_t_pre, double* alpha_t_pre) {
+    auto& s = H(h)->s;
+    out4[0] = s.cs_dyn_mean;
+    out4[1] = s.cs_dyn_max;
+    out4[2] = s.kappa_dyn_mean;
+    out4[3] = s.kappa_dyn_max;
+    const size_t n = size_t(s.nx) * s.ny;
+    if (nu_t_pre && s.nu_t_pre.size() == n) std::memcpy(nu_t_pre, s.nu_t_pre.data(), n * 8);
+    if (alpha_t_pre && s.alpha_t_pre.size() == n) std::memcpy(alpha_t_pre, s.alpha_t_pre.data(), n * 8);
+}
+
+double orc_lilly_coefficient(double num, double den) { return orc::lilly_coefficient(num, den); }
+
+// mixed_factor, src/uniform/solver.rs:1195-1202.
+double orc_mixed_factor(double a, double b, double alpha) { return std::pow(a, alpha) * std::pow(b, 1.0 - alpha); }
+
 void orc_collide(void* h, int64_t step) { H(h)->s.collide(step); }
 void orc_stream(void* h) { H(h)->s.stream(); }
 void orc_bounce_back(void* h) { H(h)->s.apply_bounce_back(); }

@@ -54,6 +54,16 @@ void orc_info(void* h, double* out);
 void orc_diag(void* h, double* out);
 void orc_set_time_step(void* h, int64_t t);
 
+/* Dynamic mixed-scale SGS model (src/uniform/solver.rs:215-220, 562-828,
+ * 1195-1261): switch, one evaluation on the current state, its statistics
+ * and per-node nu_t / alpha_t (NULL to skip), the Lilly coefficient and the
+ * mixed factor. */
+void orc_set_dynamic_sgs(void* h, int32_t on, double smag_alpha, double nu_sm_min, double eta_test);
+void orc_compute_dynamic_sgs(void* h);
+void orc_dynamic_stats(void* h, double* out4, double* nu_t_pre, double* alpha_t_pre);
+double orc_lilly_coefficient(double num, double den);
+double orc_mixed_factor(double a, double b, double alpha);
+
 /* Equilibria and lattice weights (crate oxiphysics_lbm, pinned by
  * src/uniform/tests.rs:116-133). */
 double orc_feq(int32_t i, double rho, double ux, double uy);
