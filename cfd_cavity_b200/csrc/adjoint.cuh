@@ -105,6 +105,8 @@ __global__ void __launch_bounds__(128) k_adj_step(const St* __restrict__ X, cons
                                                   const long long* step_dev, long long j,
                                                   AdjObj<typename Fmt<St>::A> obj) {
     using A = typename Fmt<St>::A;
+    pdl_wait();
+    pdl_trigger();
     long long s;
     const StepScalars<A> c = table_scalars<A>(table, S, step_dev, j, &s);
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
@@ -114,19 +116,22 @@ __global__ void __launch_bounds__(128) k_adj_step(const St* __restrict__ X, cons
     const int k = iy * W + ix;
     const int nx = G.nx, ny = G.ny;
     // 1. adjoint of this node's outputs X_{s+1}(x), gathered from its readers.
+    // Branch-free: every load reads a valid address and the unused ones are
+    // discarded by selects, so all of a node's loads are in flight together.
     A af[Q], ag[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
         const int rx = ix + CX(q), ry = iy + CY(q);
         const bool in = rx >= 0 && rx < nx && ry >= 0 && ry < ny;
-        af[q] = in ? Pin[q * Pp + ry * W + rx] : Pin[OPP(q) * Pp + k];
-        A v = A(0.0);
-        if (in && rx >= 1 && rx <= nx - 2 && ry >= 1 && ry <= ny - 2) {
-            v = Pin[(Q + q) * Pp + ry * W + rx];
-            if (ry == 1) v = v + Pin[(Q + q) * Pp + 0 * W + rx];
-            if (ry == ny - 2) v = v + Pin[(Q + q) * Pp + (ny - 1) * W + rx];
-        }
-        ag[q] = v;
+        const int kr = in ? ry * W + rx : k;
+        af[q] = Pin[(in ? q : OPP(q)) * Pp + kr];
+        const bool gin = in && rx >= 1 && rx <= nx - 2 && ry >= 1 && ry <= ny - 2;
+        const A v0 = Pin[(Q + q) * Pp + kr];
+        // rows 1 / ny-2 were copied to the wall rows 0 / ny-1: their readers add up
+        const int kw = ry == 1 ? rx : (ry == ny - 2 ? (ny - 1) * W + rx : kr);
+        const A vw = Pin[(Q + q) * Pp + (gin ? kw : kr)];
+        const bool wrow = gin && (ry == 1 || ry == ny - 2);
+        ag[q] = gin ? (wrow ? v0 + vw : v0) : A(0.0);
     }
     const A afy = Pin[18 * Pp + k];
     // 2. recompute the node's pulled inputs from X_s.
@@ -171,6 +176,8 @@ __global__ void __launch_bounds__(256) k_fwd_slot(const St* __restrict__ src, St
                                                   Geom G, const StepScalars<typename Fmt<St>::A>* __restrict__ table,
                                                   int S, const long long* step_dev, long long j) {
     using A = typename Fmt<St>::A;
+    pdl_wait();
+    pdl_trigger();
     long long s;
     const StepScalars<A> c = table_scalars<A>(table, S, step_dev, j, &s);
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;

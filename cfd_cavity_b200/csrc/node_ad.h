@@ -45,6 +45,21 @@ __host__ __device__ __forceinline__ T sqrt_(T x) {
     return sqrt(x);
 }
 
+// Division; FP32 on the device uses the fast approximate division (2 ulp),
+// as the FP32 forward step does.
+template <class T>
+__host__ __device__ __forceinline__ T div_(T a, T b) {
+    return a / b;
+}
+template <>
+__host__ __device__ __forceinline__ float div_<float>(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fdividef(a, b);
+#else
+    return a / b;
+#endif
+}
+
 // Per-step scalars of the collision (CollideCtx, src/uniform/solver.rs:1034-1043).
 template <class T>
 struct NodeScal {
@@ -63,7 +78,7 @@ __host__ __device__ __forceinline__ T node_forward(const T (&h)[9], const T (&g)
     const T jx = h[1] + h[3] - h[4] - h[5] - h[7] + h[8];
     const T jy = h[2] + h[3] + h[4] - h[6] - h[7] - h[8];
     const T r = T(1.0) + drho;
-    const T inv = T(1.0) / r;
+    const T inv = div_(T(1.0), r);
     const T ux = wall ? T(0.0) : jx * inv;
     const T uy = wall ? T(0.0) : (jy + T(0.5) * fyp) * inv;
     T t = g[0];
@@ -88,9 +103,9 @@ __host__ __device__ __forceinline__ T node_forward(const T (&h)[9], const T (&g)
     const T smag = sq * c.c1 * inv;
     const T nut = cs * cs * smag;
     const T e = T(3.0) * (c.nu + nut);
-    const T om_p = T(1.0) / (T(0.5) + e);
-    const T om_m = e / (T(0.5) * e + c.lambda);
-    const T om_g = T(1.0) / (T(0.5) + T(3.0) * (c.alpha + nut * c.inv_pr_t));
+    const T om_p = div_(T(1.0), T(0.5) + e);
+    const T om_m = div_(e, T(0.5) * e + c.lambda);
+    const T om_g = div_(T(1.0), T(0.5) + T(3.0) * (c.alpha + nut * c.inv_pr_t));
     const T k_p = T(1.0) - T(0.5) * om_p, k_m = T(1.0) - T(0.5) * om_m;
     ho[0] = h[0] - om_p * d0 + k_p * T(wd(0)) * (T(-3.0) * uy) * fy;
     for (int p = 1; p <= 4; ++p) {
@@ -125,7 +140,7 @@ __host__ __device__ __forceinline__ T node_reverse(const T (&h)[9], const T (&g)
     const T jx = h[1] + h[3] - h[4] - h[5] - h[7] + h[8];
     const T jy = h[2] + h[3] + h[4] - h[6] - h[7] - h[8];
     const T r = T(1.0) + drho;
-    const T inv = T(1.0) / r;
+    const T inv = div_(T(1.0), r);
     const T ux = wall ? T(0.0) : jx * inv;
     const T uy = wall ? T(0.0) : (jy + T(0.5) * fyp) * inv;
     T t = g[0];
@@ -149,10 +164,10 @@ __host__ __device__ __forceinline__ T node_reverse(const T (&h)[9], const T (&g)
     const T smag = sq * c.c1 * inv;
     const T nut = cs * cs * smag;
     const T e = T(3.0) * (c.nu + nut);
-    const T om_p = T(1.0) / (T(0.5) + e);
+    const T om_p = div_(T(1.0), T(0.5) + e);
     const T den_m = T(0.5) * e + c.lambda;
-    const T om_m = e / den_m;
-    const T om_g = T(1.0) / (T(0.5) + T(3.0) * (c.alpha + nut * c.inv_pr_t));
+    const T om_m = div_(e, den_m);
+    const T om_g = div_(T(1.0), T(0.5) + T(3.0) * (c.alpha + nut * c.inv_pr_t));
     const T k_p = T(1.0) - T(0.5) * om_p, k_m = T(1.0) - T(0.5) * om_m;
     const T om1 = T(1.0) - om_g;
 
@@ -219,7 +234,7 @@ __host__ __device__ __forceinline__ T node_reverse(const T (&h)[9], const T (&g)
 
     // relaxation rates -> nut -> (Cs, |S|)
     T b_nut = b_omg * (T(-3.0) * c.inv_pr_t * om_g * om_g);
-    const T b_e = b_omm * (c.lambda / (den_m * den_m)) - b_omp * om_p * om_p;
+    const T b_e = b_omm * div_(c.lambda, den_m * den_m) - b_omp * om_p * om_p;
     b_nut = b_nut + T(3.0) * b_e;
     const T b_cs = T(2.0) * cs * smag * b_nut;
     const T b_smag = cs * cs * b_nut;
@@ -227,7 +242,7 @@ __host__ __device__ __forceinline__ T node_reverse(const T (&h)[9], const T (&g)
     const T b_sq = c.c1 * inv * b_smag;
     T b_pxx = T(0.0), b_pxy = T(0.0), b_pyy = T(0.0);
     if (pi2 > T(0.0)) {  // subgradient 0 at pi = 0
-        const T k = b_sq / sq;
+        const T k = div_(b_sq, sq);
         b_pxx = k * pxx;
         b_pxy = k * T(2.0) * pxy;
         b_pyy = k * pyy;

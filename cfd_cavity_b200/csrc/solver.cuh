@@ -262,6 +262,23 @@ struct Impl final : Solver {
         CK(cudaGetLastError());
     }
 
+    // Launch with programmatic dependent launch (the kernel begins with
+    // pdl_wait(), so it overlaps only the tail of its predecessor).
+    template <typename... KArgs, typename... Args>
+    void launch_pdl(void (*kern)(KArgs...), cudaStream_t st, Args... args) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = grd;
+        cfg.blockDim = blk;
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CK(cudaLaunchKernelEx(&cfg, kern, args...));
+    }
+
     // ---- host-built initial states ----------------------------------------
     void upload_ref(const std::vector<double>& f, const std::vector<double>& g, const std::vector<double>& r,
                     const std::vector<double>& u, const std::vector<double>& v, const std::vector<double>& t) {
@@ -786,8 +803,24 @@ struct Impl final : Solver {
             A* setf[2] = {seg_fy, seg_fy2};
             long long* sd_rec = sdev2;
             long long* sd_adj = sdev2 + 1;
-            cudaStream_t rs = nullptr;
+            cudaStream_t rs = nullptr, hs = nullptr;
             CK(cudaStreamCreateWithFlags(&rs, cudaStreamNonBlocking));
+            // the adjoint sweep is the critical path: it runs on a stream of
+            // the highest priority, the recomputation fills the rest of the GPU
+            {
+                int least = 0, greatest = 0;
+                CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+                CK(cudaStreamCreateWithPriority(&hs, cudaStreamNonBlocking, greatest));
+            }
+            struct StreamGuard {
+                cudaStream_t* s;
+                ~StreamGuard() {
+                    if (*s) {
+                        cudaStreamSynchronize(*s);
+                        cudaStreamDestroy(*s);
+                    }
+                }
+            } hs_guard{&hs};
             std::vector<cudaEvent_t> ev_rec(n_ck, nullptr), ev_adj(n_ck, nullptr);
             cudaGraphExec_t g_rec[2] = {nullptr, nullptr}, g_adj[2] = {nullptr, nullptr};
             struct Cleanup {
@@ -839,7 +872,7 @@ struct Impl final : Solver {
                     if (!g_rec[set])
                         capture(rs, &g_rec[set], [&] {
                             for (int64_t j = 0; j + 1 < C; ++j)
-                                k_fwd_slot<St><<<grd, blk, 0, rs>>>(sp + popn * j, sp + popn * (j + 1), sf + fld * j,
+                                launch_pdl(k_fwd_slot<St>, rs, (const St*)sp + popn * j, sp + popn * (j + 1), sf + fld * j,
                                                                     sf + fld * (j + 1), G, table, S, sd_rec, j);
                         });
                     k_set_step<<<1, 1, 0, rs>>>(sd_rec, a);
@@ -848,7 +881,7 @@ struct Impl final : Solver {
                     launches += C - 1;
                 } else {
                     for (int64_t j = 0; j + 1 < L; ++j) {
-                        k_fwd_slot<St><<<grd, blk, 0, rs>>>(sp + popn * j, sp + popn * (j + 1), sf + fld * j,
+                        launch_pdl(k_fwd_slot<St>, rs, (const St*)sp + popn * j, sp + popn * (j + 1), sf + fld * j,
                                                             sf + fld * (j + 1), G, table, S, nullptr, a + j);
                         check_launch();
                     }
@@ -862,32 +895,32 @@ struct Impl final : Solver {
                 const int64_t a = 1 + k * C, L = seg_len(k);
                 St* sp = setp[set];
                 A* sf = setf[set];
-                CK(cudaStreamWaitEvent(stream, ev_rec[k], 0));
+                CK(cudaStreamWaitEvent(hs, ev_rec[k], 0));
                 if (use_graphs && L == C) {
                     if (cp != 0) throw ArgError{CAV_ERR_STATE, "adjoint ping-pong out of phase"};
                     if (!g_adj[set])
                         capture(stream, &g_adj[set], [&] {
                             int q = 0;
                             for (int64_t j = C - 1; j >= 0; --j) {
-                                k_adj_step<St><<<grd, blk, 0, stream>>>(sp + popn * j, sf + fld * j, P[q], P[q ^ 1],
+                                launch_pdl(k_adj_step<St>, stream, (const St*)sp + popn * j, sf + fld * j, P[q], P[q ^ 1],
                                                                         acc_cs_d, acc_th_d, G, table, S, sd_adj, j,
                                                                         obj);
                                 q ^= 1;
                             }
                         });
-                    k_set_step<<<1, 1, 0, stream>>>(sd_adj, a);
+                    k_set_step<<<1, 1, 0, hs>>>(sd_adj, a);
                     check_launch();
-                    CK(cudaGraphLaunch(g_adj[set], stream));
+                    CK(cudaGraphLaunch(g_adj[set], hs));
                     launches += C;
                 } else {
                     for (int64_t j = L - 1; j >= 0; --j) {
-                        k_adj_step<St><<<grd, blk, 0, stream>>>(sp + popn * j, sf + fld * j, P[cp], P[cp ^ 1],
+                        launch_pdl(k_adj_step<St>, hs, (const St*)sp + popn * j, sf + fld * j, P[cp], P[cp ^ 1],
                                                                 acc_cs_d, acc_th_d, G, table, S, nullptr, a + j, obj);
                         check_launch();
                         cp ^= 1;
                     }
                 }
-                CK(cudaEventRecord(ev_adj[k], stream));
+                CK(cudaEventRecord(ev_adj[k], hs));
             };
             // Build the segment graphs now, outside the timed passes (they only
             // depend on the buffers, not on the state).
@@ -898,13 +931,13 @@ struct Impl final : Solver {
                     A* sf = setf[set];
                     capture(rs, &g_rec[set], [&] {
                         for (int64_t j = 0; j + 1 < C; ++j)
-                            k_fwd_slot<St><<<grd, blk, 0, rs>>>(sp + popn * j, sp + popn * (j + 1), sf + fld * j,
+                            launch_pdl(k_fwd_slot<St>, rs, (const St*)sp + popn * j, sp + popn * (j + 1), sf + fld * j,
                                                                 sf + fld * (j + 1), G, table, S, sd_rec, j);
                     });
                     capture(stream, &g_adj[set], [&] {
                         int q = 0;
                         for (int64_t j = C - 1; j >= 0; --j) {
-                            k_adj_step<St><<<grd, blk, 0, stream>>>(sp + popn * j, sf + fld * j, P[q], P[q ^ 1],
+                            launch_pdl(k_adj_step<St>, stream, (const St*)sp + popn * j, sf + fld * j, P[q], P[q ^ 1],
                                                                     acc_cs_d, acc_th_d, G, table, S, sd_adj, j, obj);
                             q ^= 1;
                         }
@@ -944,7 +977,8 @@ struct Impl final : Solver {
                 const int64_t L_last = seg_len(n_ck - 1);
                 cp = (use_graphs && L_last != C && (L_last & 1)) ? 1 : 0;
             }
-            k_adj_final<St><<<grd, blk, 0, stream>>>(pop[cur], P[cp], G, scalars(N), obj, N);
+            CK(cudaStreamWaitEvent(hs, ev[1], 0));
+            k_adj_final<St><<<grd, blk, 0, hs>>>(pop[cur], P[cp], G, scalars(N), obj, N);
             check_launch();
             CK(cudaStreamWaitEvent(rs, ev[1], 0));  // checkpoints complete
             recompute(n_ck - 1);
@@ -952,7 +986,11 @@ struct Impl final : Solver {
                 if (k >= 1) recompute(k - 1);
                 sweep(k);
             }
-            CK(cudaEventRecord(ev[2], stream));
+            CK(cudaEventRecord(ev[2], hs));
+            CK(cudaStreamWaitEvent(stream, ev[2], 0));
+            CK(cudaStreamSynchronize(hs));
+            CK(cudaStreamDestroy(hs));
+            hs = nullptr;
             std::vector<double> acs(size_t(p.nx) * p.ny), ath(p.ny);
             CK(cudaMemcpyAsync(acs.data(), acc_cs_d, sizeof(double) * acs.size(), cudaMemcpyDeviceToHost, stream));
             CK(cudaMemcpyAsync(ath.data(), acc_th_d, sizeof(double) * ath.size(), cudaMemcpyDeviceToHost, stream));
