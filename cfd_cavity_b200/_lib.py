@@ -19,6 +19,7 @@ CAV_ERR_TIMEOUT = 5
 CAV_ERR_CUDA = 6
 CAV_ERR_STATE = 7
 CAV_ERR_NOMEM = 8
+CAV_ERR_IO = 9
 
 (CAV_PREC_F64, CAV_PREC_F32, CAV_PREC_F16, CAV_PREC_BF16, CAV_PREC_F16G, CAV_PREC_F16SR,
  CAV_PREC_BF16SR, CAV_PREC_F16GSR) = range(8)
@@ -160,6 +161,13 @@ def load(path: str | None = None):
         "cav_get_stream": (i32, [vp, ctypes.POINTER(vp)]),
         "cav_launch_count": (i32, [vp, ctypes.POINTER(i64)]),
         "cav_set_dynamic_sgs": (i32, [vp, i32, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
+        "cav_snapshot_write_fields": (i32, [ctypes.c_char_p, i64, i64, _dp, _dp, _dp, _dp]),
+        "cav_snapshot_read_fields": (i32, [ctypes.c_char_p, ctypes.POINTER(i64), ctypes.POINTER(i64), _dp, _dp,
+                                           _dp, _dp]),
+        "cav_snapshot_write": (i32, [vp, ctypes.c_char_p]),
+        "cav_restart_from_snapshot": (i32, [vp, ctypes.c_char_p]),
+        "cav_octree_snapshot_write": (i32, [vp, ctypes.c_char_p, ctypes.c_uint64]),
+        "cav_octree_restart_from_snapshot": (i32, [vp, ctypes.c_char_p]),
         "cav_dynamic_sgs_stats": (i32, [vp, _dp]),
         "cav_adjoint_run": (i32, [vp, ctypes.POINTER(CavAdjointSpec), _dp,
                                   ctypes.POINTER(CavAdjointResult)]),

@@ -7,6 +7,7 @@
 #include <mutex>
 
 #include "batch.cuh"
+#include "snapshot.cuh"
 #include "solver.cuh"
 
 using namespace cav;
@@ -296,6 +297,82 @@ int cav_sync(cav_handle* h) {
 int cav_get_stream(cav_handle* h, void** stream) {
     if (!stream) return fail(h, CAV_ERR_ARG, "null output");
     return guarded(h, [&](Solver& s) { *stream = (void*)s.stream; });
+}
+
+int cav_snapshot_write_fields(const char* path, int64_t nx, int64_t ny, const double* rho, const double* ux,
+                              const double* uy, const double* t) {
+    if (!path || !rho || !ux || !uy || !t || nx < 1 || ny < 1) return fail(nullptr, CAV_ERR_ARG, "bad arguments");
+    try {
+        snap::write_cavsnap(path, nx, ny, rho, ux, uy, t);
+    } catch (const ArgError& e) {
+        return fail(nullptr, e.code, e.msg);
+    }
+    return CAV_OK;
+}
+
+int cav_snapshot_read_fields(const char* path, int64_t* nx, int64_t* ny, double* rho, double* ux, double* uy,
+                             double* t) {
+    if (!path || !nx || !ny) return fail(nullptr, CAV_ERR_ARG, "bad arguments");
+    try {
+        const snap::Fields F = snap::read_cavsnap(path);
+        *nx = F.nx;
+        *ny = F.ny;
+        const size_t n = size_t(F.nx * F.ny);
+        if (rho) std::memcpy(rho, F.rho.data(), n * 8);
+        if (ux) std::memcpy(ux, F.ux.data(), n * 8);
+        if (uy) std::memcpy(uy, F.uy.data(), n * 8);
+        if (t) std::memcpy(t, F.t.data(), n * 8);
+    } catch (const ArgError& e) {
+        return fail(nullptr, e.code, e.msg);
+    } catch (const std::bad_alloc&) {
+        return fail(nullptr, CAV_ERR_NOMEM, "host allocation failed");
+    }
+    return CAV_OK;
+}
+
+int cav_snapshot_write(cav_handle* h, const char* path) {
+    if (!path) return fail(h, CAV_ERR_ARG, "null path");
+    return guarded(h, [&](Solver& s) {
+        const size_t n = size_t(s.p.nx) * s.p.ny;
+        std::vector<double> r(n), u(n), v(n), t(n);
+        s.get_fields(r.data(), u.data(), v.data(), t.data(), nullptr, nullptr);
+        snap::write_cavsnap(path, s.p.nx, s.p.ny, r.data(), u.data(), v.data(), t.data());
+    });
+}
+
+int cav_restart_from_snapshot(cav_handle* h, const char* path) {
+    if (!path) return fail(h, CAV_ERR_ARG, "null path");
+    return guarded(h, [&](Solver& s) {
+        const snap::Fields F = snap::read_cavsnap(path);
+        const int nx1 = s.p.nx, ny1 = s.p.ny;
+        const size_t n0 = size_t(F.nx * F.ny), n1 = size_t(nx1) * ny1;
+        // restart is not a hot path: temporary device buffers for the source
+        // and the regridded fields
+        struct Buf {
+            double* p = nullptr;
+            ~Buf() {
+                if (p) cudaFree(p);
+            }
+        } src, dst;
+        CK(cudaMalloc(&src.p, sizeof(double) * 4 * n0));
+        CK(cudaMalloc(&dst.p, sizeof(double) * 4 * n1));
+        const std::vector<double>* fs[4] = {&F.rho, &F.ux, &F.uy, &F.t};
+        for (int q = 0; q < 4; ++q) {
+            CK(cudaMemcpyAsync(src.p + q * n0, fs[q]->data(), sizeof(double) * n0, cudaMemcpyHostToDevice,
+                               s.stream));
+            if (F.nx == nx1 && F.ny == ny1) {
+                CK(cudaMemcpyAsync(dst.p + q * n1, src.p + q * n0, sizeof(double) * n1, cudaMemcpyDeviceToDevice,
+                                   s.stream));
+            } else {
+                const dim3 b(32, 4), g((nx1 + 31) / 32, (ny1 + 3) / 4);
+                snap::k_regrid<<<g, b, 0, s.stream>>>(src.p + q * n0, int(F.nx), int(F.ny), dst.p + q * n1, nx1,
+                                                      ny1);
+                ++s.launches;
+                CK(cudaGetLastError());
+            }
+        }
+        s.init_from_device_fields(dst.p, dst.p + n1, dst.p + 2 * n1, dst.p + 3 * n1);
+    });
 }
 
 int cav_set_dynamic_sgs(cav_handle* h, int32_t on, double smag_alpha, double nu_sm_min, double eta_test) {

@@ -284,6 +284,38 @@ __global__ void __launch_bounds__(256) k_materialize(const St* __restrict__ src,
     for (int i = 0; i < Q; ++i) stp(dst, G, Q + i, iy, ix, g[i]);
 }
 
+// init_from_fields (src/uniform/solver.rs:232-262) on the device: fields
+// from dense FP64 arrays (k = iy*nx + ix), populations their equilibria, then
+// no-slip on the stored velocity (the populations keep the given u).
+template <class St>
+__global__ void __launch_bounds__(256) k_init_eq(const double* __restrict__ r, const double* __restrict__ u,
+                                                 const double* __restrict__ v, const double* __restrict__ t,
+                                                 St* __restrict__ dst, typename Fmt<St>::A* __restrict__ rho,
+                                                 typename Fmt<St>::A* __restrict__ ux,
+                                                 typename Fmt<St>::A* __restrict__ uy,
+                                                 typename Fmt<St>::A* __restrict__ tt, Geom G, int geq_order) {
+    using A = typename Fmt<St>::A;
+    constexpr bool SH = Fmt<St>::SHIFT;
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= G.nx || iy >= G.ny) return;
+    const int kd = iy * G.nx + ix;
+    const long long k = (long long)iy * G.pitch + ix;
+    const double rk = r[kd], uk = u[kd], vk = v[kd], tk = t[kd];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        double fv = feq_full<double>(i, rk, uk, vk);
+        if (SH) fv -= WD(i);
+        stp(dst, G, i, iy, ix, A(fv));
+        stp(dst, G, Q + i, iy, ix, A(geq_full<double>(i, tk, uk, vk, geq_order)));
+    }
+    const bool wall = is_wall(G, ix, iy);
+    rho[k] = A(rk);
+    ux[k] = wall ? A(0.0) : A(uk);
+    uy[k] = wall ? A(0.0) : A(vk);
+    tt[k] = A(tk);
+}
+
 // Nusselt accumulation of the streamed state of a PC buffer (one thread per row).
 template <class St>
 __global__ void k_acc_nu_pc(const St* __restrict__ src, double* __restrict__ acc_hot, double* __restrict__ acc_cold,

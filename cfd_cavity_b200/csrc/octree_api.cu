@@ -1,6 +1,7 @@
 // octree_api.cu -- the cav_octree_* entry points of include/cavity.h (host
 // code only): octree::solver::CavitySolver methods onto a cav::oct::Octree.
 #include "octree.cuh"
+#include "snapshot.cuh"
 
 using namespace cav;
 using namespace cav::oct;
@@ -184,6 +185,53 @@ int cav_octree_restart_level(cav_octree* h, int32_t level, const double* rho, co
 int cav_octree_set_time_step(cav_octree* h, int64_t t) {
     return oguarded(h, [&](Octree& o) {
         o.set_time_step(t);
+        return CAV_OK;
+    });
+}
+
+int cav_octree_snapshot_write(cav_octree* h, const char* path, uint64_t step) {
+    if (!path) return ofail(h, CAV_ERR_ARG, "null path");
+    return oguarded(h, [&](Octree& o) {
+        snap::Oct s;
+        s.levels = uint32_t(o.levels);
+        s.step = step;
+        const int n_lv = o.levels == 3 ? 5 : 3;
+        s.grids.resize(n_lv);
+        for (int l = 0; l < n_lv; ++l) {
+            snap::Fields& g = s.grids[l];
+            g.nx = l == 0 ? o.nx0 : (l <= 2 ? o.nx1 : o.nx2);
+            g.ny = l == 0 ? o.ny0 : (l <= 2 ? o.ny1 : o.ny2);
+            const size_t n = size_t(g.nx * g.ny);
+            g.rho.resize(n);
+            g.ux.resize(n);
+            g.uy.resize(n);
+            g.t.resize(n);
+            o.get_level(l, g.rho.data(), g.ux.data(), g.uy.data(), g.t.data(), nullptr, nullptr);
+        }
+        snap::write_octsnap(path, s);
+        return CAV_OK;
+    });
+}
+
+int cav_octree_restart_from_snapshot(cav_octree* h, const char* path) {
+    if (!path) return ofail(h, CAV_ERR_ARG, "null path");
+    return oguarded(h, [&](Octree& o) {
+        const snap::Oct s = snap::read_octsnap(path);
+        const int n_lv = o.levels == 3 ? 5 : 3;
+        if (int(s.levels) != o.levels || int(s.grids.size()) != n_lv)
+            throw ArgError{CAV_ERR_ARG, "octree restart: snapshot levels differ from the solver's"};
+        for (int l = 0; l < n_lv; ++l) {
+            const int64_t nx = l == 0 ? o.nx0 : (l <= 2 ? o.nx1 : o.nx2);
+            const int64_t ny = l == 0 ? o.ny0 : (l <= 2 ? o.ny1 : o.ny2);
+            if (s.grids[l].nx != nx || s.grids[l].ny != ny)
+                throw ArgError{CAV_ERR_ARG, "octree restart: grid " + std::to_string(l) +
+                                                " differs from the solver's (the same level layout is required)"};
+        }
+        for (int l = 0; l < n_lv; ++l) {
+            const snap::Fields& g = s.grids[l];
+            o.restart_level(l, g.rho.data(), g.ux.data(), g.uy.data(), g.t.data());
+        }
+        o.set_time_step(0);
         return CAV_OK;
     });
 }

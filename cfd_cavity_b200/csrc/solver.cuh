@@ -110,6 +110,8 @@ struct Solver {
     virtual void alloc() = 0;
     virtual void init_default(const std::vector<double>& t0) = 0;
     virtual void init_from_fields(const double* r, const double* u, const double* v, const double* t) = 0;
+    // init_from_fields from DEVICE arrays (dense, k = iy*nx + ix).
+    virtual void init_from_device_fields(const double* r, const double* u, const double* v, const double* t) = 0;
     virtual void step(int64_t n) = 0;
     virtual void get_fields(double* r, double* u, double* v, double* t, double* nut, double* fy) = 0;
     virtual void set_fields(const double* r, const double* u, const double* v, const double* t,
@@ -335,6 +337,16 @@ struct Impl final : Solver {
     }
 
     // init_from_fields, src/uniform/solver.rs:232-262.
+    void init_from_device_fields(const double* r, const double* u, const double* v, const double* t) override {
+        k_init_eq<St><<<grd, blk, 0, stream>>>(r, u, v, t, pop[0], rho, ux, uy, tt, G, p.geq_order);
+        check_launch();
+        cur = 0;
+        pc_form = false;
+        ref_cached = false;
+        time_step = 0;
+        CK(cudaStreamSynchronize(stream));
+    }
+
     void init_from_fields(const double* r, const double* u, const double* v, const double* t) override {
         const int nx = p.nx, ny = p.ny;
         const size_t n = size_t(nx) * ny;

@@ -118,6 +118,15 @@ class OctreeSolver:
                                                        _dp(d["uy"]), _dp(d["temp"])))
         self.set_time_step(0)
 
+    def write_snapshot(self, path, step=None):
+        """``snapshot`` + ``write_snapshot_atomic`` (src/octree/snapshot.rs:147-165)."""
+        st = self.time_step if step is None else step
+        self._ck(L.load().cav_octree_snapshot_write(self._h, str(path).encode(), int(st)))
+
+    def restart_from_snapshot(self, path):
+        """``set_from_snapshot`` of an OCTSNAP1 file (same layout), time step 0."""
+        self._ck(L.load().cav_octree_restart_from_snapshot(self._h, str(path).encode()))
+
     def couple(self, which):
         """One coupling: 0 coarse_to_fine L0->L1, 1 fine_to_coarse L1->L0,
         2 / 3 the same between L1 and L2 (src/octree/interface.rs:137-206)."""

@@ -207,6 +207,16 @@ class CavitySolver:
         """``total_f_mass`` (src/uniform/solver.rs:1018-1020)."""
         return self.diag()["total_f_mass"]
 
+    # -- snapshots -----------------------------------------------------------------
+    def write_snapshot(self, path):
+        """The fields to a CAVSNAP1 file (snapshot::write_snapshot_atomic)."""
+        self._ck(L.load().cav_snapshot_write(self._h, str(path).encode()))
+
+    def restart_from_snapshot(self, path):
+        """The driver's --restart: CAVSNAP1 file, bilinear regrid when the grid
+        differs, equilibrium populations, time step 0 (on the device)."""
+        self._ck(L.load().cav_restart_from_snapshot(self._h, str(path).encode()))
+
     # -- dynamic mixed-scale subgrid model ---------------------------------------
     def set_dynamic_sgs(self, dynamic_smag, smag_alpha=0.5, nu_sm_min=-0.1, eta_test=2.0):
         """``set_dynamic_sgs`` (src/uniform/solver.rs:215-220)."""
@@ -267,3 +277,22 @@ class TimeAverager:
         v = ctypes.c_double()
         self.s._ck(L.load().cav_nusselt_from_mean(self.s._h, 1 if hot else 0, ctypes.byref(v)))
         return v.value
+
+
+def write_snapshot_fields(path, nx, ny, rho, ux, uy, t):
+    """write_snapshot_atomic (src/uniform/snapshot.rs:13-61), host only."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float64).reshape(nx * ny) for a in (rho, ux, uy, t)]
+    L.check(L.load().cav_snapshot_write_fields(str(path).encode(), nx, ny, *[_dp(a) for a in arrs]))
+
+
+def read_snapshot_fields(path):
+    """read_snapshot (src/uniform/snapshot.rs:64-97): (nx, ny, rho, ux, uy, t)."""
+    nx, ny = ctypes.c_int64(), ctypes.c_int64()
+    lib = L.load()
+    L.check(lib.cav_snapshot_read_fields(str(path).encode(), ctypes.byref(nx), ctypes.byref(ny), None, None,
+                                         None, None))
+    n = nx.value * ny.value
+    out = [np.empty(n) for _ in range(4)]
+    L.check(lib.cav_snapshot_read_fields(str(path).encode(), ctypes.byref(nx), ctypes.byref(ny),
+                                         *[_dp(a) for a in out]))
+    return (nx.value, ny.value, *out)

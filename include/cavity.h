@@ -40,6 +40,7 @@ extern "C" {
 #define CAV_ERR_CUDA 6     /* CUDA runtime error                             */
 #define CAV_ERR_STATE 7    /* call not valid in the handle's current state   */
 #define CAV_ERR_NOMEM 8    /* device allocation failed                       */
+#define CAV_ERR_IO 9       /* snapshot file missing, unwritable or malformed */
 
 /* ---- enumerations -------------------------------------------------------- */
 /* Storage precision of the populations (arithmetic: FP64 for CAV_PREC_F64,
@@ -182,6 +183,26 @@ int cav_get_stream(cav_handle* h, void** stream);
 /* Number of kernels the handle has launched so far (graph replays count
  * every kernel they contain; no counterpart in the reference). */
 int cav_launch_count(cav_handle* h, int64_t* n);
+
+/* ---- snapshots and restart ------------------------------------------------ */
+/* CAVSNAP1 files of the reference (src/uniform/snapshot.rs:10-131): rho, ux,
+ * uy, T in FP64, written atomically (temporary file + rename, as
+ * write_snapshot_atomic).  Host-only, no device needed:
+ *   cav_snapshot_write_fields  write_snapshot_atomic of caller arrays;
+ *   cav_snapshot_read_fields   read_snapshot: call with NULL arrays to get
+ *                              nx, ny, then with [nx*ny] arrays. */
+int cav_snapshot_write_fields(const char* path, int64_t nx, int64_t ny, const double* rho, const double* ux,
+                              const double* uy, const double* t);
+int cav_snapshot_read_fields(const char* path, int64_t* nx, int64_t* ny, double* rho, double* ux, double* uy,
+                             double* t);
+/* The cavity's fields to a CAVSNAP1 file (the driver's --snapshot-every). */
+int cav_snapshot_write(cav_handle* h, const char* path);
+/* The driver's --restart (src/main.rs, solver.rs:232-262): read a CAVSNAP1
+ * file, interpolate it bilinearly onto this cavity's grid when the sizes
+ * differ (interpolate_field, snapshot.rs:102-131) and set the populations
+ * to the equilibria of the fields (init_from_fields), all on the device;
+ * the time step restarts at 0. */
+int cav_restart_from_snapshot(cav_handle* h, const char* path);
 
 /* ---- dynamic mixed-scale subgrid model (--dynamic-smag) ------------------ */
 /* set_dynamic_sgs (src/uniform/solver.rs:215-220): on = 1 computes nu_t and
@@ -338,6 +359,12 @@ int cav_octree_set_level(cav_octree* h, int32_t level, const double* rho, const 
 int cav_octree_restart_level(cav_octree* h, int32_t level, const double* rho, const double* ux,
                              const double* uy, const double* t);
 int cav_octree_set_time_step(cav_octree* h, int64_t t);
+/* OCTSNAP1 files (src/octree/snapshot.rs:58-170): every level's rho, ux, uy,
+ * T and the step, written atomically; the restart (set_from_snapshot,
+ * src/octree/solver.rs:1080-1168) requires the same level layout (else
+ * CAV_ERR_ARG) and restarts the time step at 0. */
+int cav_octree_snapshot_write(cav_octree* h, const char* path, uint64_t step);
+int cav_octree_restart_from_snapshot(cav_octree* h, const char* path);
 /* One coupling on the current state: 0 = coarse_to_fine L0 -> L1,
  * 1 = fine_to_coarse L1 -> L0 + moment refresh, 2 / 3 = the same between L1
  * and L2 (src/octree/interface.rs:137-206). */

@@ -102,6 +102,7 @@ def lib():
         L.orc_dynamic_stats.argtypes = [vp, dp, dp, dp]
         L.orc_lilly_coefficient.restype = ctypes.c_double
         L.orc_lilly_coefficient.argtypes = [ctypes.c_double, ctypes.c_double]
+        L.orc_interpolate_field.argtypes = [dp, i64, i64, i64, i64, dp]
         L.orc_mixed_factor.restype = ctypes.c_double
         L.orc_mixed_factor.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double]
         i32, d = ctypes.c_int32, ctypes.c_double
@@ -133,6 +134,14 @@ def lilly_coefficient(num, den):
 
 def mixed_factor(a, b, alpha):
     return lib().orc_mixed_factor(a, b, alpha)
+
+
+def interpolate_field(src, nx0, ny0, nx1, ny1):
+    """interpolate_field (src/uniform/snapshot.rs:102-131)."""
+    s = np.ascontiguousarray(src, dtype=np.float64).reshape(nx0 * ny0)
+    d = np.empty(nx1 * ny1)
+    lib().orc_interpolate_field(_dp(s), nx0, ny0, nx1, ny1, _dp(d))
+    return d
 
 
 def feq(i, rho, ux, uy):

@@ -168,6 +168,32 @@ void orc_dynamic_stats(void* h, double* out4, double* nu_t_pre, double* alpha_t_
     if (alpha_t_pre && s.alpha_t_pre.size() == n) std::memcpy(alpha_t_pre, s.alpha_t_pre.data(), n * 8);
 }
 
+// interpolate_field, src/uniform/snapshot.rs:102-131.
+void orc_interpolate_field(const double* src, int64_t nx0, int64_t ny0, int64_t nx1, int64_t ny1, double* dst) {
+    if (nx0 == nx1 && ny0 == ny1) {
+        std::memcpy(dst, src, size_t(nx0 * ny0) * 8);
+        return;
+    }
+    for (int64_t iy = 0; iy < ny1; ++iy) {
+        const double vy = ny1 > 1 ? double(iy) / double(ny1 - 1) : 0.0;
+        const double sy = vy * double(ny0 - 1);
+        const int64_t y0 = (int64_t)std::floor(sy);
+        const int64_t y1 = std::min<int64_t>(y0 + 1, ny0 - 1);
+        const double wy = sy - double(y0);
+        for (int64_t ix = 0; ix < nx1; ++ix) {
+            const double vx = nx1 > 1 ? double(ix) / double(nx1 - 1) : 0.0;
+            const double sx = vx * double(nx0 - 1);
+            const int64_t x0 = (int64_t)std::floor(sx);
+            const int64_t x1 = std::min<int64_t>(x0 + 1, nx0 - 1);
+            const double wx = sx - double(x0);
+            const double v00 = src[y0 * nx0 + x0], v10 = src[y0 * nx0 + x1];
+            const double v01 = src[y1 * nx0 + x0], v11 = src[y1 * nx0 + x1];
+            dst[iy * nx1 + ix] = v00 * (1.0 - wx) * (1.0 - wy) + v10 * wx * (1.0 - wy) + v01 * (1.0 - wx) * wy +
+                                 v11 * wx * wy;
+        }
+    }
+}
+
 double orc_lilly_coefficient(double num, double den) { return orc::lilly_coefficient(num, den); }
 
 // mixed_factor, src/uniform/solver.rs:1195-1202.

@@ -62,6 +62,8 @@ void orc_set_dynamic_sgs(void* h, int32_t on, double smag_alpha, double nu_sm_mi
 void orc_compute_dynamic_sgs(void* h);
 void orc_dynamic_stats(void* h, double* out4, double* nu_t_pre, double* alpha_t_pre);
 double orc_lilly_coefficient(double num, double den);
+/* interpolate_field, src/uniform/snapshot.rs:102-131 (dst [nx1*ny1]). */
+void orc_interpolate_field(const double* src, int64_t nx0, int64_t ny0, int64_t nx1, int64_t ny1, double* dst);
 double orc_mixed_factor(double a, double b, double alpha);
 
 /* Equilibria and lattice weights (crate oxiphysics_lbm, pinned by
