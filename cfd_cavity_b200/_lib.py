@@ -201,6 +201,9 @@ def load(path: str | None = None):
         "cav_octree_sync": (i32, [vp]),
         "cav_octree_get_stream": (i32, [vp, ctypes.POINTER(vp)]),
         "cav_octree_launch_count": (i32, [vp, ctypes.POINTER(i64)]),
+        "cav_octree_set_dynamic_sgs": (i32, [vp, i32, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
+        "cav_octree_dynamic_stats": (i32, [vp, _dp]),
+        "cav_octree_get_nu_t": (i32, [vp, i32, _dp, _dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

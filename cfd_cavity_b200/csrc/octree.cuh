@@ -48,6 +48,7 @@ struct LvlScal {
     A a_f, b_f, a_g, c_m, c_p;           // reference (FP64) form
     A om_p, om_m, om_g, k_p, k_m;        // pairwise (FP32) form
     A beta;
+    A tp, tt;                            // tau+ and tau_t of the level (the dynamic model's base)
     // fixed-Cs Smagorinsky on the level (an extension: the reference octree
     // has none; cs = 0 is the reference)
     A cs, nu, alpha, tau_s, inv_tau_s, pr_t, inv_pr_t;
@@ -62,6 +63,14 @@ template <class A>
 struct Xi {
     A even, odd, th;
     A inv_even, inv_odd, inv_th;
+};
+
+// Per-node nu_t / alpha_t of the dynamic model for the two blocks of a launch
+// (nullptr: the level's relaxation times).
+template <class A>
+struct DynPtr {
+    const A* nut[2];
+    const A* at[2];
 };
 
 // One level (or one block of a level) as the kernels see it.
@@ -108,8 +117,27 @@ __device__ __forceinline__ const OctScal<A>& row_of(const OctScal<A>* tab, int S
 // nu_t = 0): TRT + Guo forcing for f, BGK for g.
 // ---------------------------------------------------------------------------
 template <class A, bool SHIFT>
-__device__ __forceinline__ void oct_collide(A (&f)[Q], A (&g)[Q], const Macro<A, SHIFT>& m, const LvlScal<A>& c,
-                                            A& fy_out) {
+__device__ __forceinline__ void oct_collide(A (&f)[Q], A (&g)[Q], const Macro<A, SHIFT>& m, const LvlScal<A>& c0,
+                                            A& fy_out, const A* nut = nullptr, const A* at = nullptr) {
+    LvlScal<A> c = c0;
+    if (nut) {
+        // dynamic model: relaxation times rebuilt per node from the level's
+        // tau and the node's nu_t / alpha_t (src/octree/cavity.rs:100-110)
+        const A tp = A(0.5) + A(3.0) * (c0.tp - A(0.5)) / A(3.0) + A(3.0) * *nut;
+        const A tm = A(0.5) + A(LAMBDA_TRT) / (tp - A(0.5));
+        const A tt = A(0.5) + A(3.0) * (c0.tt - A(0.5)) / A(3.0) + A(3.0) * *at;
+        c.a_f = A(0.5) * (A(1.0) / tp + A(1.0) / tm);
+        c.b_f = A(0.5) * (A(1.0) / tp - A(1.0) / tm);
+        c.a_g = A(1.0) / tt;
+        c.c_m = A(1.0) - A(0.5) / tm;
+        c.c_p = A(1.0) - A(0.5) / tp;
+        c.om_p = A(1.0) / tp;
+        c.om_m = A(1.0) / tm;
+        c.om_g = A(1.0) / tt;
+        c.k_p = c.c_p;
+        c.k_m = c.c_m;
+        c.cs = A(0.0);
+    }
     if (c.cs != A(0.0)) {
         // with the Smagorinsky extension: the uniform solver's collision
         // (collide_node, src/uniform/solver.rs:1054-1185) with the level's
@@ -345,7 +373,7 @@ __device__ __forceinline__ void split_k(int k, int nx, float inv_nx, int& x, int
 template <class St, bool COARSE>
 __global__ void __launch_bounds__(OT) k_oct_step(LvlPair<St> P, const OctScal<typename Fmt<St>::A>* __restrict__ tab,
                                                  int S, const long long* __restrict__ step_dev, int off, int lvl,
-                                                 uint32_t seed, int phase, float inv_nx) {
+                                                 uint32_t seed, int phase, float inv_nx, int collide) {
     pdl_wait();
     pdl_trigger();
     using A = typename Fmt<St>::A;
@@ -382,19 +410,20 @@ __global__ void __launch_bounds__(OT) k_oct_step(LvlPair<St> P, const OctScal<ty
     L.mac[L.n + k] = m.ux;
     L.mac[2 * L.n + k] = m.uy;
     L.mac[3 * L.n + k] = m.t;
-    if (ghost) return;
+    if (ghost || !collide) return;
     A fy_new;
     oct_collide<A, SH>(f, g, m, sc, fy_new);
     L.fy[k] = fy_new;
     store_pops<St>(L.pc_out, L.n, k, f, g, true, seed, s * 16 + phase, (long long)L.node_off + k);
 }
 
-// Collision of the REF state into PC (the first collision after the state
-// was set from the host).
+// Collision of the REF state into PC: the first collision after the state
+// was set from the host, and every collision of the dynamic model (with the
+// per-node nu_t / alpha_t of D).
 template <class St, bool COARSE>
 __global__ void __launch_bounds__(OT) k_oct_collide(LvlPair<St> P, const OctScal<typename Fmt<St>::A>* __restrict__ tab,
                                                     int S, const long long* __restrict__ step_dev, int lvl,
-                                                    uint32_t seed, int phase) {
+                                                    uint32_t seed, int phase, DynPtr<typename Fmt<St>::A> D) {
     pdl_wait();
     pdl_trigger();
     using A = typename Fmt<St>::A;
@@ -416,8 +445,10 @@ __global__ void __launch_bounds__(OT) k_oct_collide(LvlPair<St> P, const OctScal
     m.uy = L.mac[2 * L.n + k];
     m.t = L.mac[3 * L.n + k];
     m.inv_rho = A(1.0) / m.rho;
+    const A* nut = D.nut[blockIdx.y];
+    const A* at = D.at[blockIdx.y];
     A fy_new;
-    oct_collide<A, SH>(f, g, m, sc, fy_new);
+    oct_collide<A, SH>(f, g, m, sc, fy_new, nut ? nut + k : nullptr, at ? at + k : nullptr);
     L.fy[k] = fy_new;
     store_pops<St>(L.pc_out, L.n, k, f, g, true, seed, s * 16 + phase, (long long)L.node_off + k);
 }
@@ -516,8 +547,9 @@ __device__ __forceinline__ void group_sum(A (&c)[NC]) {
 template <class StC, class StF>
 __global__ void __launch_bounds__(OT) k_oct_c2f(LvlPair<StC> C, LvlPair<StF> F,
                                                 const GhostE<typename Fmt<StF>::A>* __restrict__ tab, int n_ghost,
-                                                Xi<typename Fmt<StF>::A> xi, const long long* __restrict__ step_dev,
-                                                uint32_t seed, int phase) {
+                                                Xi<typename Fmt<StF>::A> xi_h,
+                                                const Xi<typename Fmt<StF>::A>* __restrict__ xi_dev,
+                                                const long long* __restrict__ step_dev, uint32_t seed, int phase) {
     pdl_wait();
     pdl_trigger();
     using A = typename Fmt<StF>::A;
@@ -542,6 +574,7 @@ __global__ void __launch_bounds__(OT) k_oct_c2f(LvlPair<StC> C, LvlPair<StF> F,
     }
     group_sum<A, 4, 4>(c);
     if (!act || s != 0) return;
+    const Xi<A> xi = xi_dev ? xi_dev[blockIdx.y] : xi_h;
     const A rho = c[0], ux = c[1], uy = c[2], tt = c[3];
     A fn[Q], fr[Q], f[Q], g[Q];
 #pragma unroll
@@ -562,15 +595,17 @@ __global__ void __launch_bounds__(OT) k_oct_c2f(LvlPair<StC> C, LvlPair<StF> F,
 
 // fine_to_coarse (src/octree/interface.rs:175-206) + refresh of the
 // coincident node (src/octree/solver.rs:874-876, 936-942) + that node's next
-// collision into the coarser level's PC.  Four lanes per coincident node
+// collision into the coarser level's PC (not with the dynamic model, whose
+// collisions run after its own model evaluation).  Four lanes per coincident node
 // (eight nodes per warp): lane l takes the stencil nodes l, l + 4 (and 8 for
 // lane 0) in three rounds, and the round sums are added in stencil order.
 template <class StF, class StC>
 __global__ void __launch_bounds__(OT) k_oct_f2c(LvlPair<StF> F, LvlPair<StC> C, const CoinE* __restrict__ tab, int n0,
-                                                int n1, Xi<typename Fmt<StF>::A> xi,
+                                                int n1, Xi<typename Fmt<StF>::A> xi_h,
+                                                const Xi<typename Fmt<StF>::A>* __restrict__ xi_dev,
                                                 const OctScal<typename Fmt<StF>::A>* __restrict__ stab, int S,
                                                 const long long* __restrict__ step_dev, int off, int lvl_c,
-                                                uint32_t seed, int phase) {
+                                                uint32_t seed, int phase, int collide) {
     pdl_wait();
     pdl_trigger();
     using A = typename Fmt<StF>::A;
@@ -615,6 +650,7 @@ __global__ void __launch_bounds__(OT) k_oct_f2c(LvlPair<StF> F, LvlPair<StC> C, 
                 }
     }
     if (!act_e || l != 0) return;
+    const Xi<A> xi = xi_dev ? xi_dev[blk] : xi_h;
     const A rho = c[0], ux = c[1], uy = c[2], tt = c[3];
     A fn[Q], fr[Q], f[Q], g[Q];
 #pragma unroll
@@ -634,10 +670,181 @@ __global__ void __launch_bounds__(OT) k_oct_f2c(LvlPair<StF> F, LvlPair<StC> C, 
     Lc.mac[Lc.n + e.kc] = m.ux;
     Lc.mac[2 * Lc.n + e.kc] = m.uy;
     Lc.mac[3 * Lc.n + e.kc] = m.t;
+    if (!collide) return;
     A fy_new;
     oct_collide<A, SH>(f, g, m, sc, fy_new);
     Lc.fy[e.kc] = fy_new;
     store_pops<StC>(Lc.pc_out, Lc.n, e.kc, f, g, true, seed, sidx * 16 + phase + 1, (long long)Lc.node_off + e.kc);
+}
+
+// ---------------------------------------------------------------------------
+// Dynamic model: rescaling factors from the mean effective relaxation times
+// (step_cavity, src/octree/solver.rs:690-711 for xi A and :808-829 for xi B):
+// tau_eff = RelaxTimes::from_nu_alpha(nu + mean nu_t, alpha + mean alpha_t),
+// xi = rescaling_factors_multilevel(tau_eff coarser, tau_eff finer, 2,
+// odd_exact).  One CTA: each view's means in a fixed order, then thread 0.
+// ---------------------------------------------------------------------------
+template <class A>
+struct MeanView {
+    const A* nut;
+    const A* at;
+    int n;
+};
+template <class A>
+struct XiJob {
+    MeanView<A> v[4];
+    int mode;  // 0: xi A from v0 (L0) and v1 + v2 (both L1 blocks); 1: xi B of block b from v[b] (L1), v[2 + b] (L2)
+    double nu_c, al_c, nu_f, al_f;  // molecular nu / alpha of the coarser and finer level (ramped)
+    int odd_exact;
+};
+
+__device__ __forceinline__ void relax_of(double nu, double al, double& tp, double& tm, double& tt) {
+    tp = 0.5 + 3.0 * nu;
+    tm = 0.5 + LAMBDA_TRT / (tp - 0.5);
+    tt = 0.5 + 3.0 * al;
+}
+
+constexpr int DYN_PARTS = 64;  // CTAs of the dynamic model's reductions (fixed partition)
+
+// Fixed-order sum of a CTA's 256 values (deterministic).
+__device__ __forceinline__ double cta_sum(double v, double* sh) {
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+__device__ __forceinline__ double cta_max(double v, double* sh) {
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + w]);
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// Partial sums of nu_t and alpha_t: CTA (b, v) sums chunk b of view v into
+// part[(v * DYN_PARTS + b) * 2 + {0, 1}].
+template <class A>
+__global__ void __launch_bounds__(256) k_oct_mean_parts(XiJob<A> J, double* __restrict__ part) {
+    __shared__ double sh[256];
+    const MeanView<A> V = J.v[blockIdx.y];
+    const int chunk = (V.n + DYN_PARTS - 1) / DYN_PARTS;
+    const int k0 = blockIdx.x * chunk, k1 = min(V.n, k0 + chunk);
+    double a = 0.0, b = 0.0;
+    for (int k = k0 + threadIdx.x; k < k1; k += 256) {
+        a += double(V.nut[k]);
+        b += double(V.at[k]);
+    }
+    a = cta_sum(a, sh);
+    b = cta_sum(b, sh);
+    if (threadIdx.x == 0) {
+        part[(blockIdx.y * DYN_PARTS + blockIdx.x) * 2 + 0] = a;
+        part[(blockIdx.y * DYN_PARTS + blockIdx.x) * 2 + 1] = b;
+    }
+}
+
+template <class A>
+__global__ void k_oct_xi(XiJob<A> J, const double* __restrict__ part, Xi<A>* __restrict__ xi_out,
+                         double* __restrict__ xi_log) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int nv = J.mode == 0 ? 3 : 4;
+    double mean[4][2];
+    for (int v = 0; v < nv; ++v) {
+        double a = 0.0, b = 0.0;
+        for (int c = 0; c < DYN_PARTS; ++c) {
+            a += part[(v * DYN_PARTS + c) * 2 + 0];
+            b += part[(v * DYN_PARTS + c) * 2 + 1];
+        }
+        mean[v][0] = a / double(J.v[v].n);
+        mean[v][1] = b / double(J.v[v].n);
+    }
+    const int nxi = J.mode == 0 ? 1 : 2;
+    for (int b = 0; b < nxi; ++b) {
+        double ntc, atc, ntf, atf;
+        if (J.mode == 0) {
+            ntc = mean[0][0];
+            atc = mean[0][1];
+            ntf = (0.0 + mean[1][0] + mean[2][0]) / 2.0;
+            atf = (0.0 + mean[1][1] + mean[2][1]) / 2.0;
+        } else {
+            ntc = mean[b][0];
+            atc = mean[b][1];
+            ntf = mean[2 + b][0];
+            atf = mean[2 + b][1];
+        }
+        double tpc, tmc, ttc, tpf, tmf, ttf;
+        relax_of(J.nu_c + ntc, J.al_c + atc, tpc, tmc, ttc);
+        relax_of(J.nu_f + ntf, J.al_f + atf, tpf, tmf, ttf);
+        const double dt = 1.0 / 2.0;
+        const double x[3] = {dt * tpf / tpc, J.odd_exact ? dt * tmf / tmc : dt, dt * ttf / ttc};
+        Xi<A> o;
+        o.even = A(x[0]);
+        o.odd = A(x[1]);
+        o.th = A(x[2]);
+        o.inv_even = A(1.0 / x[0]);
+        o.inv_odd = A(1.0 / x[1]);
+        o.inv_th = A(1.0 / x[2]);
+        const int slot = J.mode == 0 ? 0 : b;
+        xi_out[slot] = o;
+        if (J.mode == 0) xi_out[1] = o;
+        for (int i = 0; i < 3; ++i) xi_log[3 * slot + i] = x[i];
+    }
+}
+
+// Partial statistics of the L0 model's Lilly coefficients (cs_dyn_mean /
+// _max, kappa_dyn_mean / _max, src/octree/smag.rs:369-378): CTA b writes
+// sum / max of C_nu and of C_kappa over chunk b; the host adds the parts in
+// order.
+static __global__ void __launch_bounds__(256) k_oct_sgs_parts(const double* __restrict__ W, int n,
+                                                              double* __restrict__ part) {
+    __shared__ double sh[256];
+    const long long P = n;
+    const int chunk = (n + DYN_PARTS - 1) / DYN_PARTS;
+    const int k0 = blockIdx.x * chunk, k1 = min(n, k0 + chunk);
+    double s0 = 0.0, m0 = 0.0, s1 = 0.0, m1 = 0.0;
+    for (int k = k0 + threadIdx.x; k < k1; k += 256) {
+        const double a = W[S_CNU * P + k], b = W[S_CK * P + k];
+        s0 += a;
+        m0 = fmax(m0, a);
+        s1 += b;
+        m1 = fmax(m1, b);
+    }
+    s0 = cta_sum(s0, sh);
+    m0 = cta_max(m0, sh);
+    s1 = cta_sum(s1, sh);
+    m1 = cta_max(m1, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x * 4 + 0] = s0;
+        part[blockIdx.x * 4 + 1] = m0;
+        part[blockIdx.x * 4 + 2] = s1;
+        part[blockIdx.x * 4 + 3] = m1;
+    }
+}
+
+// nu_t_max (src/octree/solver.rs:918-933): max |nu_t| over every level.
+template <class A>
+__global__ void __launch_bounds__(256) k_oct_nutmax(MeanView<A> v0, MeanView<A> v1, MeanView<A> v2, MeanView<A> v3,
+                                                    MeanView<A> v4, int nv, double* __restrict__ out) {
+    __shared__ double sh[256];
+    const MeanView<A> V[5] = {v0, v1, v2, v3, v4};
+    double m = 0.0;
+    for (int v = 0; v < nv; ++v)
+        for (int k = threadIdx.x; k < V[v].n; k += 256) m = fmax(m, fabs(double(V[v].nut[k])));
+    sh[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sh[0];
 }
 
 // ---------------------------------------------------------------------------
@@ -846,6 +1053,9 @@ struct Octree {
     virtual void restart_level(int lvl, const double* rho, const double* ux, const double* uy, const double* t) = 0;
     virtual void set_time_step(int64_t t) = 0;
     virtual void sync() = 0;
+    virtual void set_dynamic_sgs(bool on, double smag_alpha, double nu_sm_min, double eta_test) = 0;
+    virtual void dynamic_stats(double* out14) = 0;
+    virtual void get_nut(int lvl, double* nut, double* at) = 0;
 
     cav_octree_params p{};
     int levels = 2, nx0 = 0, ny0 = 0, nx1 = 0, ny1 = 0, nx2 = 0, ny2 = 0;
@@ -973,10 +1183,25 @@ struct OctImpl final : Octree {
     bool pc_valid = false;
     Xi<A> xa{}, xb{};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    // dynamic mixed-scale SGS model (set_dynamic_sgs, src/octree/solver.rs:476-481)
+    bool dyn = false;
+    double dyn_alpha = 0.5, dyn_min = -0.1, dyn_eta = 2.0;
+    double* sgs_w = nullptr;              // S_NPLANES work planes of the largest level
+    A* nut0 = nullptr;                    // nu_t_pre, then alpha_t_pre, of L0
+    A* nut1[2] = {nullptr, nullptr};      // of the L1 blocks
+    A* nut2[2] = {nullptr, nullptr};      // of the L2 strips
+    Xi<A>* xi_dev = nullptr;              // xi A (slots 0, 1), xi B hot / cold (slots 2, 3)
+    bool xi_dyn = false;                  // xi_dev holds the factors in use (a dynamic step ran)
+    double* dstat = nullptr;              // cs / kappa mean, max; nu_t_max; xi A, xi B hot, xi B cold
+    double* mpart = nullptr;              // partial sums of the xi means (4 views x DYN_PARTS x 2)
+    double* spart = nullptr;              // partial statistics of the L0 model (DYN_PARTS x 4)
+    cudaGraphExec_t dgraph[2] = {nullptr, nullptr};  // OCT_GRAPH_STEPS dynamic coarse steps
     std::vector<void*> allocs;
 
     ~OctImpl() override {
         for (auto& gx : graph)
+            if (gx) cudaGraphExecDestroy(gx);
+        for (auto& gx : dgraph)
             if (gx) cudaGraphExecDestroy(gx);
         for (void* b : allocs) cudaFree(b);
         if (stream) cudaStreamDestroy(stream);
@@ -1035,6 +1260,8 @@ struct OctImpl final : Octree {
         c.k_p = A(1.0 - 0.5 / tp);
         c.k_m = A(1.0 - 0.5 / tm);
         c.beta = A(beta);
+        c.tp = A(tp);
+        c.tt = A(tt);
         const double ts = 0.5 + 3.0 * std::fmax(nu_l, 0.002 / 3.0);
         c.cs = A(p.cs);
         c.nu = A(nu_l);
@@ -1365,64 +1592,299 @@ struct OctImpl final : Octree {
         {
             LvlPair<StC> q = pair_cur(L0, L0);
             launch(k_oct_collide<StC, true>, grid_of(L0.n, 1), q, (const OctScal<A>*)tab, S,
-                   (const long long*)step_dev, 0, seed32, 10);
+                   (const long long*)step_dev, 0, seed32, 10, DynPtr<A>{});
         }
         {
             LvlPair<StF> q = pair_cur(L1[0], L1[1]);
             launch(k_oct_collide<StF, false>, grid_of(L1[0].n, 2), q, (const OctScal<A>*)tab, S,
-                   (const long long*)step_dev, 1, seed32, 11);
+                   (const long long*)step_dev, 1, seed32, 11, DynPtr<A>{});
         }
         if (levels == 3) {
             LvlPair<StF> q = pair_cur(L2[0], L2[1]);
             launch(k_oct_collide<StF, false>, grid_of(L2[0].n, 2), q, (const OctScal<A>*)tab, S,
-                   (const long long*)step_dev, 2, seed32, 12);
+                   (const long long*)step_dev, 2, seed32, 12, DynPtr<A>{});
         }
         pc_valid = true;
     }
 
+    // The dynamic model's rescaling factors live on the device (xi_dev); the
+    // molecular ones are launch arguments.  Once a dynamic step has run, the
+    // device factors stay in use with the model off too: the reference never
+    // rewrites xi in that mode (src/octree/solver.rs:690-698).
+    const Xi<A>* xi_a_dev() const { return xi_dyn ? xi_dev : nullptr; }
+    const Xi<A>* xi_b_dev() const { return xi_dyn ? xi_dev + 2 : nullptr; }
+
     void c2f_L1() {
         LvlPair<StC> c = pair_cur(L0, L0);
         LvlPair<StF> f = pair_cur(L1[0], L1[1]);
-        launch(k_oct_c2f<StC, StF>, grid_of(4 * n_ghost, 2), c, f, (const GhostE<A>*)gh1, n_ghost, xa,
+        launch(k_oct_c2f<StC, StF>, grid_of(4 * n_ghost, 2), c, f, (const GhostE<A>*)gh1, n_ghost, xa, xi_a_dev(),
                (const long long*)step_dev, seed32, 2);
     }
     void c2f_L2() {
         LvlPair<StF> c = pair_cur(L1[0], L1[1]);
         LvlPair<StF> f = pair_cur(L2[0], L2[1]);
-        launch(k_oct_c2f<StF, StF>, grid_of(4 * n_ghost2, 2), c, f, (const GhostE<A>*)gh2, n_ghost2, xb,
+        launch(k_oct_c2f<StF, StF>, grid_of(4 * n_ghost2, 2), c, f, (const GhostE<A>*)gh2, n_ghost2, xb, xi_b_dev(),
                (const long long*)step_dev, seed32, 4);
     }
     void f2c_L2(int off) {
         LvlPair<StF> f = pair_cur(L2[0], L2[1]);
         LvlPair<StF> c = pair_cur(L1[0], L1[1]);
         launch(k_oct_f2c<StF, StF>, grid_of(4 * std::max(n_co2_0, n_co2_1), 2), f, c, (const CoinE*)co2, n_co2_0,
-               n_co2_1, xb, (const OctScal<A>*)tab, S, (const long long*)step_dev, off, 1, seed32, 7);
+               n_co2_1, xb, xi_b_dev(), (const OctScal<A>*)tab, S, (const long long*)step_dev, off, 1, seed32, 7,
+               int(!dyn));
     }
     void f2c_L1(int off) {
         LvlPair<StF> f = pair_cur(L1[0], L1[1]);
         LvlPair<StC> c = pair_cur(L0, L0);
         launch(k_oct_f2c<StF, StC>, grid_of(4 * std::max(n_co0, n_co1), 2), f, c, (const CoinE*)co1, n_co0, n_co1,
-               xa, (const OctScal<A>*)tab, S, (const long long*)step_dev, off, 0, seed32, 13);
+               xa, xi_a_dev(), (const OctScal<A>*)tab, S, (const long long*)step_dev, off, 0, seed32, 13, int(!dyn));
     }
     void step_L0() {
         LvlPair<StC> q = pair(L0, L0);
         launch(k_oct_step<StC, true>, grid_of(L0.n, 1), q, (const OctScal<A>*)tab, S, (const long long*)step_dev, 1,
-               0, seed32, 1, 1.0f / float(L0.nx));
+               0, seed32, 1, 1.0f / float(L0.nx), int(!dyn));
         L0.cur ^= 1;
     }
     void step_L1(int off, int phase) {
         LvlPair<StF> q = pair(L1[0], L1[1]);
         launch(k_oct_step<StF, false>, grid_of(L1[0].n, 2), q, (const OctScal<A>*)tab, S,
-               (const long long*)step_dev, off, 1, seed32, phase, 1.0f / float(L1[0].nx));
+               (const long long*)step_dev, off, 1, seed32, phase, 1.0f / float(L1[0].nx), int(!dyn));
         L1[0].cur ^= 1;
         L1[1].cur ^= 1;
     }
     void step_L2(int off, int phase) {
         LvlPair<StF> q = pair(L2[0], L2[1]);
         launch(k_oct_step<StF, false>, grid_of(L2[0].n, 2), q, (const OctScal<A>*)tab, S,
-               (const long long*)step_dev, off, 2, seed32, phase, 1.0f / float(L2[0].nx));
+               (const long long*)step_dev, off, 2, seed32, phase, 1.0f / float(L2[0].nx), int(!dyn));
         L2[0].cur ^= 1;
         L2[1].cur ^= 1;
+    }
+
+    // ---- dynamic mixed-scale SGS model ------------------------------------
+    void set_dynamic_sgs(bool on, double smag_alpha, double nu_sm_min, double eta_test) override {
+        if (!(smag_alpha >= 0.0 && smag_alpha <= 1.0) || !(eta_test >= 1.0) || !std::isfinite(nu_sm_min))
+            throw ArgError{CAV_ERR_ARG, "dynamic SGS: smag_alpha in [0, 1], eta_test >= 1, finite nu_sm_min"};
+        if (on && p.cs != 0.0)
+            throw ArgError{CAV_ERR_ARG, "dynamic SGS and the fixed-Cs extension (cs != 0) are exclusive"};
+        CK(cudaStreamSynchronize(stream));
+        if (on && !sgs_w) {
+            const int nmax = std::max(std::max(L0.n, L1[0].n), levels == 3 ? L2[0].n : 0);
+            sgs_w = dalloc<double>(size_t(S_NPLANES) * nmax);
+            nut0 = dalloc<A>(2 * size_t(L0.n));
+            for (int b = 0; b < 2; ++b) {
+                nut1[b] = dalloc<A>(2 * size_t(L1[b].n));
+                if (levels == 3) nut2[b] = dalloc<A>(2 * size_t(L2[b].n));
+            }
+            xi_dev = dalloc<Xi<A>>(4);
+            dstat = dalloc<double>(16);
+            mpart = dalloc<double>(size_t(4) * DYN_PARTS * 2);
+            spart = dalloc<double>(size_t(DYN_PARTS) * 4);
+            // before the first dynamic step: the molecular factors
+            double h[16] = {0, 0, 0, 0, 0, xiA[0], xiA[1], xiA[2], xiB[0], xiB[1], xiB[2], xiB[0], xiB[1], xiB[2], 0, 0};
+            CK(cudaMemcpyAsync(dstat, h, sizeof(h), cudaMemcpyHostToDevice, stream));
+            const Xi<A> x4[4] = {xa, xa, xb, xb};
+            CK(cudaMemcpyAsync(xi_dev, x4, sizeof(x4), cudaMemcpyHostToDevice, stream));
+            CK(cudaStreamSynchronize(stream));
+        }
+        // new model constants: the dynamic graphs are captured anew
+        for (auto& gx : dgraph)
+            if (gx) {
+                CK(cudaGraphExecDestroy(gx));
+                gx = nullptr;
+            }
+        // leaving the model: the molecular path collides from REF again, and
+        // its graphs are captured anew with the device factors
+        if (dyn && !on) {
+            pc_valid = false;
+            for (auto& gx : graph)
+                if (gx) {
+                    CK(cudaGraphExecDestroy(gx));
+                    gx = nullptr;
+                }
+        }
+        dyn = on;
+        dyn_alpha = smag_alpha;
+        dyn_min = nu_sm_min;
+        dyn_eta = eta_test;
+    }
+
+    template <class St>
+    void sgs_level(const Lvl<St>& L, A* nut, double tau_mol, double nu_l, double al_l) {
+        const Geom G{L.nx, L.ny, L.nx, (long long)L.n};
+        SgsParams sp;
+        const double eta = std::max(dyn_eta, 1.0);
+        sp.width = std::max((int)std::llround(eta), 1);
+        sp.dtest = eta * 1.0;
+        sp.alpha_exp = dyn_alpha;
+        sp.tau_s = tau_mol;
+        sp.nu_mol = nu_l;
+        sp.alpha_mol = al_l;
+        sp.nu_sm_min = dyn_min;
+        sp.rho_off = SH ? 1.0 : 0.0;
+        const dim3 blk(32, 4), grd((L.nx + 31) / 32, (L.ny + 3) / 4);
+        const A* mac = L.mac;
+        k_sgs_a<A><<<grd, blk, 0, stream>>>(mac + L.n, mac + 2 * L.n, mac + 3 * L.n, sgs_w, G, sp);
+        check_launch();
+        k_sgs_b<St><<<grd, blk, 0, stream>>>(L.ref[L.cur], mac, mac + L.n, mac + 2 * L.n, mac + 3 * L.n, sgs_w, G,
+                                             sp);
+        check_launch();
+        k_sgs_c<<<grd, blk, 0, stream>>>(sgs_w, G, sp);
+        check_launch();
+        k_sgs_d<A><<<grd, blk, 0, stream>>>(sgs_w, nut, nut + L.n, G, sp);
+        check_launch();
+    }
+
+    template <class St>
+    static MeanView<A> mview(const Lvl<St>& L, const A* nut) {
+        return MeanView<A>{nut, nut + L.n, L.n};
+    }
+
+    void ramp_of(int64_t s, double& nu_eff, double& al_eff) const {
+        nu_eff = nu;
+        al_eff = alpha;
+        if (nu_start_mult != 1.0) {
+            const double m = 1.0 + (nu_start_mult - 1.0) * std::exp(-double(s) / 1000.0);
+            nu_eff = nu * m;
+            al_eff = alpha * m;
+        }
+    }
+
+    // step_cavity with the dynamic model (src/octree/solver.rs:647-947): each
+    // level's model on its REF state, then its collision with the per-node
+    // nu_t / alpha_t (REF -> PC), then pull + BC + macroscopic + no-slip
+    // without the fused next collision; xi A / xi B from the mean effective
+    // taus.  Host-driven launches (the model's constants follow the ramp).
+    void dyn_coarse_step() {
+        xi_dyn = true;
+        double nu_eff, al_eff;
+        ramp_of(time_step, nu_eff, al_eff);
+        // L0 model, its coefficient statistics, xi A (L1 nu_t of the previous step)
+        sgs_level(L0, nut0, 0.5 + 3.0 * nu_eff, nu_eff, al_eff);
+        k_oct_sgs_parts<<<DYN_PARTS, 256, 0, stream>>>(sgs_w, L0.n, spart);
+        check_launch();
+        {
+            XiJob<A> J{};
+            J.v[0] = mview(L0, nut0);
+            J.v[1] = mview(L1[0], nut1[0]);
+            J.v[2] = mview(L1[1], nut1[1]);
+            J.mode = 0;
+            J.nu_c = nu_eff;
+            J.al_c = al_eff;
+            J.nu_f = 2.0 * nu_eff;
+            J.al_f = 2.0 * al_eff;
+            J.odd_exact = p.odd_exact ? 1 : 0;
+            k_oct_mean_parts<A><<<dim3(DYN_PARTS, 3), 256, 0, stream>>>(J, mpart);
+            check_launch();
+            k_oct_xi<A><<<1, 32, 0, stream>>>(J, (const double*)mpart, xi_dev, dstat + 5);
+            check_launch();
+        }
+        const DynPtr<A> d0{{nut0, nut0}, {nut0 + L0.n, nut0 + L0.n}};
+        const DynPtr<A> d1{{nut1[0], nut1[1]}, {nut1[0] + L1[0].n, nut1[1] + L1[1].n}};
+        launch(k_oct_collide<StC, true>, grid_of(L0.n, 1), pair_cur(L0, L0), (const OctScal<A>*)tab, S,
+               (const long long*)step_dev, 0, seed32, 1, d0);
+        step_L0();
+        c2f_L1();
+        const double tau_mol_l1 = 0.5 + 3.0 * 2.0 * nu_eff, tau_mol_l2 = 0.5 + 3.0 * 4.0 * nu_eff;
+        for (int b = 0; b < 2; ++b) sgs_level(L1[b], nut1[b], tau_mol_l1, 2.0 * nu_eff, 2.0 * al_eff);
+        launch(k_oct_collide<StF, false>, grid_of(L1[0].n, 2), pair_cur(L1[0], L1[1]), (const OctScal<A>*)tab, S,
+               (const long long*)step_dev, 1, seed32, 3, d1);
+        step_L1(0, 3);
+        if (levels == 3) {
+            XiJob<A> J{};
+            J.v[0] = mview(L1[0], nut1[0]);
+            J.v[1] = mview(L1[1], nut1[1]);
+            J.v[2] = mview(L2[0], nut2[0]);
+            J.v[3] = mview(L2[1], nut2[1]);
+            J.mode = 1;
+            J.nu_c = 2.0 * nu_eff;
+            J.al_c = 2.0 * al_eff;
+            J.nu_f = 4.0 * nu_eff;
+            J.al_f = 4.0 * al_eff;
+            J.odd_exact = p.odd_exact ? 1 : 0;
+            k_oct_mean_parts<A><<<dim3(DYN_PARTS, 4), 256, 0, stream>>>(J, mpart);
+            check_launch();
+            k_oct_xi<A><<<1, 32, 0, stream>>>(J, (const double*)mpart, xi_dev + 2, dstat + 8);
+            check_launch();
+            c2f_L2();
+            const DynPtr<A> d2{{nut2[0], nut2[1]}, {nut2[0] + L2[0].n, nut2[1] + L2[1].n}};
+            for (int sp = 0; sp < 2; ++sp) {
+                for (int b = 0; b < 2; ++b) sgs_level(L2[b], nut2[b], tau_mol_l2, 4.0 * nu_eff, 4.0 * al_eff);
+                launch(k_oct_collide<StF, false>, grid_of(L2[0].n, 2), pair_cur(L2[0], L2[1]),
+                       (const OctScal<A>*)tab, S, (const long long*)step_dev, 2, seed32, 5 + sp, d2);
+                step_L2(0, 5 + sp);
+            }
+            f2c_L2(0);
+        }
+        // the second L1 model takes the unramped nu / alpha (src/octree/solver.rs:882-890)
+        for (int b = 0; b < 2; ++b) sgs_level(L1[b], nut1[b], tau_mol_l1, 2.0 * nu, 2.0 * alpha);
+        launch(k_oct_collide<StF, false>, grid_of(L1[0].n, 2), pair_cur(L1[0], L1[1]), (const OctScal<A>*)tab, S,
+               (const long long*)step_dev, 1, seed32, 9, d1);
+        step_L1(0, 9);
+        f2c_L1(0);
+        k_add_step<<<1, 1, 0, stream>>>(step_dev, 1);
+        check_launch();
+    }
+
+    int64_t dyn_launches = 0;  // launches of one dynamic coarse step
+
+    void dynamic_stats(double* out) override {
+        if (!dstat) {
+            for (int i = 0; i < 5; ++i) out[i] = 0.0;
+            for (int i = 0; i < 3; ++i) out[5 + i] = xiA[i];
+            for (int b = 0; b < 2; ++b)
+                for (int i = 0; i < 3; ++i) out[8 + 3 * b + i] = levels == 3 ? xiB[i] : 0.0;
+            return;
+        }
+        const bool l3 = levels == 3;
+        k_oct_nutmax<A><<<1, 256, 0, stream>>>(mview(L0, nut0), mview(L1[0], nut1[0]), mview(L1[1], nut1[1]),
+                                               l3 ? mview(L2[0], nut2[0]) : MeanView<A>{},
+                                               l3 ? mview(L2[1], nut2[1]) : MeanView<A>{}, l3 ? 5 : 3, dstat + 4);
+        check_launch();
+        double h[14], sp[DYN_PARTS * 4];
+        CK(cudaMemcpyAsync(h, dstat, sizeof(h), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(sp, spart, sizeof(sp), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        for (int i = 0; i < 14; ++i) out[i] = h[i];
+        if (xi_dyn) {
+            double s0 = 0.0, m0 = 0.0, s1 = 0.0, m1 = 0.0;
+            for (int c = 0; c < DYN_PARTS; ++c) {
+                s0 += sp[c * 4 + 0];
+                m0 = std::fmax(m0, sp[c * 4 + 1]);
+                s1 += sp[c * 4 + 2];
+                m1 = std::fmax(m1, sp[c * 4 + 3]);
+            }
+            out[0] = s0 / double(L0.n);
+            out[1] = m0;
+            out[2] = s1 / double(L0.n);
+            out[3] = m1;
+        }
+        if (!l3)
+            for (int i = 8; i < 14; ++i) out[i] = 0.0;
+    }
+
+    void get_nut(int lvl, double* nt, double* at) override {
+        const A* src = nullptr;
+        int n = 0;
+        if (lvl == 0) {
+            src = nut0;
+            n = L0.n;
+        } else if (lvl == 1 || lvl == 2) {
+            src = nut1[lvl - 1];
+            n = L1[lvl - 1].n;
+        } else if (levels == 3 && (lvl == 3 || lvl == 4)) {
+            src = nut2[lvl - 3];
+            n = L2[lvl - 3].n;
+        } else {
+            throw ArgError{CAV_ERR_ARG, "no such level"};
+        }
+        if (!src) throw ArgError{CAV_ERR_STATE, "the dynamic model was never enabled"};
+        std::vector<A> h(2 * size_t(n));
+        CK(cudaMemcpyAsync(h.data(), src, sizeof(A) * h.size(), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        for (int k = 0; k < n; ++k) {
+            if (nt) nt[k] = double(h[k]);
+            if (at) at[k] = double(h[size_t(n) + k]);
+        }
     }
 
     // One step_cavity (src/octree/solver.rs:647-947), all launches on `stream`,
@@ -1463,8 +1925,50 @@ struct OctImpl final : Octree {
 
     int per_step_launches() const { return levels == 3 ? 10 : 6; }
 
+    // OCT_GRAPH_STEPS dynamic coarse steps in one graph: valid once the
+    // viscosity ramp has converged (the model's constants no longer change).
+    cudaGraphExec_t get_dyn_graph() {
+        cudaGraphExec_t& gx = dgraph[L0.cur];
+        if (gx) return gx;
+        const int c0 = L0.cur, c1 = L1[0].cur, c2 = L2[0].cur;
+        const int64_t l0 = launches;
+        CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        for (int j = 0; j < OCT_GRAPH_STEPS; ++j) dyn_coarse_step();
+        cudaGraph_t gr;
+        CK(cudaStreamEndCapture(stream, &gr));
+        dyn_launches = (launches - l0) / OCT_GRAPH_STEPS;
+        L0.cur = c0;
+        L1[0].cur = L1[1].cur = c1;
+        L2[0].cur = L2[1].cur = c2;
+        launches = l0;
+        CK(cudaGraphInstantiate(&gx, gr, 0));
+        cudaGraphDestroy(gr);
+        return gx;
+    }
+
     void step(int64_t n) override {
         if (n <= 0) return;
+        if (dyn) {
+            set_step_dev();
+            while (n > 0) {
+                if (n >= OCT_GRAPH_STEPS && time_step >= S) {
+                    const int64_t l0 = launches;
+                    cudaGraphExec_t gx = get_dyn_graph();
+                    CK(cudaGraphLaunch(gx, stream));
+                    launches = l0 + int64_t(OCT_GRAPH_STEPS) * dyn_launches;
+                    xi_dyn = true;
+                    time_step += OCT_GRAPH_STEPS;
+                    n -= OCT_GRAPH_STEPS;
+                } else {
+                    dyn_coarse_step();
+                    time_step += 1;
+                    n -= 1;
+                }
+                step_dev_val = time_step;
+            }
+            CK(cudaGetLastError());
+            return;
+        }
         if (!pc_valid) collide_all();
         set_step_dev();
         while (n > 0) {

@@ -302,4 +302,26 @@ int cav_octree_launch_count(cav_octree* h, int64_t* n) {
     });
 }
 
+int cav_octree_set_dynamic_sgs(cav_octree* h, int32_t on, double smag_alpha, double nu_sm_min, double eta_test) {
+    return oguarded(h, [&](Octree& o) {
+        o.set_dynamic_sgs(on != 0, smag_alpha, nu_sm_min, eta_test);
+        return CAV_OK;
+    });
+}
+
+int cav_octree_dynamic_stats(cav_octree* h, double* out14) {
+    if (!out14) return ofail(h, CAV_ERR_ARG, "null output");
+    return oguarded(h, [&](Octree& o) {
+        o.dynamic_stats(out14);
+        return CAV_OK;
+    });
+}
+
+int cav_octree_get_nu_t(cav_octree* h, int32_t level, double* nu_t, double* alpha_t) {
+    return oguarded(h, [&](Octree& o) {
+        o.get_nut(level, nu_t, alpha_t);
+        return CAV_OK;
+    });
+}
+
 }  // extern "C"

@@ -2,7 +2,9 @@
 // (compute_dynamic_sgs, src/uniform/solver.rs:562-828; box_filter / ddx /
 // ddy / lilly_coefficient :1195-1261), evaluated on the GPU before the
 // collision of a step, on the REF state (post-stream populations and
-// fields).
+// fields).  The octree runs the same kernels on each level
+// (compute_dynamic_sgs_level, src/octree/smag.rs:144-416: the same
+// algorithm with the level's tau, nu and alpha in its own lattice units).
 //
 // Four kernels, each one thread per node, every quantity in FP64 whatever
 // the storage format (the reference's arithmetic):
@@ -40,11 +42,13 @@ enum SgsPlane {
 };
 
 struct SgsParams {
-    int width;         // box width in nodes: max(round(eta_test), 1)
-    double dtest;      // test filter width eta * dx (dx = 1)
-    double alpha_exp;  // smag_alpha
-    double tau_s;      // 0.5 + 3 max(nu_eff, 0.002/3), as in the collision
-    double nu_mol, alpha_mol, nu_sm_min;
+    int width = 2;           // box width in nodes: max(round(eta_test), 1)
+    double dtest = 2.0;      // test filter width eta * dx (dx = 1)
+    double alpha_exp = 0.5;  // smag_alpha
+    double tau_s = 0.5;      // uniform: 0.5 + 3 max(nu_eff, 0.002/3), as in the collision;
+                             // octree level: 0.5 + 3 nu of the level
+    double nu_mol = 0.0, alpha_mol = 0.0, nu_sm_min = -0.1;
+    double rho_off = 0.0;    // added to the stored density (1 when the format stores rho - 1)
 };
 
 struct Window {
@@ -135,7 +139,7 @@ __global__ void __launch_bounds__(128) k_sgs_b(const St* __restrict__ pops, cons
     if (ix >= G.nx || iy >= G.ny) return;
     const long long P = G.plane;
     const int k = iy * G.pitch + ix;
-    const double rho_k = rho[k], ux_k = ux[k], uy_k = uy[k], t_k = tt[k];
+    const double rho_k = double(rho[k]) + sp.rho_off, ux_k = ux[k], uy_k = uy[k], t_k = tt[k];
     double pi_xx = 0.0, pi_xy = 0.0, pi_yy = 0.0;
 #pragma unroll
     for (int i = 0; i < Q; ++i) {

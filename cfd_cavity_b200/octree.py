@@ -17,6 +17,9 @@ import numpy as np
 from . import _lib as L
 
 COARSE, HOT_L1, COLD_L1, HOT_L2, COLD_L2 = range(5)
+OCT_DYN_KEYS = ("cs_dyn_mean", "cs_dyn_max", "kappa_dyn_mean", "kappa_dyn_max", "nu_t_max",
+                "xi_even", "xi_odd", "xi_th", "xi_b_hot_even", "xi_b_hot_odd", "xi_b_hot_th",
+                "xi_b_cold_even", "xi_b_cold_odd", "xi_b_cold_th")
 
 
 def _dp(a):
@@ -174,6 +177,28 @@ class OctreeSolver:
         n = ctypes.c_int64()
         self._ck(L.load().cav_octree_launch_count(self._h, ctypes.byref(n)))
         return n.value
+
+    def set_dynamic_sgs(self, on, smag_alpha=0.5, nu_sm_min=-0.1, eta_test=2.0):
+        """``set_dynamic_sgs`` (src/octree/solver.rs:476-481): the dynamic
+        mixed-scale model on every level (src/octree/smag.rs)."""
+        self._ck(L.load().cav_octree_set_dynamic_sgs(self._h, int(bool(on)), float(smag_alpha),
+                                                     float(nu_sm_min), float(eta_test)))
+
+    def dynamic_stats(self):
+        """``cs_dyn_mean`` / ``cs_dyn_max`` / ``kappa_dyn_mean`` /
+        ``kappa_dyn_max`` of the last L0 model, ``nu_t_max`` over every level,
+        and the rescaling factors in use (xi A, xi B of each strip)."""
+        o = np.empty(len(OCT_DYN_KEYS))
+        self._ck(L.load().cav_octree_dynamic_stats(self._h, _dp(o)))
+        return dict(zip(OCT_DYN_KEYS, o.tolist()))
+
+    def nu_t(self, lvl):
+        """(nu_t_pre, alpha_t_pre) of a level as last computed by the model."""
+        i = self.info()
+        n = i["nx"][lvl] * i["ny"][lvl]
+        a, b = np.empty(n), np.empty(n)
+        self._ck(L.load().cav_octree_get_nu_t(self._h, int(lvl), _dp(a), _dp(b)))
+        return a, b
 
     @property
     def time_step(self):

@@ -274,8 +274,7 @@ int cav_batch_get_stream(cav_batch* b, void** stream);
 int cav_batch_launch_count(cav_batch* b, int64_t* n);
 
 /* ---- block-refined (octree) cavity: src/octree/ ------------------------- */
-/* Replaces octree::solver::CavitySolver (src/octree/solver.rs:284-1206) with
- * the dynamic SGS model off (the default, src/cli.rs:117):
+/* Replaces octree::solver::CavitySolver (src/octree/solver.rs:284-1206):
  *   cav_octree_create   CavitySolver::new (solver.rs:284-471), init_cavity
  *                       (:504-578)
  *   cav_octree_step     n x step_cavity (:647-947)
@@ -376,6 +375,22 @@ int cav_octree_check_guards(cav_octree* h, double max_u_abort);
 int cav_octree_sync(cav_octree* h);
 int cav_octree_get_stream(cav_octree* h, void** stream);
 int cav_octree_launch_count(cav_octree* h, int64_t* n);
+/* set_dynamic_sgs (src/octree/solver.rs:476-481): on = 1 runs the dynamic
+ * mixed-scale model on every level before each of its collisions
+ * (compute_dynamic_sgs_level, src/octree/smag.rs:144-416) and rescales the
+ * interfaces with the mean effective relaxation times (step_cavity,
+ * solver.rs:690-711, 808-829).  CAV_ERR_ARG for smag_alpha outside [0, 1],
+ * eta_test < 1, a non-finite nu_sm_min, or on = 1 with cs != 0. */
+int cav_octree_set_dynamic_sgs(cav_octree* h, int32_t on, double smag_alpha, double nu_sm_min, double eta_test);
+/* out14: cs_dyn_mean, cs_dyn_max, kappa_dyn_mean, kappa_dyn_max (the L0
+ * model of the last step), nu_t_max (all levels), then the rescaling factors
+ * in use: xi A (even, odd, thermal), xi B of the hot strip, of the cold strip
+ * (0 with levels = 2).  Before the first dynamic step: zeros and the
+ * molecular factors. */
+int cav_octree_dynamic_stats(cav_octree* h, double* out14);
+/* nu_t_pre and alpha_t_pre of a level as last computed (CAV_ERR_STATE if the
+ * model was never enabled); either pointer may be NULL. */
+int cav_octree_get_nu_t(cav_octree* h, int32_t level, double* nu_t, double* alpha_t);
 
 /* ---- diagnostics without device allocation ------------------------------ */
 /* No counterpart in the reference.  The diagnostics of cav_diag computed on a

@@ -120,6 +120,10 @@ def lib():
         L.orc_oct_restart_level.restype = i32
         L.orc_oct_restart_level.argtypes = [vp, i32, dp, dp, dp, dp]
         L.orc_oct_set_time_step.argtypes = [vp, i64]
+        L.orc_oct_set_dynamic_sgs.argtypes = [vp, i32, d, d, d]
+        L.orc_oct_dynamic_stats.argtypes = [vp, dp]
+        L.orc_oct_get_nut.restype = i32
+        L.orc_oct_get_nut.argtypes = [vp, i32, dp, dp]
         _lib = L
     return _lib
 
@@ -380,6 +384,9 @@ OCT_INFO_KEYS = ("nu", "alpha", "beta_eff_coarse", "tau_plus_l0", "tau_plus_l1",
                  "n_ghosts")
 OCT_DIAG_KEYS = ("nu_hot", "nu_hot_link0", "nu_cold", "nu_hot_fine", "max_u", "mass",
                  "max_rho_dev", "max_rho_dev_ifaces", "finite")
+OCT_DYN_KEYS = ("cs_dyn_mean", "cs_dyn_max", "kappa_dyn_mean", "kappa_dyn_max", "nu_t_max",
+                "xi_even", "xi_odd", "xi_th", "xi_b_hot_even", "xi_b_hot_odd", "xi_b_hot_th",
+                "xi_b_cold_even", "xi_b_cold_odd", "xi_b_cold_th")
 
 
 class OracleOctree:
@@ -446,3 +453,23 @@ class OracleOctree:
         o = np.empty(len(OCT_DIAG_KEYS))
         lib().orc_oct_diag(self._h, _dp(o))
         return dict(zip(OCT_DIAG_KEYS, o.tolist()))
+
+    def set_dynamic_sgs(self, on, smag_alpha=0.5, nu_sm_min=-0.1, eta_test=2.0):
+        """set_dynamic_sgs (src/octree/solver.rs:476-481)."""
+        lib().orc_oct_set_dynamic_sgs(self._h, int(bool(on)), float(smag_alpha), float(nu_sm_min),
+                                      float(eta_test))
+
+    def dynamic_stats(self):
+        """cs_dyn_mean / _max, kappa_dyn_mean / _max (the L0 model of the last
+        step), nu_t_max (all levels) and the current rescaling factors."""
+        o = np.empty(len(OCT_DYN_KEYS))
+        lib().orc_oct_dynamic_stats(self._h, _dp(o))
+        return dict(zip(OCT_DYN_KEYS, o.tolist()))
+
+    def nu_t(self, level):
+        """(nu_t_pre, alpha_t_pre) of a level, as last computed."""
+        nx, ny = self.level_dims(level)
+        a, b = np.empty(nx * ny), np.empty(nx * ny)
+        if lib().orc_oct_get_nut(self._h, level, _dp(a), _dp(b)):
+            raise OracleError(f"no level {level}")
+        return a, b

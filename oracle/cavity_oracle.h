@@ -90,8 +90,8 @@ double orc_nusselt_from_mean(void* h, const double* t_mean, int32_t hot);
 int orc_tl_nusselt(const orc_params* p, int64_t n_steps, int64_t ws, const double* dtheta, double dcs,
                    double* J, double* dJ);
 
-/* Block-refined (octree) cavity, src/octree/solver.rs (fixed Cs, no dynamic
- * SGS).  levels 2 or 3; odd_exact selects the tau- ratio for the odd
+/* Block-refined (octree) cavity, src/octree/solver.rs (molecular, or the
+ * dynamic mixed-scale SGS model of src/octree/smag.rs).  levels 2 or 3; odd_exact selects the tau- ratio for the odd
  * rescaling.  *err = 1 on invalid arguments (CavitySolver::new asserts). */
 void* orc_oct_create(int32_t nx0, int32_t ny0, int32_t bl_width, double ra, double pr, double utarget,
                      uint64_t seed, int32_t odd_exact, int32_t levels, double nu_start_mult, int32_t has_nu,
@@ -107,6 +107,9 @@ int32_t orc_oct_restart_level(void* h, int32_t level, const double* rho, const d
                               const double* t);
 void orc_oct_set_time_step(void* h, int64_t t);
 void orc_oct_diag(void* h, double* out9);
+void orc_oct_set_dynamic_sgs(void* h, int32_t on, double smag_alpha, double nu_sm_min, double eta_test);
+void orc_oct_dynamic_stats(void* h, double* out14);
+int32_t orc_oct_get_nut(void* h, int32_t level, double* nut, double* at);
 
 #ifdef __cplusplus
 }

@@ -113,6 +113,171 @@ inline double fmax_rs(double a, double b) { return std::fmax(a, b); }
 // ---------------------------------------------------------------------------
 enum InitMode { INIT_LINEAR = 0, INIT_ZERO = 1 };
 
+// ---------------------------------------------------------------------------
+// Dynamic mixed-scale SGS model on one grid: compute_dynamic_sgs
+// (src/uniform/solver.rs:562-828) and its per-level twin
+// compute_dynamic_sgs_level (src/octree/smag.rs:144-416), which differ only
+// in where tau comes from (tau_s of the collision, or 0.5 + 3 nu of the
+// level).  Everything in lattice units of the grid (dx = 1), sequential sums.
+// ---------------------------------------------------------------------------
+struct DynSgs {
+    std::vector<double> nu_t, alpha_t;
+    double cnu_mean = 0.0, cnu_max = 0.0, ck_mean = 0.0, ck_max = 0.0;
+};
+
+// box_filter (src/uniform/solver.rs:1204-1227, src/octree/smag.rs:54-77):
+// window of `width` nodes starting half_left = (width - 1) / 2 before the
+// node, clamped at the walls.
+inline std::vector<double> box_filter(const std::vector<double>& fld, int nx, int ny, int width) {
+    std::vector<double> out(size_t(nx) * ny, 0.0);
+    const int hl = (width - 1) / 2;
+    for (int iy = 0; iy < ny; ++iy) {
+        const int y0 = std::max(iy - hl, 0), y1 = std::min(iy + width - hl, ny);
+        for (int ix = 0; ix < nx; ++ix) {
+            const int x0 = std::max(ix - hl, 0), x1 = std::min(ix + width - hl, nx);
+            double sum = 0.0;
+            for (int yy = y0; yy < y1; ++yy)
+                for (int xx = x0; xx < x1; ++xx) sum += fld[size_t(yy) * nx + xx];
+            out[size_t(iy) * nx + ix] = sum / double((y1 - y0) * (x1 - x0));
+        }
+    }
+    return out;
+}
+// ddx / ddy (src/uniform/solver.rs:1229-1245, src/octree/smag.rs:80-95):
+// central differences, one-sided by clamping at the walls.
+inline double ddx(const std::vector<double>& fld, int nx, int ix, int iy) {
+    const int xm = ix == 0 ? 0 : ix - 1, xp = ix + 1 >= nx ? nx - 1 : ix + 1;
+    return 0.5 * (fld[size_t(iy) * nx + xp] - fld[size_t(iy) * nx + xm]);
+}
+inline double ddy(const std::vector<double>& fld, int nx, int ny, int ix, int iy) {
+    const int ym = iy == 0 ? 0 : iy - 1, yp = iy + 1 >= ny ? ny - 1 : iy + 1;
+    return 0.5 * (fld[size_t(yp) * nx + ix] - fld[size_t(ym) * nx + ix]);
+}
+
+inline DynSgs dynamic_sgs_grid(int nx, int ny, const std::vector<std::array<double, Q>>& f,
+                               const std::vector<double>& rho, const std::vector<double>& ux,
+                               const std::vector<double>& uy, const std::vector<double>& T, double tau_s,
+                               double alpha_exp, double eta_test, double nu_mol, double alpha_mol,
+                               double nu_sm_min) {
+    const int n = nx * ny;
+    const double eta = std::max(eta_test, 1.0);
+    const int width = std::max((int)std::llround(eta), 1);
+    const double dx = 1.0, dtest = eta * dx, delta_t = DELTA_T;
+    auto ubx = box_filter(ux, nx, ny, width), uby = box_filter(uy, nx, ny, width);
+    auto tb = box_filter(T, nx, ny, width);
+    std::vector<double> pxx(n), pxy(n), pyy(n), ptx(n), pty(n);
+    for (int k = 0; k < n; ++k) {
+        pxx[k] = ux[k] * ux[k];
+        pxy[k] = ux[k] * uy[k];
+        pyy[k] = uy[k] * uy[k];
+        ptx[k] = ux[k] * T[k];
+        pty[k] = uy[k] * T[k];
+    }
+    auto lbuxx = box_filter(pxx, nx, ny, width), lbuxy = box_filter(pxy, nx, ny, width);
+    auto lbuyy = box_filter(pyy, nx, ny, width), lbutx = box_filter(ptx, nx, ny, width);
+    auto lbuty = box_filter(pty, nx, ny, width);
+    std::vector<double> shxx(n), shxy(n), shyy(n), smag_hat(n), sbxx(n), sbxy(n), sbyy(n), smag_bar(n),
+        gtx(n), gty(n), gbx(n), gby(n), qsm_h(n), phi_h(n), tmag_hat(n), tmag_bar(n);
+    for (int iy = 0; iy < ny; ++iy)
+        for (int ix = 0; ix < nx; ++ix) {
+            const int k = iy * nx + ix;
+            const double rho_k = rho[k], ux_k = ux[k], uy_k = uy[k], t_k = T[k];
+            double pi_xx = 0.0, pi_xy = 0.0, pi_yy = 0.0;
+            for (int i = 0; i < Q; ++i) {
+                const double cx = CX[i], cy = CY[i];
+                const double fneq = f[k][i] - feq<double>(i, rho_k, ux_k, uy_k);
+                pi_xx += fneq * cx * cx;
+                pi_xy += fneq * cx * cy;
+                pi_yy += fneq * cy * cy;
+            }
+            const double rho_m = rho_k > 1e-12 ? rho_k : 1e-12;
+            const double denom = 2.0 * CS2 * tau_s * rho_m;
+            const double pi2 = pi_xx * pi_xx + 2.0 * pi_xy * pi_xy + pi_yy * pi_yy;
+            shxx[k] = -pi_xx / denom;
+            shxy[k] = -pi_xy / denom;
+            shyy[k] = -pi_yy / denom;
+            smag_hat[k] = std::sqrt(pi2) / denom;
+            const double sxx = ddx(ubx, nx, ix, iy);
+            const double syy = ddy(uby, nx, ny, ix, iy);
+            const double sxy = 0.5 * (ddx(uby, nx, ix, iy) + ddy(ubx, nx, ny, ix, iy));
+            sbxx[k] = sxx;
+            sbxy[k] = sxy;
+            sbyy[k] = syy;
+            smag_bar[k] = std::sqrt(sxx * sxx + 2.0 * sxy * sxy + syy * syy);
+            gtx[k] = ddx(T, nx, ix, iy);
+            gty[k] = ddy(T, nx, ny, ix, iy);
+            gbx[k] = ddx(tb, nx, ix, iy);
+            gby[k] = ddy(tb, nx, ny, ix, iy);
+            const double dux = ux_k - ubx[k], duy = uy_k - uby[k];
+            const double du2 = dux * dux + duy * duy;
+            qsm_h[k] = std::sqrt(0.5 * du2) / 2.0;
+            const double dt_local = t_k - tb[k];
+            phi_h[k] = 0.5 * std::fabs(dt_local) * std::sqrt(0.5 * du2);
+            const double th_x = gtx[k] * shxx[k] + gty[k] * shxy[k];
+            const double th_y = gtx[k] * shxy[k] + gty[k] * shyy[k];
+            tmag_hat[k] = std::sqrt(2.0 * (th_x * th_x + th_y * th_y));
+            const double tb_x = gbx[k] * sbxx[k] + gby[k] * sbxy[k];
+            const double tb_y = gbx[k] * sbxy[k] + gby[k] * sbyy[k];
+            tmag_bar[k] = std::sqrt(2.0 * (tb_x * tb_x + tb_y * tb_y));
+        }
+    auto qbar_h = box_filter(qsm_h, nx, ny, width), phibar_h = box_filter(phi_h, nx, ny, width);
+    std::vector<double> num_v(n), den_v(n), num_k(n), den_k(n), nu_mix_grid(n), kap_mix_grid(n);
+    for (int k = 0; k < n; ++k) {
+        const double nu_mix_t =
+            std::pow(dtest * dtest * smag_bar[k], alpha_exp) * std::pow(dtest * qbar_h[k], 1.0 - alpha_exp);
+        const double nu_mix_g =
+            std::pow(dx * dx * smag_hat[k], alpha_exp) * std::pow(dx * qsm_h[k], 1.0 - alpha_exp);
+        const double kap_mix_t = std::pow(dtest * dtest * dtest / delta_t * tmag_bar[k], alpha_exp) *
+                                 std::pow(dtest / delta_t * phibar_h[k], 1.0 - alpha_exp);
+        const double kap_mix_g = std::pow(dx * dx * dx / delta_t * tmag_hat[k], alpha_exp) *
+                                 std::pow(dx / delta_t * phi_h[k], 1.0 - alpha_exp);
+        nu_mix_grid[k] = nu_mix_g;
+        kap_mix_grid[k] = kap_mix_g;
+        const double mxx = nu_mix_t * sbxx[k] - nu_mix_g * shxx[k];
+        const double mxy = nu_mix_t * sbxy[k] - nu_mix_g * shxy[k];
+        const double myy = nu_mix_t * sbyy[k] - nu_mix_g * shyy[k];
+        const double mx = kap_mix_t * gbx[k] - kap_mix_g * gtx[k];
+        const double my = kap_mix_t * gby[k] - kap_mix_g * gty[k];
+        const double lxx = lbuxx[k] - ubx[k] * ubx[k];
+        const double lxy = lbuxy[k] - ubx[k] * uby[k];
+        const double lyy = lbuyy[k] - uby[k] * uby[k];
+        const double lkk3 = (lxx + lyy) / 3.0;
+        const double ldxx = lxx - lkk3, ldyy = lyy - lkk3;
+        const double ljx = lbutx[k] - ubx[k] * tb[k];
+        const double ljy = lbuty[k] - uby[k] * tb[k];
+        num_v[k] = ldxx * mxx + 2.0 * lxy * mxy + ldyy * myy;
+        den_v[k] = mxx * mxx + 2.0 * mxy * mxy + myy * myy;
+        num_k[k] = ljx * mx + ljy * my;
+        den_k[k] = mx * mx + my * my;
+    }
+    auto num_v_b = box_filter(num_v, nx, ny, width), den_v_b = box_filter(den_v, nx, ny, width);
+    auto num_k_b = box_filter(num_k, nx, ny, width), den_k_b = box_filter(den_k, nx, ny, width);
+    DynSgs d;
+    d.nu_t.assign(n, 0.0);
+    d.alpha_t.assign(n, 0.0);
+    double cnu_sum = 0.0, cnu_max = 0.0, ck_sum = 0.0, ck_max = 0.0;
+    const double margin = (TAU_TRT_FLOOR - 0.5) / 3.0;
+    for (int k = 0; k < n; ++k) {
+        const double cnu = lilly_coefficient(num_v_b[k], den_v_b[k]);
+        const double ck = lilly_coefficient(num_k_b[k], den_k_b[k]);
+        cnu_sum += cnu;
+        if (cnu > cnu_max) cnu_max = cnu;
+        ck_sum += ck;
+        if (ck > ck_max) ck_max = ck;
+        const double nt = cnu * nu_mix_grid[k];
+        const double nu_t_min = fmax_rs(nu_sm_min * nu_mol, margin - nu_mol);
+        d.nu_t[k] = nt < nu_t_min ? nu_t_min : nt;
+        const double at = ck * kap_mix_grid[k];
+        const double alpha_t_min = fmax_rs(nu_sm_min * alpha_mol, margin - alpha_mol);
+        d.alpha_t[k] = at < alpha_t_min ? alpha_t_min : at;
+    }
+    d.cnu_mean = cnu_sum / double(n);
+    d.cnu_max = cnu_max;
+    d.ck_mean = ck_sum / double(n);
+    d.ck_max = ck_max;
+    return d;
+}
+
 struct Params {
     int nx = 64, ny = 256;
     double ra = 1e6, pr = 0.71, cs = 0.10, pr_t = 0.9, utarget = 0.02;
@@ -476,156 +641,19 @@ struct Solver {
     }
 
     // ---- dynamic mixed-scale SGS model, src/uniform/solver.rs:562-828 ------
-    // box_filter (:1204-1227): window of `width` nodes starting half_left
-    // = (width - 1) / 2 before the node, clamped at the walls.
-    static std::vector<double> box_filter(const std::vector<double>& fld, int nx, int ny, int width) {
-        std::vector<double> out(size_t(nx) * ny, 0.0);
-        const int hl = (width - 1) / 2;
-        for (int iy = 0; iy < ny; ++iy) {
-            const int y0 = std::max(iy - hl, 0), y1 = std::min(iy + width - hl, ny);
-            for (int ix = 0; ix < nx; ++ix) {
-                const int x0 = std::max(ix - hl, 0), x1 = std::min(ix + width - hl, nx);
-                double sum = 0.0;
-                for (int yy = y0; yy < y1; ++yy)
-                    for (int xx = x0; xx < x1; ++xx) sum += fld[size_t(yy) * nx + xx];
-                out[size_t(iy) * nx + ix] = sum / double((y1 - y0) * (x1 - x0));
-            }
-        }
-        return out;
-    }
-    // ddx / ddy (:1229-1245): central differences, one-sided by clamping at walls.
-    static double ddx(const std::vector<double>& fld, int nx, int ix, int iy) {
-        const int xm = ix == 0 ? 0 : ix - 1, xp = ix + 1 >= nx ? nx - 1 : ix + 1;
-        return 0.5 * (fld[size_t(iy) * nx + xp] - fld[size_t(iy) * nx + xm]);
-    }
-    static double ddy(const std::vector<double>& fld, int nx, int ny, int ix, int iy) {
-        const int ym = iy == 0 ? 0 : iy - 1, yp = iy + 1 >= ny ? ny - 1 : iy + 1;
-        return 0.5 * (fld[size_t(yp) * nx + ix] - fld[size_t(ym) * nx + ix]);
-    }
-
     void compute_dynamic_sgs() {
         if constexpr (std::is_same<R, double>::value) {
-            const int n = nx * ny;
             double nu_eff, alpha_eff;
             ramp_nu_alpha(time_step, nu_eff, alpha_eff);
             const double tau_s = 0.5 + 3.0 * fmax_rs(nu_eff, 0.002 / 3.0);
-            const double alpha_exp = smag_alpha;
-            const double eta = std::max(eta_test, 1.0);
-            const int width = std::max((int)std::llround(eta), 1);
-            const double dx = 1.0, dtest = eta * dx, delta_t = DELTA_T;
-            const double nu_mol = nu, alpha_mol = alpha;
-            const std::vector<double>& T = temperature;
-            auto ubx = box_filter(ux, nx, ny, width), uby = box_filter(uy, nx, ny, width);
-            auto tb = box_filter(T, nx, ny, width);
-            std::vector<double> pxx(n), pxy(n), pyy(n), ptx(n), pty(n);
-            for (int k = 0; k < n; ++k) {
-                pxx[k] = ux[k] * ux[k];
-                pxy[k] = ux[k] * uy[k];
-                pyy[k] = uy[k] * uy[k];
-                ptx[k] = ux[k] * T[k];
-                pty[k] = uy[k] * T[k];
-            }
-            auto lbuxx = box_filter(pxx, nx, ny, width), lbuxy = box_filter(pxy, nx, ny, width);
-            auto lbuyy = box_filter(pyy, nx, ny, width), lbutx = box_filter(ptx, nx, ny, width);
-            auto lbuty = box_filter(pty, nx, ny, width);
-            std::vector<double> shxx(n), shxy(n), shyy(n), smag_hat(n), sbxx(n), sbxy(n), sbyy(n), smag_bar(n),
-                gtx(n), gty(n), gbx(n), gby(n), qsm_h(n), phi_h(n), tmag_hat(n), tmag_bar(n);
-            for (int iy = 0; iy < ny; ++iy)
-                for (int ix = 0; ix < nx; ++ix) {
-                    const int k = iy * nx + ix;
-                    const double rho_k = rho[k], ux_k = ux[k], uy_k = uy[k], t_k = T[k];
-                    double pi_xx = 0.0, pi_xy = 0.0, pi_yy = 0.0;
-                    for (int i = 0; i < Q; ++i) {
-                        const double cx = CX[i], cy = CY[i];
-                        const double fneq = f[k][i] - feq<double>(i, rho_k, ux_k, uy_k);
-                        pi_xx += fneq * cx * cx;
-                        pi_xy += fneq * cx * cy;
-                        pi_yy += fneq * cy * cy;
-                    }
-                    const double rho_m = rho_k > 1e-12 ? rho_k : 1e-12;
-                    const double denom = 2.0 * CS2 * tau_s * rho_m;
-                    const double pi2 = pi_xx * pi_xx + 2.0 * pi_xy * pi_xy + pi_yy * pi_yy;
-                    shxx[k] = -pi_xx / denom;
-                    shxy[k] = -pi_xy / denom;
-                    shyy[k] = -pi_yy / denom;
-                    smag_hat[k] = std::sqrt(pi2) / denom;
-                    const double sxx = ddx(ubx, nx, ix, iy);
-                    const double syy = ddy(uby, nx, ny, ix, iy);
-                    const double sxy = 0.5 * (ddx(uby, nx, ix, iy) + ddy(ubx, nx, ny, ix, iy));
-                    sbxx[k] = sxx;
-                    sbxy[k] = sxy;
-                    sbyy[k] = syy;
-                    smag_bar[k] = std::sqrt(sxx * sxx + 2.0 * sxy * sxy + syy * syy);
-                    gtx[k] = ddx(T, nx, ix, iy);
-                    gty[k] = ddy(T, nx, ny, ix, iy);
-                    gbx[k] = ddx(tb, nx, ix, iy);
-                    gby[k] = ddy(tb, nx, ny, ix, iy);
-                    const double dux = ux_k - ubx[k], duy = uy_k - uby[k];
-                    const double du2 = dux * dux + duy * duy;
-                    qsm_h[k] = std::sqrt(0.5 * du2) / 2.0;
-                    const double dt_local = t_k - tb[k];
-                    phi_h[k] = 0.5 * std::fabs(dt_local) * std::sqrt(0.5 * du2);
-                    const double th_x = gtx[k] * shxx[k] + gty[k] * shxy[k];
-                    const double th_y = gtx[k] * shxy[k] + gty[k] * shyy[k];
-                    tmag_hat[k] = std::sqrt(2.0 * (th_x * th_x + th_y * th_y));
-                    const double tb_x = gbx[k] * sbxx[k] + gby[k] * sbxy[k];
-                    const double tb_y = gbx[k] * sbxy[k] + gby[k] * sbyy[k];
-                    tmag_bar[k] = std::sqrt(2.0 * (tb_x * tb_x + tb_y * tb_y));
-                }
-            auto qbar_h = box_filter(qsm_h, nx, ny, width), phibar_h = box_filter(phi_h, nx, ny, width);
-            std::vector<double> num_v(n), den_v(n), num_k(n), den_k(n), nu_mix_grid(n), kap_mix_grid(n);
-            for (int k = 0; k < n; ++k) {
-                const double nu_mix_t =
-                    std::pow(dtest * dtest * smag_bar[k], alpha_exp) * std::pow(dtest * qbar_h[k], 1.0 - alpha_exp);
-                const double nu_mix_g =
-                    std::pow(dx * dx * smag_hat[k], alpha_exp) * std::pow(dx * qsm_h[k], 1.0 - alpha_exp);
-                const double kap_mix_t = std::pow(dtest * dtest * dtest / delta_t * tmag_bar[k], alpha_exp) *
-                                         std::pow(dtest / delta_t * phibar_h[k], 1.0 - alpha_exp);
-                const double kap_mix_g = std::pow(dx * dx * dx / delta_t * tmag_hat[k], alpha_exp) *
-                                         std::pow(dx / delta_t * phi_h[k], 1.0 - alpha_exp);
-                nu_mix_grid[k] = nu_mix_g;
-                kap_mix_grid[k] = kap_mix_g;
-                const double mxx = nu_mix_t * sbxx[k] - nu_mix_g * shxx[k];
-                const double mxy = nu_mix_t * sbxy[k] - nu_mix_g * shxy[k];
-                const double myy = nu_mix_t * sbyy[k] - nu_mix_g * shyy[k];
-                const double mx = kap_mix_t * gbx[k] - kap_mix_g * gtx[k];
-                const double my = kap_mix_t * gby[k] - kap_mix_g * gty[k];
-                const double lxx = lbuxx[k] - ubx[k] * ubx[k];
-                const double lxy = lbuxy[k] - ubx[k] * uby[k];
-                const double lyy = lbuyy[k] - uby[k] * uby[k];
-                const double lkk3 = (lxx + lyy) / 3.0;
-                const double ldxx = lxx - lkk3, ldyy = lyy - lkk3;
-                const double ljx = lbutx[k] - ubx[k] * tb[k];
-                const double ljy = lbuty[k] - uby[k] * tb[k];
-                num_v[k] = ldxx * mxx + 2.0 * lxy * mxy + ldyy * myy;
-                den_v[k] = mxx * mxx + 2.0 * mxy * mxy + myy * myy;
-                num_k[k] = ljx * mx + ljy * my;
-                den_k[k] = mx * mx + my * my;
-            }
-            auto num_v_b = box_filter(num_v, nx, ny, width), den_v_b = box_filter(den_v, nx, ny, width);
-            auto num_k_b = box_filter(num_k, nx, ny, width), den_k_b = box_filter(den_k, nx, ny, width);
-            nu_t_pre.assign(n, 0.0);
-            alpha_t_pre.assign(n, 0.0);
-            double cnu_sum = 0.0, cnu_max = 0.0, ck_sum = 0.0, ck_max = 0.0;
-            const double margin = (TAU_TRT_FLOOR - 0.5) / 3.0;
-            for (int k = 0; k < n; ++k) {
-                const double cnu = lilly_coefficient(num_v_b[k], den_v_b[k]);
-                const double ck = lilly_coefficient(num_k_b[k], den_k_b[k]);
-                cnu_sum += cnu;
-                if (cnu > cnu_max) cnu_max = cnu;
-                ck_sum += ck;
-                if (ck > ck_max) ck_max = ck;
-                const double nt = cnu * nu_mix_grid[k];
-                const double nu_t_min = fmax_rs(nu_sm_min * nu_mol, margin - nu_mol);
-                nu_t_pre[k] = nt < nu_t_min ? nu_t_min : nt;
-                const double at = ck * kap_mix_grid[k];
-                const double alpha_t_min = fmax_rs(nu_sm_min * alpha_mol, margin - alpha_mol);
-                alpha_t_pre[k] = at < alpha_t_min ? alpha_t_min : at;
-            }
-            cs_dyn_mean = cnu_sum / double(n);
-            cs_dyn_max = cnu_max;
-            kappa_dyn_mean = ck_sum / double(n);
-            kappa_dyn_max = ck_max;
+            const DynSgs d = dynamic_sgs_grid(nx, ny, f, rho, ux, uy, temperature, tau_s, smag_alpha, eta_test, nu,
+                                              alpha, nu_sm_min);
+            nu_t_pre = d.nu_t;
+            alpha_t_pre = d.alpha_t;
+            cs_dyn_mean = d.cnu_mean;
+            cs_dyn_max = d.cnu_max;
+            kappa_dyn_mean = d.ck_mean;
+            kappa_dyn_max = d.ck_max;
         }
     }
 

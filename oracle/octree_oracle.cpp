@@ -1,12 +1,13 @@
 // octree_oracle.cpp -- TEST INFRASTRUCTURE ONLY (the oracle).
 //
 // FP64 restatement of the reference's block-refined (octree) cavity solver,
-// fixed-Cs path (no dynamic SGS): src/octree/grid.rs (tables),
+// molecular and dynamic mixed-scale SGS paths: src/octree/grid.rs (tables),
 // src/octree/interface.rs (coarse <-> fine transfers), src/octree/lbm.rs,
 // src/octree/cavity.rs (per-level physics, block-aware streaming and
 // boundary conditions, diagnostics) and src/octree/solver.rs (CavitySolver::
-// new, init_cavity, step_cavity, noise_stats).  Same arithmetic conventions
-// and parity status as cavity_oracle.hpp.
+// new, init_cavity, step_cavity, noise_stats), src/octree/smag.rs (the
+// dynamic model, shared with the uniform restatement: dynamic_sgs_grid).
+// Same arithmetic conventions and parity status as cavity_oracle.hpp.
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -247,15 +248,24 @@ static void refresh_nodes(Level& l, const std::vector<int>& nodes) {
     }
 }
 
-// collide_node_cavity, src/octree/cavity.rs:70-150 (nu_t = 0).
-static void collide_node(Pop& fn, Pop& gn, double& fy_out, double r, double u, double v, double temp, const Relax& tau,
-                         double beta, int geq_order) {
+// collide_node_cavity, src/octree/cavity.rs:70-150.  With nut / at (the
+// dynamic model's per-node nu_t / alpha_t) the relaxation times are rebuilt
+// per node (:100-110); without, the level's.
+static void collide_node(Pop& fn, Pop& gn, double& fy_out, double r, double u, double v, double temp,
+                         const Relax& tau_l, double beta, int geq_order, const double* nut = nullptr,
+                         const double* at = nullptr) {
     const double fyv = r * beta * 1.0 * (temp - 0.0);
     fy_out = fyv;
     Pop feq_, geq_;
     for (int i = 0; i < Q; ++i) {
         feq_[i] = feq<double>(i, r, u, v);
         geq_[i] = geq<double>(i, temp, u, v, geq_order);
+    }
+    Relax tau = tau_l;
+    if (nut && at) {
+        tau.tp = 0.5 + 3.0 * (tau_l.tp - 0.5) / 3.0 + 3.0 * *nut;
+        tau.tm = 0.5 + LAMBDA_TRT / (tau.tp - 0.5);
+        tau.tt = 0.5 + 3.0 * (tau_l.tt - 0.5) / 3.0 + 3.0 * *at;
     }
     const double a_f = 0.5 * (1.0 / tau.tp + 1.0 / tau.tm);
     const double b_f = 0.5 * (1.0 / tau.tp - 1.0 / tau.tm);
@@ -281,14 +291,23 @@ static void collide_node(Pop& fn, Pop& gn, double& fy_out, double r, double u, d
 
 // collide_cavity, cavity.rs:167-245.
 static void collide_level(Level& l, const Relax& tau, double beta, std::vector<double>& fy, bool interior,
-                          int geq_order) {
+                          int geq_order, const std::vector<double>* nut = nullptr,
+                          const std::vector<double>* at = nullptr) {
     const int x0 = interior ? 1 : 0, x1 = interior ? l.nx - 1 : l.nx;
     const int y0 = interior ? 1 : 0, y1 = interior ? l.ny - 1 : l.ny;
     for (int iy = y0; iy < y1; ++iy)
         for (int ix = x0; ix < x1; ++ix) {
             const int k = iy * l.nx + ix;
-            collide_node(l.f[k], l.g[k], fy[k], l.rho[k], l.ux[k], l.uy[k], l.temp[k], tau, beta, geq_order);
+            collide_node(l.f[k], l.g[k], fy[k], l.rho[k], l.ux[k], l.uy[k], l.temp[k], tau, beta, geq_order,
+                         nut ? &(*nut)[k] : nullptr, at ? &(*at)[k] : nullptr);
         }
+}
+
+// mean_field, src/octree/solver.rs:1176-1178 (sequential sum).
+static double mean_field(const std::vector<double>& v) {
+    double s = 0.0;
+    for (double x : v) s += x;
+    return s / double(v.size());
 }
 
 // update_macroscopic_guo, cavity.rs:252-325.
@@ -410,11 +429,13 @@ struct Sub {
     Relax tau;
     Xi xi_down;
     std::vector<double> fy;
+    std::vector<double> nut, at;  // nu_t_pre / alpha_t_pre of the dynamic model
 };
 struct Block {
     Grid grid;
     Level fine;
     std::vector<double> fy;
+    std::vector<double> nut, at;
     bool hot, cold;
     bool has_sub = false;
     Sub sub;
@@ -431,8 +452,14 @@ struct Octree {
     long spin_up, time_step = 0;
     std::vector<double> fy_c;
     int error = 0;
+    bool odd_exact = false;
+    // dynamic mixed-scale SGS (set_dynamic_sgs, src/octree/solver.rs:476-481)
+    bool dynamic_smag = false;
+    double smag_alpha = 0.5, nu_sm_min = -0.1, eta_test = 2.0;
+    std::vector<double> nut_c, at_c;
+    double cs_dyn_mean = 0.0, cs_dyn_max = 0.0, kappa_dyn_mean = 0.0, kappa_dyn_max = 0.0, nu_t_max = 0.0;
 
-    void init(int nx0_, int ny0_, int blw, double ra, double pr, double utarget, uint64_t seed, bool odd_exact,
+    void init(int nx0_, int ny0_, int blw, double ra, double pr, double utarget, uint64_t seed, bool odd_exact_,
               int levels_, double nu_start_mult_, int has_nu, double nu_over) {
         error = 0;
         if (blw < 2 || 2 * blw >= nx0_ || (levels_ != 2 && levels_ != 3) || ny0_ < 4) {
@@ -442,6 +469,7 @@ struct Octree {
         nx0 = nx0_;
         ny0 = ny0_;
         levels = levels_;
+        odd_exact = odd_exact_;
         const double lz = double(ny0 - 1);
         const double nu_cal = std::pow(utarget * std::sqrt(pr) * lz / (1.7 * std::sqrt(ra)), 2.0 / 3.0);
         nu = has_nu ? nu_over : std::fmax(nu_cal, 0.002);
@@ -455,6 +483,8 @@ struct Octree {
         const Xi xi_sub = xi_multilevel(tau_f, tau_s, 2, odd_exact);
         coarse.alloc(nx0, ny0);
         fy_c.assign(size_t(nx0) * ny0, 0.0);
+        nut_c.assign(size_t(nx0) * ny0, 0.0);
+        at_c.assign(size_t(nx0) * ny0, 0.0);
         blocks.clear();
         const int spec[2][4] = {{0, blw, 1, 0}, {nx0 - 1 - blw, nx0 - 1, 0, 1}};
         for (auto& sp : spec) {
@@ -462,6 +492,8 @@ struct Octree {
             b.grid.build(nx0, ny0, sp[0], 0, sp[1], ny0 - 1, false, false, false, false);
             b.fine.alloc(b.grid.nx1, b.grid.ny1);
             b.fy.assign(size_t(b.grid.nx1) * b.grid.ny1, 0.0);
+            b.nut.assign(size_t(b.grid.nx1) * b.grid.ny1, 0.0);
+            b.at.assign(size_t(b.grid.nx1) * b.grid.ny1, 0.0);
             b.hot = sp[2];
             b.cold = sp[3];
             if (levels >= 3) {
@@ -472,6 +504,8 @@ struct Octree {
                 b.sub.tau = tau_s;
                 b.sub.xi_down = xi_sub;
                 b.sub.fy.assign(size_t(b.sub.grid.nx1) * b.sub.grid.ny1, 0.0);
+                b.sub.nut.assign(size_t(b.sub.grid.nx1) * b.sub.grid.ny1, 0.0);
+                b.sub.at.assign(size_t(b.sub.grid.nx1) * b.sub.grid.ny1, 0.0);
             }
             blocks.push_back(std::move(b));
         }
@@ -551,41 +585,101 @@ struct Octree {
         return double(step) / double(spin_up);
     }
 
-    void sub_step(Level& l, const Relax& tau, double beta, std::vector<double>& fy, bool hot, bool cold) {
-        collide_level(l, tau, beta, fy, true, geq_order);
+    void sub_step(Level& l, const Relax& tau, double beta, std::vector<double>& fy, bool hot, bool cold,
+                  const std::vector<double>* nut = nullptr, const std::vector<double>* at = nullptr) {
+        collide_level(l, tau, beta, fy, true, geq_order, nut, at);
         stream_block(l, hot, cold, true, true);
         thermal_bc_block(l, hot, cold, geq_order);
         macro_guo(l, fy);
         noslip_block(l, hot, cold);
     }
 
-    // step_cavity, src/octree/solver.rs:647-947 (fixed Cs).
+    // compute_dynamic_sgs_level (src/octree/smag.rs:144-416) of one level:
+    // tau = tau_mol, nu / alpha in the level's lattice units.
+    void dyn_level(const Level& l, double tau_mol, double nu_l, double al_l, std::vector<double>& nut,
+                   std::vector<double>& at, bool stats) {
+        DynSgs d = dynamic_sgs_grid(l.nx, l.ny, l.f, l.rho, l.ux, l.uy, l.temp, tau_mol, smag_alpha, eta_test, nu_l,
+                                    al_l, nu_sm_min);
+        nut = std::move(d.nu_t);
+        at = std::move(d.alpha_t);
+        if (stats) {
+            cs_dyn_mean = d.cnu_mean;
+            cs_dyn_max = d.cnu_max;
+            kappa_dyn_mean = d.ck_mean;
+            kappa_dyn_max = d.ck_max;
+        }
+    }
+
+    // step_cavity, src/octree/solver.rs:647-947.
     void step() {
         double nu_eff, al_eff;
         ramp(time_step, nu_eff, al_eff);
         const Relax tc = Relax::from(nu_eff, al_eff);
         const Relax tf = Relax::from(2.0 * nu_eff, 2.0 * al_eff);
         const Relax ts = Relax::from(4.0 * nu_eff, 4.0 * al_eff);
+        const bool dyn = dynamic_smag;
+        if (dyn) {
+            // L0 model before the L0 collision, then xi A from the mean
+            // effective taus (L1's nu_t of the previous step) (:663-711)
+            dyn_level(coarse, 0.5 + 3.0 * nu_eff, nu_eff, al_eff, nut_c, at_c, true);
+            const double nt0 = mean_field(nut_c), at0 = mean_field(at_c);
+            double nt1 = 0.0, at1 = 0.0;
+            for (const Block& b : blocks) {
+                nt1 += mean_field(b.nut);
+                at1 += mean_field(b.at);
+            }
+            const double nb = double(blocks.size());
+            const Relax tce = Relax::from(nu_eff + nt0, al_eff + at0);
+            const Relax tfe = Relax::from(2.0 * nu_eff + nt1 / nb, 2.0 * al_eff + at1 / nb);
+            xi = xi_multilevel(tce, tfe, 2, odd_exact);
+        }
         const double br = beta_factor(time_step);
-        collide_level(coarse, tc, beta_c * br, fy_c, false, geq_order);
+        collide_level(coarse, tc, beta_c * br, fy_c, false, geq_order, dyn ? &nut_c : nullptr,
+                      dyn ? &at_c : nullptr);
         stream_plain(coarse);
         thermal_bc(coarse, geq_order);
         macro_guo(coarse, fy_c);
         noslip(coarse);
         for (Block& b : blocks) coarse_to_fine(b.grid, coarse, b.fine, xi, geq_order);
         const double bf = beta_f * br, bs = 0.25 * beta_c * br;
+        const double tau_mol_l1 = 0.5 + 3.0 * 2.0 * nu_eff, tau_mol_l2 = 0.5 + 3.0 * 4.0 * nu_eff;
         for (Block& b : blocks) {
-            sub_step(b.fine, tf, bf, b.fy, b.hot, b.cold);
+            if (dyn) dyn_level(b.fine, tau_mol_l1, 2.0 * nu_eff, 2.0 * al_eff, b.nut, b.at, false);
+            sub_step(b.fine, tf, bf, b.fy, b.hot, b.cold, dyn ? &b.nut : nullptr, dyn ? &b.at : nullptr);
             if (b.has_sub) {
+                if (dyn) {
+                    // xi B from L1's fresh and L2's previous nu_t (:808-829)
+                    const double nt1b = mean_field(b.nut), at1b = mean_field(b.at);
+                    const double nt2 = mean_field(b.sub.nut), at2 = mean_field(b.sub.at);
+                    const Relax t1e = Relax::from(2.0 * nu_eff + nt1b, 2.0 * al_eff + at1b);
+                    const Relax t2e = Relax::from(4.0 * nu_eff + nt2, 4.0 * al_eff + at2);
+                    b.sub.xi_down = xi_multilevel(t1e, t2e, 2, odd_exact);
+                }
                 coarse_to_fine(b.sub.grid, b.fine, b.sub.lvl, b.sub.xi_down, geq_order);
-                for (int sp = 0; sp < 2; ++sp) sub_step(b.sub.lvl, ts, bs, b.sub.fy, b.hot, b.cold);
+                for (int sp = 0; sp < 2; ++sp) {
+                    if (dyn) dyn_level(b.sub.lvl, tau_mol_l2, 4.0 * nu_eff, 4.0 * al_eff, b.sub.nut, b.sub.at, false);
+                    sub_step(b.sub.lvl, ts, bs, b.sub.fy, b.hot, b.cold, dyn ? &b.sub.nut : nullptr,
+                             dyn ? &b.sub.at : nullptr);
+                }
                 fine_to_coarse(b.sub.grid, b.sub.lvl, b.fine, b.sub.xi_down, geq_order);
                 std::vector<int> idx;
                 for (const CoinE& c : b.sub.grid.coin) idx.push_back(c.kc);
                 refresh_nodes(b.fine, idx);
             }
-            sub_step(b.fine, tf, bf, b.fy, b.hot, b.cold);
+            // the second L1 model takes the unramped nu / alpha (:882-890)
+            if (dyn) dyn_level(b.fine, tau_mol_l1, 2.0 * nu, 2.0 * alpha, b.nut, b.at, false);
+            sub_step(b.fine, tf, bf, b.fy, b.hot, b.cold, dyn ? &b.nut : nullptr, dyn ? &b.at : nullptr);
             fine_to_coarse(b.grid, b.fine, coarse, xi, geq_order);
+        }
+        if (dyn) {
+            double m = 0.0;
+            for (double v : nut_c) m = std::fmax(m, std::fabs(v));
+            for (const Block& b : blocks) {
+                for (double v : b.nut) m = std::fmax(m, std::fabs(v));
+                if (b.has_sub)
+                    for (double v : b.sub.nut) m = std::fmax(m, std::fabs(v));
+            }
+            nu_t_max = m;
         }
         std::vector<int> idx;
         for (const Block& b : blocks)
@@ -679,6 +773,57 @@ int32_t orc_oct_restart_level(void* h, int32_t level, const double* rho, const d
 }
 
 void orc_oct_set_time_step(void* h, int64_t t) { static_cast<Octree*>(h)->time_step = t; }
+
+// set_dynamic_sgs, src/octree/solver.rs:476-481 (no validation, as there).
+void orc_oct_set_dynamic_sgs(void* h, int32_t on, double smag_alpha, double nu_sm_min, double eta_test) {
+    Octree* o = static_cast<Octree*>(h);
+    o->dynamic_smag = on != 0;
+    o->smag_alpha = smag_alpha;
+    o->nu_sm_min = nu_sm_min;
+    o->eta_test = eta_test;
+}
+
+// out: cs_dyn_mean, cs_dyn_max, kappa_dyn_mean, kappa_dyn_max, nu_t_max,
+// xi A (even, odd, th), xi B hot (even, odd, th), xi B cold (even, odd, th).
+void orc_oct_dynamic_stats(void* h, double* out) {
+    Octree* o = static_cast<Octree*>(h);
+    out[0] = o->cs_dyn_mean;
+    out[1] = o->cs_dyn_max;
+    out[2] = o->kappa_dyn_mean;
+    out[3] = o->kappa_dyn_max;
+    out[4] = o->nu_t_max;
+    out[5] = o->xi.even;
+    out[6] = o->xi.odd;
+    out[7] = o->xi.th;
+    for (int b = 0; b < 2; ++b) {
+        const bool l3 = o->levels >= 3;
+        out[8 + 3 * b] = l3 ? o->blocks[b].sub.xi_down.even : 0.0;
+        out[9 + 3 * b] = l3 ? o->blocks[b].sub.xi_down.odd : 0.0;
+        out[10 + 3 * b] = l3 ? o->blocks[b].sub.xi_down.th : 0.0;
+    }
+}
+
+// nu_t_pre and alpha_t_pre of a level (0 = L0, 1/2 = L1 hot/cold, 3/4 = L2).
+int32_t orc_oct_get_nut(void* h, int32_t level, double* nut, double* at) {
+    Octree* o = static_cast<Octree*>(h);
+    const std::vector<double>* a = nullptr;
+    const std::vector<double>* b = nullptr;
+    if (level == 0) {
+        a = &o->nut_c;
+        b = &o->at_c;
+    } else if (level == 1 || level == 2) {
+        a = &o->blocks[level - 1].nut;
+        b = &o->blocks[level - 1].at;
+    } else if (o->levels >= 3 && (level == 3 || level == 4)) {
+        a = &o->blocks[level - 3].sub.nut;
+        b = &o->blocks[level - 3].sub.at;
+    } else {
+        return 1;
+    }
+    if (nut) std::memcpy(nut, a->data(), a->size() * 8);
+    if (at) std::memcpy(at, b->data(), b->size() * 8);
+    return 0;
+}
 
 // out: nu (L0 lattice), alpha, beta_c, tau+ L0, tau+ L1, tau+ L2, xi_even A,
 // xi_odd A, xi_th A, xi_even B, time_step, coincident L0 count, ghost count.
