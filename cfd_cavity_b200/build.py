@@ -1,4 +1,5 @@
-"""Builds the CUDA library ``libcavity_b200.so`` in-tree for sm_100a.
+"""Builds the CUDA library ``libcavity_b200.so`` in-tree for sm_100a, and the
+driver binary ``cavity_les`` (host C++ over the library's C ABI).
 
 Each translation unit is compiled by nvcc with
 ``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3``; the FP64 units
@@ -18,6 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT, "libcavity_b200.so")
+DRIVER = os.path.join(OUT, "cavity_les")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
                  "-I" + os.path.join(HERE, "..", "include"), "--expt-relaxed-constexpr"]
@@ -79,6 +81,12 @@ def build(force: bool = False, verbose: bool = False, extra_flags=()) -> str:
         list(ex.map(run, jobs))
     if jobs or not os.path.exists(LIB):
         run([nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"])
+    drv_src = [os.path.join(CSRC, "driver.cpp"), os.path.join(CSRC, "rustfmt.h"),
+               os.path.join(HERE, "..", "include", "cavity.h")]
+    if force or _sources_newer(DRIVER, drv_src + [LIB, __file__]):
+        run([shutil.which("g++") or "g++", "-std=c++17", "-O2", "-Wall", "-Wextra",
+             "-I" + os.path.join(HERE, "..", "include"), "-I" + CSRC, drv_src[0], "-o", DRIVER,
+             "-L" + OUT, "-lcavity_b200", "-Wl,-rpath,$ORIGIN"])
     return LIB
 
 
