@@ -128,16 +128,18 @@ class CavityBatch:
     def tuning(self):
         t = L.CavBatchTuning()
         self._ck(L.load().cav_batch_get_tuning(self._b, ctypes.byref(t)))
-        return {"rows_per_item": t.rows_per_item, "ctas_per_sm": t.ctas_per_sm}
+        return {"rows_per_item": t.rows_per_item, "ctas_per_sm": t.ctas_per_sm, "tiles": t.tiles}
 
-    def set_tuning(self, rows_per_item, ctas_per_sm):
-        t = L.CavBatchTuning(rows_per_item, ctas_per_sm)
+    def set_tuning(self, rows_per_item, ctas_per_sm, tiles=1):
+        """rows_per_item / ctas_per_sm of the global-memory kernel (tiles=0),
+        or the grid of the TMA tile kernel in tile shape 1 (the default) or 2."""
+        t = L.CavBatchTuning(rows_per_item, ctas_per_sm, int(tiles))
         self._ck(L.load().cav_batch_set_tuning(self._b, ctypes.byref(t)))
 
     def autotune(self, trial_steps=64):
         t = L.CavBatchTuning()
         self._ck(L.load().cav_batch_autotune(self._b, int(trial_steps), ctypes.byref(t)))
-        return {"rows_per_item": t.rows_per_item, "ctas_per_sm": t.ctas_per_sm}
+        return {"rows_per_item": t.rows_per_item, "ctas_per_sm": t.ctas_per_sm, "tiles": t.tiles}
 
     def sync(self):
         self._ck(L.load().cav_batch_sync(self._b))

@@ -16,6 +16,7 @@
 #pragma once
 
 #include "solver.cuh"
+#include "tile.cuh"
 
 namespace cav {
 
@@ -66,6 +67,7 @@ __global__ void __launch_bounds__(BATCH_THREADS)
 struct BatchTuning {
     int rows_per_item = 8;
     int ctas_per_sm = 8;
+    int tiles = 1;  // 1, 2: the TMA tile kernel (k_tile) in tile shape 1 or 2; 0: k_batch
 };
 
 struct BatchBase {
@@ -96,10 +98,19 @@ struct Batch final : BatchBase {
     int n_items = 0, grid = 0, n_sm = 0, table_rows = 0;
     cudaGraphExec_t graph = nullptr;
     bool cavs_dirty = true;
+    // the tile kernel (tile.cuh)
+    TileCav<St>* d_tcavs = nullptr;
+    CUtensorMap* d_maps[3] = {nullptr, nullptr, nullptr};   // per tile shape
+    TileItem* d_titems[3] = {nullptr, nullptr, nullptr};
+    unsigned* d_err = nullptr;
+    unsigned* h_err = nullptr;  // pinned copy of *d_err
+    int n_titems[3] = {0, 0, 0}, tgrid = 0;
 
     ~Batch() override {
         if (graph) cudaGraphExecDestroy(graph);
-        void* bufs[] = {d_cavs, d_items, d_table, step_dev};
+        if (h_err) cudaFreeHost(h_err);
+        void* bufs[] = {d_cavs,     d_items,     d_table,     step_dev,    d_tcavs, d_maps[1],
+                        d_maps[2], d_titems[1], d_titems[2], d_err};
         for (void* b : bufs)
             if (b) cudaFree(b);
         for (Solver* s : cavs) delete s;
@@ -127,12 +138,53 @@ struct Batch final : BatchBase {
                            stream));
         CK(cudaMalloc(&d_cavs, sizeof(BatchCav<St>) * n));
         CK(cudaMalloc(&step_dev, sizeof(long long)));
+        CK(cudaMalloc(&d_tcavs, sizeof(TileCav<St>) * n));
+        CK(cudaMalloc(&d_err, sizeof(unsigned)));
+        CK(cudaMemsetAsync(d_err, 0, sizeof(unsigned), stream));
+        CK(cudaMallocHost(&h_err, sizeof(unsigned)));
+        *h_err = 0;
+        setup_tiles<1>();
+        setup_tiles<2>();
         set_tuning(tun);
         CK(cudaStreamSynchronize(stream));
     }
 
+    // Tensor maps of both population buffers of every cavity and the tile
+    // list, for tile shape V.
+    template <int V>
+    void setup_tiles() {
+        const int n = int(cv.size());
+        std::vector<CUtensorMap> maps(2 * size_t(n));
+        for (int i = 0; i < n; ++i)
+            for (int b = 0; b < 2; ++b) maps[2 * size_t(i) + b] = make_tile_map<St, V>(cv[i]->pop[b], cv[i]->G);
+        CK(cudaMalloc(&d_maps[V], sizeof(CUtensorMap) * maps.size()));
+        CK(cudaMemcpyAsync(d_maps[V], maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice,
+                           stream));
+        std::vector<std::pair<int, int>> sizes;
+        for (auto* c : cv) sizes.push_back({c->p.nx, c->p.ny});
+        std::vector<TileItem> ti;
+        tile_items(sizes, TileShape<St, V>::TY, ti);
+        n_titems[V] = int(ti.size());
+        CK(cudaMalloc(&d_titems[V], sizeof(TileItem) * ti.size()));
+        CK(cudaMemcpyAsync(d_titems[V], ti.data(), sizeof(TileItem) * ti.size(), cudaMemcpyHostToDevice, stream));
+        CK(cudaFuncSetAttribute(k_tile<St, V, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                TileShape<St, V>::SMEM));
+        CK(cudaFuncSetAttribute(k_tile<St, V, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                TileShape<St, V>::SMEM));
+        CK(cudaStreamSynchronize(stream));
+    }
+
+    template <int V>
+    int tile_grid(int ctas_per_sm) {
+        int occ = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tile<St, V, false, false>, TileShape<St, V>::THREADS,
+                                                         TileShape<St, V>::SMEM));
+        return std::max(1, std::min(n_titems[V], std::max(1, std::min(ctas_per_sm, occ)) * n_sm));
+    }
+
     void set_tuning(const BatchTuning& t) override {
-        if (t.rows_per_item < 1 || t.rows_per_item > 1024 || t.ctas_per_sm < 1 || t.ctas_per_sm > 32)
+        if (t.rows_per_item < 1 || t.rows_per_item > 1024 || t.ctas_per_sm < 1 || t.ctas_per_sm > 32 ||
+            t.tiles < 0 || t.tiles > 2)
             throw ArgError{CAV_ERR_ARG, "tuning out of range"};
         tun = t;
         std::vector<BatchItem> items;
@@ -147,6 +199,8 @@ struct Batch final : BatchBase {
         CK(cudaMemcpyAsync(d_items, items.data(), sizeof(BatchItem) * items.size(), cudaMemcpyHostToDevice,
                            stream));
         grid = std::max(1, std::min(n_items, t.ctas_per_sm * n_sm));
+        if (t.tiles == 1) tgrid = tile_grid<1>(t.ctas_per_sm);
+        if (t.tiles == 2) tgrid = tile_grid<2>(t.ctas_per_sm);
         if (graph) {
             cudaGraphExecDestroy(graph);
             graph = nullptr;
@@ -186,12 +240,51 @@ struct Batch final : BatchBase {
                 h[i].spin_up = int(c->spin_up);
             }
             CK(cudaMemcpyAsync(d_cavs, h.data(), sizeof(BatchCav<St>) * h.size(), cudaMemcpyHostToDevice, stream));
+            std::vector<TileCav<St>> t(cv.size());
+            for (size_t i = 0; i < cv.size(); ++i) {
+                t[i].pop[0] = h[i].pop[0];
+                t[i].pop[1] = h[i].pop[1];
+                t[i].fy = h[i].fy;
+                t[i].nut = h[i].nut;
+                t[i].acc_hot = nullptr;
+                t[i].acc_cold = nullptr;
+                t[i].G = h[i].G;
+                t[i].parity = h[i].parity;
+                t[i].spin_up = h[i].spin_up;
+            }
+            CK(cudaMemcpyAsync(d_tcavs, t.data(), sizeof(TileCav<St>) * t.size(), cudaMemcpyHostToDevice, stream));
             CK(cudaStreamSynchronize(stream));
             cavs_dirty = false;
         }
     }
 
+    template <int V, bool WN>
+    void launch_tiles(const long long* sdev, long long step) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(tgrid);
+        cfg.blockDim = dim3(TileShape<St, V>::THREADS);
+        cfg.dynamicSmemBytes = TileShape<St, V>::SMEM;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CK(cudaLaunchKernelEx(&cfg, k_tile<St, V, WN, false>, (const TileCav<St>*)d_tcavs,
+                              (const CUtensorMap*)d_maps[V], (const TileItem*)d_titems[V], n_titems[V],
+                              (const StepScalars<A>*)d_table, int(cv.size()), step, sdev, d_err));
+    }
+
     void launch(bool write_nut, const long long* sdev, long long step) {
+        if (tun.tiles) {
+            if (tun.tiles == 1)
+                write_nut ? launch_tiles<1, true>(sdev, step) : launch_tiles<1, false>(sdev, step);
+            else
+                write_nut ? launch_tiles<2, true>(sdev, step) : launch_tiles<2, false>(sdev, step);
+            ++launches;
+            CK(cudaGetLastError());
+            return;
+        }
         if (write_nut)
             k_batch<St, true><<<grid, BATCH_THREADS, 0, stream>>>(d_cavs, d_items, n_items, d_table, int(cv.size()),
                                                                    step, sdev);
@@ -263,6 +356,7 @@ struct Batch final : BatchBase {
         step(steps);
         CK(cudaEventRecord(b, stream));
         CK(cudaEventSynchronize(b));
+        check_err();
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, a, b));
         cudaEventDestroy(a);
@@ -270,7 +364,14 @@ struct Batch final : BatchBase {
         return ms;
     }
 
-    void sync() override { CK(cudaStreamSynchronize(stream)); }
+    // A tile CTA that gave up waiting for its copies (k_tile) sets *d_err.
+    void check_err() {
+        CK(cudaMemcpyAsync(h_err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        if (*h_err) throw ArgError{CAV_ERR_TIMEOUT, "a tile copy did not complete within its bounded wait"};
+    }
+
+    void sync() override { check_err(); }
 };
 
 }  // namespace cav

@@ -589,6 +589,7 @@ int cav_batch_get_tuning(cav_batch* b, cav_batch_tuning* t) {
     return bguarded(b, [&](BatchBase& x) {
         t->rows_per_item = x.tun.rows_per_item;
         t->ctas_per_sm = x.tun.ctas_per_sm;
+        t->tiles = x.tun.tiles;
     });
 }
 
@@ -598,6 +599,7 @@ int cav_batch_set_tuning(cav_batch* b, const cav_batch_tuning* t) {
         BatchTuning bt;
         bt.rows_per_item = t->rows_per_item;
         bt.ctas_per_sm = t->ctas_per_sm;
+        bt.tiles = t->tiles;
         x.set_tuning(bt);
     });
 }
@@ -614,22 +616,35 @@ int cav_batch_autotune(cav_batch* b, int32_t trial_steps, cav_batch_tuning* chos
             ps.push_back(p);
         }
         std::unique_ptr<BatchBase> twin(build_batch(ps.data(), int(ps.size())));
-        const int rows_c[] = {2, 4, 8, 16, 32};
-        const int ctas_c[] = {4, 8, 12, 16};
-        BatchTuning best = x.tun;
-        double best_ms = 1e300;
-        for (int r : rows_c)
-            for (int c : ctas_c) {
+        // candidates: the global-memory kernel over tile heights and grid
+        // sizes, then the shared-memory tile kernel over its grid sizes
+        std::vector<BatchTuning> cand;
+        for (int r : {2, 4, 8, 16, 32})
+            for (int c : {4, 8, 12, 16}) {
                 BatchTuning t;
                 t.rows_per_item = r;
                 t.ctas_per_sm = c;
-                twin->set_tuning(t);
-                double ms = twin->time_steps(trial_steps);
-                if (ms < best_ms) {
-                    best_ms = ms;
-                    best = t;
-                }
+                t.tiles = 0;
+                cand.push_back(t);
             }
+        for (int v : {1, 2})
+            for (int c : {1, 2, 3, 4}) {
+                BatchTuning t;
+                t.rows_per_item = x.tun.rows_per_item;
+                t.ctas_per_sm = c;
+                t.tiles = v;
+                cand.push_back(t);
+            }
+        BatchTuning best = x.tun;
+        double best_ms = 1e300;
+        for (const BatchTuning& t : cand) {
+            twin->set_tuning(t);
+            double ms = twin->time_steps(trial_steps);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = t;
+            }
+        }
         x.set_tuning(best);
         {
             std::lock_guard<std::mutex> lk(g_tune_mutex);
@@ -638,6 +653,7 @@ int cav_batch_autotune(cav_batch* b, int32_t trial_steps, cav_batch_tuning* chos
         if (chosen) {
             chosen->rows_per_item = best.rows_per_item;
             chosen->ctas_per_sm = best.ctas_per_sm;
+            chosen->tiles = best.tiles;
         }
     });
 }

@@ -154,26 +154,30 @@ __device__ __forceinline__ bool is_wall(const Geom& G, int ix, int iy) {
 // array in the production step, where every node reads then rewrites its own
 // entry; separate arrays when states are kept, as in the adjoint's
 // recomputation).
-template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE>
-__device__ __forceinline__ void fused_node_io(const St* __restrict__ src, St* __restrict__ dst,
-                                              const typename Fmt<St>::A* fy_in, typename Fmt<St>::A* fy_out,
-                                              typename Fmt<St>::A* __restrict__ nut, double* __restrict__ acc_hot,
-                                              double* __restrict__ acc_cold, const Geom& G, int ix, int iy,
-                                              const StepScalars<typename Fmt<St>::A>& c) {
+// Everything of the step after the pull (f, g streamed into the node):
+// macroscopic, no-slip, the Nusselt accumulation (t_at(x) gives T of the
+// streamed state at column x of the same row), the collision, the stores.
+// Shared by the global-memory pull (fused_node_io) and the shared-memory
+// tiles (tile.cuh), so both give the same bits.
+template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE, class TAt>
+__device__ __forceinline__ void fused_core(typename Fmt<St>::A (&f)[Q], typename Fmt<St>::A (&g)[Q],
+                                           St* __restrict__ dst, const typename Fmt<St>::A* fy_in,
+                                           typename Fmt<St>::A* fy_out, typename Fmt<St>::A* __restrict__ nut,
+                                           double* __restrict__ acc_hot, double* __restrict__ acc_cold,
+                                           const Geom& G, int ix, int iy, const StepScalars<typename Fmt<St>::A>& c,
+                                           TAt&& t_at) {
     using A = typename Fmt<St>::A;
     constexpr bool SH = Fmt<St>::SHIFT;
     const int k = iy * G.pitch + ix;
-    A f[Q], g[Q];
-    pull_node<St>(src, G, ix, iy, c, f, g);
     const bool wall = is_wall(G, ix, iy);
     Macro<A, SH> m = macro_node<A, SH>(f, g, fy_in[k], wall);
     if (ACC_NU) {
         if (ix == 1) {
-            A t2 = gather_t<St>(src, G, 2, iy, c);
+            A t2 = t_at(2);
             acc_hot[iy] += fabs(double(m.t) - double(t2));
         }
         if (ix == G.nx - 2) {
-            A t0 = gather_t<St>(src, G, G.nx - 3, iy, c);
+            A t0 = t_at(G.nx - 3);
             acc_cold[iy] += fabs(double(m.t) - double(t0));
         }
     }
@@ -184,6 +188,19 @@ __device__ __forceinline__ void fused_node_io(const St* __restrict__ src, St* __
         if (WRITE_NUT) nut[k] = nutv;
     }
     store_node<St>(dst, G, iy, ix, f, g, c);
+}
+
+template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE>
+__device__ __forceinline__ void fused_node_io(const St* __restrict__ src, St* __restrict__ dst,
+                                              const typename Fmt<St>::A* fy_in, typename Fmt<St>::A* fy_out,
+                                              typename Fmt<St>::A* __restrict__ nut, double* __restrict__ acc_hot,
+                                              double* __restrict__ acc_cold, const Geom& G, int ix, int iy,
+                                              const StepScalars<typename Fmt<St>::A>& c) {
+    using A = typename Fmt<St>::A;
+    A f[Q], g[Q];
+    pull_node<St>(src, G, ix, iy, c, f, g);
+    fused_core<St, WRITE_NUT, ACC_NU, NO_COLLIDE>(f, g, dst, fy_in, fy_out, nut, acc_hot, acc_cold, G, ix, iy, c,
+                                                  [&](int x) { return gather_t<St>(src, G, x, iy, c); });
 }
 
 template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE>

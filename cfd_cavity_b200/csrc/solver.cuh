@@ -33,6 +33,7 @@
 
 #include "../../include/cavity.h"
 #include "adjoint.cuh"
+#include "errors.cuh"
 #include "diag.cuh"
 #include "kernels.cuh"
 #include "sgs.cuh"
@@ -56,22 +57,6 @@ struct Rng {
         return x * 0x2545F4914F6CDD1Dull;
     }
     double next_f64() { return double(next_u64() >> 11) / double(1ull << 53); }
-};
-
-struct CudaError {
-    cudaError_t e;
-    const char* where;
-};
-
-#define CK(call)                                               \
-    do {                                                       \
-        cudaError_t _e = (call);                               \
-        if (_e != cudaSuccess) throw CudaError{_e, #call};     \
-    } while (0)
-
-struct ArgError {
-    int code;
-    std::string msg;
 };
 
 // Lattice units of CavitySolver::new (src/uniform/solver.rs:123-154).

@@ -250,8 +250,12 @@ int cav_adjoint_run(cav_handle* h, const cav_adjoint_spec* spec, double* grad_th
  * bit-identically to the same cavity created with cav_create. */
 typedef struct cav_batch cav_batch;
 typedef struct cav_batch_tuning {
-    int32_t rows_per_item; /* tile height (tiles are 32 columns wide)        */
-    int32_t ctas_per_sm;   /* persistent grid = ctas_per_sm x #SMs CTAs     */
+    int32_t rows_per_item; /* tile height of k_batch (tiles are 32 columns wide) */
+    int32_t ctas_per_sm;   /* persistent grid = ctas_per_sm x #SMs CTAs (the tile
+                              kernel: at most its resident CTAs per SM)          */
+    int32_t tiles;         /* 1, 2: TMA-staged shared-memory tiles in shape 1
+                              (default) or 2 (taller); 0: one thread per node
+                              from global memory                                 */
 } cav_batch_tuning;
 int cav_batch_create(const cav_params* params, int32_t n, cav_batch** out);
 int cav_batch_destroy(cav_batch* b);

@@ -40,17 +40,26 @@ def test_batch_is_bitwise_equal_to_single_cavities(precision):
         assert np.array_equal(pb[0], ps[0]) and np.array_equal(pb[1], ps[1])
 
 
-def test_batch_tuning_does_not_change_results():
-    a = CavityBatch(MIXED, precision="f16sr")
-    b = CavityBatch(MIXED, precision="f16sr")
-    a.set_tuning(3, 2)
-    b.set_tuning(32, 16)
+@pytest.mark.parametrize("precision", ["f64", "f32", "f16sr", "bf16", "f16gsr"])
+def test_batch_tuning_does_not_change_results(precision):
+    """Tile heights, grid sizes and the kernel (TMA-staged shared-memory tiles
+    or one thread per node from global memory) change no bit."""
+    a = CavityBatch(MIXED, precision=precision)
+    b = CavityBatch(MIXED, precision=precision)
+    a.set_tuning(3, 2, tiles=0)
+    b.set_tuning(32, 16, tiles=1)
     a.step(90)
     b.step(40)
-    b.set_tuning(5, 7)
-    b.step(50)
+    b.set_tuning(5, 7, tiles=0)
+    b.step(20)
+    b.set_tuning(5, 1, tiles=2)
+    b.step(30)
     for i in range(len(MIXED)):
-        assert np.array_equal(a.fields(i)["temperature"], b.fields(i)["temperature"])
+        fa, fb = a.fields(i), b.fields(i)
+        for k in fa:
+            assert np.array_equal(fa[k], fb[k]), (i, k)
+        pa, pb = a.populations(i), b.populations(i)
+        assert np.array_equal(pa[0], pb[0]) and np.array_equal(pa[1], pb[1])
 
 
 def test_autotune_picks_a_candidate_and_leaves_the_state_alone():
@@ -59,7 +68,11 @@ def test_autotune_picks_a_candidate_and_leaves_the_state_alone():
     b.step(10)
     ref.step(10)
     t = b.autotune(trial_steps=16)
-    assert t["rows_per_item"] in (2, 4, 8, 16, 32) and t["ctas_per_sm"] in (4, 8, 12, 16)
+    assert t["tiles"] in (0, 1, 2)
+    if t["tiles"] == 0:
+        assert t["rows_per_item"] in (2, 4, 8, 16, 32) and t["ctas_per_sm"] in (4, 8, 12, 16)
+    else:
+        assert t["ctas_per_sm"] in (1, 2, 3, 4)
     assert b.tuning() == t
     assert b.info()["time_step"] == 10
     b.step(70)
