@@ -304,6 +304,21 @@ __global__ void __launch_bounds__(256) k_materialize(const St* __restrict__ src,
 // init_from_fields (src/uniform/solver.rs:232-262) on the device: fields
 // from dense FP64 arrays (k = iy*nx + ix), populations their equilibria, then
 // no-slip on the stored velocity (the populations keep the given u).
+// feq_full / geq_full in FP64 with explicit round-to-nearest operations (no
+// contraction in any translation unit): the host's init_from_fields
+// arithmetic bit for bit, in the reference's expression order.
+__device__ __forceinline__ double eq_rn(int i, double a, double ux, double uy, int order) {
+    const double cs2 = CS2;
+    const double eu = __dadd_rn(__dmul_rn(double(CX(i)), ux), __dmul_rn(double(CY(i)), uy));
+    double br = __dadd_rn(1.0, __ddiv_rn(eu, cs2));
+    if (order != 1) {
+        const double u2 = __dadd_rn(__dmul_rn(ux, ux), __dmul_rn(uy, uy));
+        br = __dadd_rn(br, __ddiv_rn(__dmul_rn(eu, eu), __dmul_rn(__dmul_rn(2.0, cs2), cs2)));
+        br = __dsub_rn(br, __ddiv_rn(u2, __dmul_rn(2.0, cs2)));
+    }
+    return __dmul_rn(__dmul_rn(WD(i), a), br);
+}
+
 template <class St>
 __global__ void __launch_bounds__(256) k_init_eq(const double* __restrict__ r, const double* __restrict__ u,
                                                  const double* __restrict__ v, const double* __restrict__ t,
@@ -321,16 +336,25 @@ __global__ void __launch_bounds__(256) k_init_eq(const double* __restrict__ r, c
     const double rk = r[kd], uk = u[kd], vk = v[kd], tk = t[kd];
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
-        double fv = feq_full<double>(i, rk, uk, vk);
-        if (SH) fv -= WD(i);
+        double fv = eq_rn(i, rk, uk, vk, 2);
+        if (SH) fv = __dsub_rn(fv, WD(i));
         stp(dst, G, i, iy, ix, A(fv));
-        stp(dst, G, Q + i, iy, ix, A(geq_full<double>(i, tk, uk, vk, geq_order)));
+        stp(dst, G, Q + i, iy, ix, A(eq_rn(i, tk, uk, vk, geq_order)));
     }
     const bool wall = is_wall(G, ix, iy);
     rho[k] = A(rk);
     ux[k] = wall ? A(0.0) : A(uk);
     uy[k] = wall ? A(0.0) : A(vk);
     tt[k] = A(tk);
+}
+
+// A pitched field of the arithmetic type to a dense FP64 array (k = iy*nx + ix).
+template <class A>
+__global__ void __launch_bounds__(256) k_field_to_dense(const A* __restrict__ src, double* __restrict__ dst, Geom G) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= G.nx || iy >= G.ny) return;
+    dst[iy * G.nx + ix] = double(src[(long long)iy * G.pitch + ix]);
 }
 
 // Nusselt accumulation of the streamed state of a PC buffer (one thread per row).

@@ -332,23 +332,16 @@ struct Impl final : Solver {
         CK(cudaStreamSynchronize(stream));
     }
 
+    // init_from_fields (src/uniform/solver.rs:232-262) from host arrays: the
+    // fields go to the device and the equilibria are set there (k_init_eq,
+    // the host's FP64 arithmetic bit for bit).
     void init_from_fields(const double* r, const double* u, const double* v, const double* t) override {
-        const int nx = p.nx, ny = p.ny;
-        const size_t n = size_t(nx) * ny;
-        std::vector<double> f(n * Q), g(n * Q), rr(r, r + n), uu(u, u + n), vv(v, v + n), tt0(t, t + n);
-        for (size_t k = 0; k < n; ++k)
-            for (int i = 0; i < Q; ++i) {
-                f[k * Q + i] = feq_full<double>(i, r[k], u[k], v[k]);
-                g[k * Q + i] = geq_full<double>(i, t[k], u[k], v[k], p.geq_order);
-            }
-        for (int iy = 0; iy < ny; ++iy)
-            for (int ix = 0; ix < nx; ++ix)
-                if (ix == 0 || ix == nx - 1 || iy == 0 || iy == ny - 1) {
-                    uu[size_t(iy) * nx + ix] = 0.0;
-                    vv[size_t(iy) * nx + ix] = 0.0;
-                }
-        upload_ref(f, g, rr, uu, vv, tt0);
-        time_step = 0;
+        ensure_aos();
+        const size_t n = size_t(p.nx) * p.ny;
+        const double* src[4] = {r, u, v, t};
+        for (int j = 0; j < 4; ++j)
+            CK(cudaMemcpyAsync(aos + j * n, src[j], sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+        init_from_device_fields(aos, aos + n, aos + 2 * n, aos + 3 * n);
     }
 
     // ---- form transitions ------------------------------------------------------
@@ -549,14 +542,21 @@ struct Impl final : Solver {
     }
 
     // ---- observables --------------------------------------------------------------
+    // The fields, converted to dense FP64 on the device and copied straight
+    // into the caller's arrays (one synchronisation).
     void get_fields(double* r, double* u, double* v, double* t, double* nu_t, double* fyo) override {
         ensure_ref();
-        if (r) download_field(rho, r);
-        if (u) download_field(ux, u);
-        if (v) download_field(uy, v);
-        if (t) download_field(tt, t);
-        if (nu_t) download_field(nut, nu_t);
-        if (fyo) download_field(fy, fyo);
+        ensure_aos();
+        const size_t n = size_t(p.nx) * p.ny;
+        const A* src[6] = {rho, ux, uy, tt, nut, fy};
+        double* dst[6] = {r, u, v, t, nu_t, fyo};
+        for (int j = 0; j < 6; ++j) {
+            if (!dst[j]) continue;
+            k_field_to_dense<A><<<grd, blk, 0, stream>>>(src[j], aos + j * n, G);
+            check_launch();
+            CK(cudaMemcpyAsync(dst[j], aos + j * n, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+        }
+        CK(cudaStreamSynchronize(stream));
     }
 
     void set_fields(const double* r, const double* u, const double* v, const double* t, const double* fyi) override {
