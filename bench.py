@@ -274,6 +274,36 @@ def octree_c5(dev, chain=(30_000, 30_000, 60_000), window=40_000, sample_every=1
     return out
 
 
+def batch_only(precision, steps, tiles):
+    """C3 batch timing alone (profiling runs): the 64-cavity sweep in one
+    storage format with a fixed tuning (tile height 16, 4 CTAs per SM for
+    the global-memory kernel; the tile kernel's resident CTAs otherwise),
+    250 spin-up steps, then `steps` timed lattice steps."""
+    import torch
+
+    from cfd_cavity_b200 import CavityBatch, sweep_configs
+
+    cfg = sweep_configs(64)
+    nodes = sum(c["nx"] * c["ny"] for c in cfg)
+    bt = CavityBatch(cfg, precision=precision, device=0)
+    bt.set_tuning(16, 4 if tiles == 0 else 3, tiles=tiles)
+    bt.step(250)
+    st = torch.cuda.ExternalStream(bt.stream_handle(), device=0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(st):
+        e0.record(st)
+    bt.step(steps)
+    with torch.cuda.stream(st):
+        e1.record(st)
+    e1.synchronize()
+    bt.sync()
+    ms = e0.elapsed_time(e1)
+    print(json.dumps({"workload": f"batched sweep 64 cavities {precision}", "tiles": tiles, "steps": steps,
+                      "us_per_step": ms * 1e3 / steps, "mlups": nodes * steps / (ms * 1e-3) / 1e6}), flush=True)
+    bt.close()
+    return 0
+
+
 def octree_only(coarse_steps):
     """C5 octree timing alone: a few warm-up coarse steps, then
     `coarse_steps` timed with CUDA events on the octree's stream."""
@@ -347,10 +377,16 @@ def main():
     ap.add_argument("--octree-only", type=int, default=0, metavar="COARSE_STEPS",
                     help="only time COARSE_STEPS octree coarse steps of the 256x1024 levels-3 cavity "
                          "(FP32 / binary16) and print their device time (profiling runs)")
+    ap.add_argument("--batch-only", default="", metavar="PRECISION",
+                    help="only time the 64-cavity batched sweep in PRECISION for --steps lattice steps "
+                         "(profiling runs); --batch-tiles selects the kernel")
+    ap.add_argument("--batch-tiles", type=int, default=0, choices=[0, 1, 2])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.octree_only:
         return octree_only(args.octree_only)
+    if args.batch_only:
+        return batch_only(args.batch_only, args.steps, args.batch_tiles)
     world, rank, local, dist = dist_setup(args)
     if args.impl == "reference":
         rc = run_reference(args, world, rank, dist)

@@ -41,7 +41,7 @@
 namespace cav {
 
 constexpr int GRAPH_STEPS = 64;  // even: a replay leaves the buffer parity unchanged
-constexpr int BX = 32, BY = 4;
+constexpr int BX = 32, BY = 2;
 constexpr int DIAG_BLOCKS_MAX = 592;  // 4 x 148 SMs
 
 // xorshift64* (src/uniform/rng.rs:5-31) for the initial temperature noise.
