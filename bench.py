@@ -333,6 +333,23 @@ def octree_only(coarse_steps):
     return 0
 
 
+def max_over_ranks(dist, x, device):
+    """x reduced with MAX over every rank of the process group (x itself
+    without one): the job time is the slowest rank's."""
+    if not dist:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_mlups(nodes, lattice_steps, world, seconds):
+    """Whole-job throughput: each of `world` replicas advanced `nodes` x
+    `lattice_steps` node updates, the slowest within `seconds`."""
+    return nodes * lattice_steps * world / seconds / 1e6
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -440,13 +457,8 @@ def main():
     launches = s.launch_count() - launches0
     ms = [a.elapsed_time(b) for a, b in ev]
     t_total = sum(ms) / 1e3
-    t_max = t_total
-    if dist:
-        tt = torch.tensor([t_total], device=f"cuda:{dev}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-    updates = nodes * args.chunk * args.steps * world
-    value = updates / t_max / 1e6
+    t_max = max_over_ranks(dist, t_total, f"cuda:{dev}")
+    value = whole_job_mlups(nodes, args.chunk * args.steps, world, t_max)
     kernel_us = t_total / (args.chunk * args.steps) * 1e6  # per fused launch
     bpn = BYTES_PER_NODE[prec]
     achieved = bpn * nodes / (kernel_us * 1e-6) / 1e9
@@ -475,15 +487,11 @@ def main():
     for _ in range(e2e_steps):
         e2e_once()
     barrier()
-    te = time.perf_counter() - t0
-    if dist:
-        tt = torch.tensor([te], device=f"cuda:{dev}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        te = float(tt.item())
-    e2e_value = nodes * args.chunk * e2e_steps * world / te / 1e6
+    te = max_over_ranks(dist, time.perf_counter() - t0, f"cuda:{dev}")
+    e2e_value = whole_job_mlups(nodes, args.chunk * e2e_steps, world, te)
 
     extras = {}
-    if not args.no_extras:
+    if not args.no_extras and world == 1:  # single-GPU workloads: reported at N = 1
         # FP32 storage on the same single cavity, same timing method
         s32 = CavitySolver(NX, NY, RA, PHYS["pr"], PHYS["cs"], PHYS["pr_t"], PHYS["utarget"],
                            PHYS["seed"], precision="f32", init_mode=L.CAV_INIT_ZERO, noise_amp=1e-4,
