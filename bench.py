@@ -163,6 +163,34 @@ def batched_sweep(precisions, dev, steps=300):
     return out
 
 
+def c2_nusselt_error(dev, precisions=("f32", "f16sr", "f16gsr", "bf16sr")):
+    """The accuracy half of the headline: configs[1] (128x512, Ra = 1e8,
+    theta = 0 + 1e-4 noise) for 200 000 steps, the per-step hot / cold wall
+    Nu (post.rs:68-111) averaged over steps 150 001-200 000 on the device,
+    against the same average of the FP64 oracle (the committed fixture
+    tests/golden/c2_128x512_ra1e8.json, made by the oracle)."""
+    from cfd_cavity_b200 import CavitySolver
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "tests", "golden", "c2_128x512_ra1e8.json")) as f:
+        gd = json.load(f)
+    c = gd["config"]
+    out = {"reference": "FP64 oracle", "nu_hot_step_mean_fp64": gd["nu_hot_step_mean"],
+           "window_steps": c["window"]}
+    for p in precisions:
+        g = CavitySolver(c["nx"], c["ny"], c["ra"], c["pr"], c["cs"], c["pr_t"], c["utarget"], c["seed"],
+                         precision=p, init_mode=1, noise_amp=c["noise_amp"], device=dev)
+        g.step(c["steps"] - c["window"])
+        g.nu_accumulate(True)
+        g.step(c["window"])
+        hot, cold, n = g.nu_accumulated()
+        g.close()
+        out[p] = {"nu_hot": hot, "nu_cold": cold,
+                  "rel_err_hot": abs(hot - gd["nu_hot_step_mean"]) / gd["nu_hot_step_mean"],
+                  "rel_err_cold": abs(cold - gd["nu_cold_step_mean"]) / gd["nu_cold_step_mean"]}
+    return out
+
+
 def adjoint_c4(dev):
     """96x384, Ra=1e7, FP32; J = mean hot-wall Nu over steps
     40 001-60 000 of 60 000, gradient w.r.t. the 384-value hot-wall profile
@@ -507,6 +535,7 @@ def main():
         e1.synchronize()
         extras["fp32_single_cavity_mlups"] = nodes * args.chunk * 3 / (e0.elapsed_time(e1) * 1e-3) / 1e6
         s32.close()
+        extras["c2_nusselt"] = c2_nusselt_error(dev)
         extras["batched_sweep"] = batched_sweep(["f32", "f16sr", "f16gsr", "bf16sr", "f16"], dev)
         extras["adjoint_c4"] = adjoint_c4(dev)
         extras["octree_c5"] = octree_c5(dev)

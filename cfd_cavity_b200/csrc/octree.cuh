@@ -1186,7 +1186,8 @@ struct OctImpl final : Octree {
     // dynamic mixed-scale SGS model (set_dynamic_sgs, src/octree/solver.rs:476-481)
     bool dyn = false;
     double dyn_alpha = 0.5, dyn_min = -0.1, dyn_eta = 2.0;
-    double* sgs_w = nullptr;              // S_NPLANES work planes of the largest level
+    double* sgs_w = nullptr;              // 2 x S_NPLANES work planes of the largest level
+    size_t sgs_stride = 0;                // elements of one block's work planes
     A* nut0 = nullptr;                    // nu_t_pre, then alpha_t_pre, of L0
     A* nut1[2] = {nullptr, nullptr};      // of the L1 blocks
     A* nut2[2] = {nullptr, nullptr};      // of the L2 strips
@@ -1669,7 +1670,8 @@ struct OctImpl final : Octree {
         CK(cudaStreamSynchronize(stream));
         if (on && !sgs_w) {
             const int nmax = std::max(std::max(L0.n, L1[0].n), levels == 3 ? L2[0].n : 0);
-            sgs_w = dalloc<double>(size_t(S_NPLANES) * nmax);
+            sgs_stride = size_t(S_NPLANES) * nmax;
+            sgs_w = dalloc<double>(2 * sgs_stride);
             nut0 = dalloc<A>(2 * size_t(L0.n));
             for (int b = 0; b < 2; ++b) {
                 nut1[b] = dalloc<A>(2 * size_t(L1[b].n));
@@ -1708,8 +1710,11 @@ struct OctImpl final : Octree {
         dyn_eta = eta_test;
     }
 
+    // The model on nb (1 or 2) blocks of one level shape in one launch per
+    // kernel (blockIdx.z = block).
     template <class St>
-    void sgs_level(const Lvl<St>& L, A* nut, double tau_mol, double nu_l, double al_l) {
+    void sgs_levels(const Lvl<St>* Ls, int nb, A* const* nuts, double tau_mol, double nu_l, double al_l) {
+        const Lvl<St>& L = Ls[0];
         const Geom G{L.nx, L.ny, L.nx, (long long)L.n};
         SgsParams sp;
         const double eta = std::max(dyn_eta, 1.0);
@@ -1721,16 +1726,18 @@ struct OctImpl final : Octree {
         sp.alpha_mol = al_l;
         sp.nu_sm_min = dyn_min;
         sp.rho_off = SH ? 1.0 : 0.0;
-        const dim3 blk(32, 4), grd((L.nx + 31) / 32, (L.ny + 3) / 4);
-        const A* mac = L.mac;
-        k_sgs_a<A><<<grd, blk, 0, stream>>>(mac + L.n, mac + 2 * L.n, mac + 3 * L.n, sgs_w, G, sp);
+        SgsGrids<St> S{};
+        for (int b = 0; b < nb; ++b) {
+            const A* mac = Ls[b].mac;
+            S.g[b] = SgsGrid<St>{Ls[b].ref[Ls[b].cur], mac,       mac + L.n, mac + 2 * L.n, mac + 3 * L.n,
+                                 sgs_w + b * sgs_stride, nuts[b], nuts[b] + L.n};
+        }
+        const dim3 blk(32, 4), grd((L.nx + 31) / 32, (L.ny + 3) / 4, nb);
+        k_sgs_b<St><<<grd, blk, 0, stream>>>(S, G, sp);
         check_launch();
-        k_sgs_b<St><<<grd, blk, 0, stream>>>(L.ref[L.cur], mac, mac + L.n, mac + 2 * L.n, mac + 3 * L.n, sgs_w, G,
-                                             sp);
+        k_sgs_c<St><<<grd, blk, 0, stream>>>(S, G, sp);
         check_launch();
-        k_sgs_c<<<grd, blk, 0, stream>>>(sgs_w, G, sp);
-        check_launch();
-        k_sgs_d<A><<<grd, blk, 0, stream>>>(sgs_w, nut, nut + L.n, G, sp);
+        k_sgs_d<St><<<grd, blk, 0, stream>>>(S, G, sp);
         check_launch();
     }
 
@@ -1759,7 +1766,7 @@ struct OctImpl final : Octree {
         double nu_eff, al_eff;
         ramp_of(time_step, nu_eff, al_eff);
         // L0 model, its coefficient statistics, xi A (L1 nu_t of the previous step)
-        sgs_level(L0, nut0, 0.5 + 3.0 * nu_eff, nu_eff, al_eff);
+        sgs_levels(&L0, 1, &nut0, 0.5 + 3.0 * nu_eff, nu_eff, al_eff);
         k_oct_sgs_parts<<<DYN_PARTS, 256, 0, stream>>>(sgs_w, L0.n, spart);
         check_launch();
         {
@@ -1785,7 +1792,7 @@ struct OctImpl final : Octree {
         step_L0();
         c2f_L1();
         const double tau_mol_l1 = 0.5 + 3.0 * 2.0 * nu_eff, tau_mol_l2 = 0.5 + 3.0 * 4.0 * nu_eff;
-        for (int b = 0; b < 2; ++b) sgs_level(L1[b], nut1[b], tau_mol_l1, 2.0 * nu_eff, 2.0 * al_eff);
+        sgs_levels(L1, 2, nut1, tau_mol_l1, 2.0 * nu_eff, 2.0 * al_eff);
         launch(k_oct_collide<StF, false>, grid_of(L1[0].n, 2), pair_cur(L1[0], L1[1]), (const OctScal<A>*)tab, S,
                (const long long*)step_dev, 1, seed32, 3, d1);
         step_L1(0, 3);
@@ -1808,7 +1815,7 @@ struct OctImpl final : Octree {
             c2f_L2();
             const DynPtr<A> d2{{nut2[0], nut2[1]}, {nut2[0] + L2[0].n, nut2[1] + L2[1].n}};
             for (int sp = 0; sp < 2; ++sp) {
-                for (int b = 0; b < 2; ++b) sgs_level(L2[b], nut2[b], tau_mol_l2, 4.0 * nu_eff, 4.0 * al_eff);
+                sgs_levels(L2, 2, nut2, tau_mol_l2, 4.0 * nu_eff, 4.0 * al_eff);
                 launch(k_oct_collide<StF, false>, grid_of(L2[0].n, 2), pair_cur(L2[0], L2[1]),
                        (const OctScal<A>*)tab, S, (const long long*)step_dev, 2, seed32, 5 + sp, d2);
                 step_L2(0, 5 + sp);
@@ -1816,7 +1823,7 @@ struct OctImpl final : Octree {
             f2c_L2(0);
         }
         // the second L1 model takes the unramped nu / alpha (src/octree/solver.rs:882-890)
-        for (int b = 0; b < 2; ++b) sgs_level(L1[b], nut1[b], tau_mol_l1, 2.0 * nu, 2.0 * alpha);
+        sgs_levels(L1, 2, nut1, tau_mol_l1, 2.0 * nu, 2.0 * alpha);
         launch(k_oct_collide<StF, false>, grid_of(L1[0].n, 2), pair_cur(L1[0], L1[1]), (const OctScal<A>*)tab, S,
                (const long long*)step_dev, 1, seed32, 9, d1);
         step_L1(0, 9);

@@ -6,13 +6,16 @@
 // (compute_dynamic_sgs_level, src/octree/smag.rs:144-416: the same
 // algorithm with the level's tau, nu and alpha in its own lattice units).
 //
-// Four kernels, each one thread per node, every quantity in FP64 whatever
-// the storage format (the reference's arithmetic):
-//   k_sgs_a  test-filter box of u_x, u_y, T and of the five products
-//            (Leonard terms at the test level);
-//   k_sgs_b  grid-level S~ and |S~| from pi_neq (the collision's formula),
-//            test-level S-bar and temperature gradients by central
-//            differences, similarity scales qsm^1/2 and Phi_sm^1/2, |T~|, |T-bar|;
+// Three kernels, each one thread per node, every quantity in FP64 whatever
+// the storage format (the reference's arithmetic); a launch covers
+// gridDim.z grids of one shape (the two blocks of an octree level):
+//   k_sgs_b  test-filter boxes of u_x, u_y, T (at the node and at the four
+//            neighbours its central differences read, each box summed in
+//            the reference's window order) and of the five products
+//            (Leonard terms at the test level); grid-level S~ and |S~| from
+//            pi_neq (the collision's formula), test-level S-bar and
+//            temperature gradients by central differences, similarity scales
+//            qsm^1/2 and Phi_sm^1/2, |T~|, |T-bar|;
 //   k_sgs_c  box of qsm^1/2 and Phi_sm^1/2, the interpolated mixed forms
 //            (a^alpha b^(1-alpha)), Germano tensors M and L, Lilly numerators
 //            and denominators;
@@ -39,6 +42,23 @@ enum SgsPlane {
     S_NUMV, S_DENV, S_NUMK, S_DENK, S_NUMIX, S_KAPMIX,               // k_sgs_c
     S_CNU, S_CK,                                                     // k_sgs_d
     S_NPLANES
+};
+
+// One grid's inputs and outputs; a launch takes two (blockIdx.z).
+template <class St>
+struct SgsGrid {
+    const St* pops;                    // REF populations
+    const typename Fmt<St>::A* rho;    // fields (rho stored minus sp.rho_off)
+    const typename Fmt<St>::A* ux;
+    const typename Fmt<St>::A* uy;
+    const typename Fmt<St>::A* tt;
+    double* W;                          // S_NPLANES work planes
+    typename Fmt<St>::A* nut;           // nu_t_pre out
+    typename Fmt<St>::A* at;            // alpha_t_pre out
+};
+template <class St>
+struct SgsGrids {
+    SgsGrid<St> g[2];
 };
 
 struct SgsParams {
@@ -70,14 +90,6 @@ __device__ __forceinline__ Window box_window(const Geom& G, int ix, int iy, int 
 }
 
 // ddx / ddy (src/uniform/solver.rs:1229-1245): central, clamped at the walls.
-__device__ __forceinline__ double ddx_p(const double* __restrict__ p, const Geom& G, int ix, int iy) {
-    const int xm = ix == 0 ? 0 : ix - 1, xp = ix + 1 >= G.nx ? G.nx - 1 : ix + 1;
-    return 0.5 * (p[iy * G.pitch + xp] - p[iy * G.pitch + xm]);
-}
-__device__ __forceinline__ double ddy_p(const double* __restrict__ p, const Geom& G, int ix, int iy) {
-    const int ym = iy == 0 ? 0 : iy - 1, yp = iy + 1 >= G.ny ? G.ny - 1 : iy + 1;
-    return 0.5 * (p[yp * G.pitch + ix] - p[ym * G.pitch + ix]);
-}
 template <class A>
 __device__ __forceinline__ double ddx_f(const A* __restrict__ p, const Geom& G, int ix, int iy) {
     const int xm = ix == 0 ? 0 : ix - 1, xp = ix + 1 >= G.nx ? G.nx - 1 : ix + 1;
@@ -97,54 +109,73 @@ __host__ __device__ __forceinline__ double lilly_coefficient(double num, double 
     return c < 0.0 ? 0.0 : (c > C_DYN_MAX ? C_DYN_MAX : c);
 }
 
+// Test-filter box of u_x, u_y, T at (x, y): box_filter's window and order.
 template <class A>
-__global__ void __launch_bounds__(128) k_sgs_a(const A* __restrict__ ux, const A* __restrict__ uy,
-                                               const A* __restrict__ tt, double* __restrict__ W, Geom G,
-                                               SgsParams sp) {
-    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
-    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
-    if (ix >= G.nx || iy >= G.ny) return;
-    const Window w = box_window(G, ix, iy, sp.width);
-    double s[8];
-#pragma unroll
-    for (int p = 0; p < 8; ++p) s[p] = 0.0;
+__device__ __forceinline__ void box3(const A* __restrict__ ux, const A* __restrict__ uy, const A* __restrict__ tt,
+                                     const Geom& G, int x, int y, int width, double& bu, double& bv, double& bt) {
+    const Window w = box_window(G, x, y, width);
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
     for (int yy = w.y0; yy < w.y1; ++yy)
         for (int xx = w.x0; xx < w.x1; ++xx) {
             const int k = yy * G.pitch + xx;
-            const double u = ux[k], v = uy[k], t = tt[k];
-            s[0] += u;
-            s[1] += v;
-            s[2] += t;
-            s[3] += u * u;
-            s[4] += u * v;
-            s[5] += v * v;
-            s[6] += u * t;
-            s[7] += v * t;
+            s0 += double(ux[k]);
+            s1 += double(uy[k]);
+            s2 += double(tt[k]);
         }
-    const long long P = G.plane;
-    const int k = iy * G.pitch + ix;
-#pragma unroll
-    for (int p = 0; p < 8; ++p) W[(S_UBX + p) * P + k] = s[p] / w.cnt;
+    bu = s0 / w.cnt;
+    bv = s1 / w.cnt;
+    bt = s2 / w.cnt;
 }
 
 template <class St>
-__global__ void __launch_bounds__(128) k_sgs_b(const St* __restrict__ pops, const typename Fmt<St>::A* __restrict__ rho,
-                                               const typename Fmt<St>::A* __restrict__ ux,
-                                               const typename Fmt<St>::A* __restrict__ uy,
-                                               const typename Fmt<St>::A* __restrict__ tt, double* __restrict__ W,
-                                               Geom G, SgsParams sp) {
+__global__ void __launch_bounds__(128) k_sgs_b(SgsGrids<St> S, Geom G, SgsParams sp) {
+    using A = typename Fmt<St>::A;
     constexpr bool SH = Fmt<St>::SHIFT;
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iy = blockIdx.y * blockDim.y + threadIdx.y;
     if (ix >= G.nx || iy >= G.ny) return;
+    const SgsGrid<St> io = S.g[blockIdx.z];
+    double* __restrict__ W = io.W;
+    const A* ux = io.ux;
+    const A* uy = io.uy;
+    const A* tt = io.tt;
     const long long P = G.plane;
     const int k = iy * G.pitch + ix;
-    const double rho_k = double(rho[k]) + sp.rho_off, ux_k = ux[k], uy_k = uy[k], t_k = tt[k];
+    // test-filter boxes at the node and at the neighbours of its central
+    // differences (ddx / ddy clamp at the walls), and the Leonard boxes
+    const int xm = ix == 0 ? 0 : ix - 1, xp = ix + 1 >= G.nx ? G.nx - 1 : ix + 1;
+    const int ym = iy == 0 ? 0 : iy - 1, yp = iy + 1 >= G.ny ? G.ny - 1 : iy + 1;
+    double ubx, uby, tb, ubx_xm, uby_xm, tb_xm, ubx_xp, uby_xp, tb_xp, ubx_ym, uby_ym, tb_ym, ubx_yp, uby_yp, tb_yp;
+    box3<A>(ux, uy, tt, G, ix, iy, sp.width, ubx, uby, tb);
+    box3<A>(ux, uy, tt, G, xm, iy, sp.width, ubx_xm, uby_xm, tb_xm);
+    box3<A>(ux, uy, tt, G, xp, iy, sp.width, ubx_xp, uby_xp, tb_xp);
+    box3<A>(ux, uy, tt, G, ix, ym, sp.width, ubx_ym, uby_ym, tb_ym);
+    box3<A>(ux, uy, tt, G, ix, yp, sp.width, ubx_yp, uby_yp, tb_yp);
+    {
+        const Window w = box_window(G, ix, iy, sp.width);
+        double l[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int yy = w.y0; yy < w.y1; ++yy)
+            for (int xx = w.x0; xx < w.x1; ++xx) {
+                const int kk = yy * G.pitch + xx;
+                const double u = ux[kk], v = uy[kk], t = tt[kk];
+                l[0] += u * u;
+                l[1] += u * v;
+                l[2] += v * v;
+                l[3] += u * t;
+                l[4] += v * t;
+            }
+        W[S_UBX * P + k] = ubx;
+        W[S_UBY * P + k] = uby;
+        W[S_TB * P + k] = tb;
+#pragma unroll
+        for (int p = 0; p < 5; ++p) W[(S_LXX + p) * P + k] = l[p] / w.cnt;
+    }
+    const double rho_k = double(io.rho[k]) + sp.rho_off, ux_k = ux[k], uy_k = uy[k], t_k = tt[k];
     double pi_xx = 0.0, pi_xy = 0.0, pi_yy = 0.0;
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
         const double cx = CX(i), cy = CY(i);
-        const double fi = double(ldp(pops, G, i, iy, ix)) + (SH ? WD(i) : 0.0);
+        const double fi = double(ldp(io.pops, G, i, iy, ix)) + (SH ? WD(i) : 0.0);
         const double fneq = fi - feq_full<double>(i, rho_k, ux_k, uy_k);
         pi_xx += fneq * cx * cx;
         pi_xy += fneq * cx * cy;
@@ -158,26 +189,24 @@ __global__ void __launch_bounds__(128) k_sgs_b(const St* __restrict__ pops, cons
     W[S_SHXY * P + k] = shxy;
     W[S_SHYY * P + k] = shyy;
     W[S_SMH * P + k] = sqrt(pi2) / denom;
-    const double* ubx = W + S_UBX * P;
-    const double* uby = W + S_UBY * P;
-    const double* tb = W + S_TB * P;
-    const double sxx = ddx_p(ubx, G, ix, iy);
-    const double syy = ddy_p(uby, G, ix, iy);
-    const double sxy = 0.5 * (ddx_p(uby, G, ix, iy) + ddy_p(ubx, G, ix, iy));
+    // ddx / ddy of the boxed fields (src/uniform/solver.rs:1229-1245)
+    const double sxx = 0.5 * (ubx_xp - ubx_xm);
+    const double syy = 0.5 * (uby_yp - uby_ym);
+    const double sxy = 0.5 * (0.5 * (uby_xp - uby_xm) + 0.5 * (ubx_yp - ubx_ym));
     W[S_SBXX * P + k] = sxx;
     W[S_SBXY * P + k] = sxy;
     W[S_SBYY * P + k] = syy;
     W[S_SMB * P + k] = sqrt(sxx * sxx + 2.0 * sxy * sxy + syy * syy);
     const double gtx = ddx_f(tt, G, ix, iy), gty = ddy_f(tt, G, ix, iy);
-    const double gbx = ddx_p(tb, G, ix, iy), gby = ddy_p(tb, G, ix, iy);
+    const double gbx = 0.5 * (tb_xp - tb_xm), gby = 0.5 * (tb_yp - tb_ym);
     W[S_GTX * P + k] = gtx;
     W[S_GTY * P + k] = gty;
     W[S_GBX * P + k] = gbx;
     W[S_GBY * P + k] = gby;
-    const double dux = ux_k - ubx[k], duy = uy_k - uby[k];
+    const double dux = ux_k - ubx, duy = uy_k - uby;
     const double du2 = dux * dux + duy * duy;
     W[S_QSM * P + k] = sqrt(0.5 * du2) / 2.0;
-    const double dt_local = t_k - tb[k];
+    const double dt_local = t_k - tb;
     W[S_PHI * P + k] = 0.5 * fabs(dt_local) * sqrt(0.5 * du2);
     const double th_x = gtx * shxx + gty * shxy;
     const double th_y = gtx * shxy + gty * shyy;
@@ -187,10 +216,12 @@ __global__ void __launch_bounds__(128) k_sgs_b(const St* __restrict__ pops, cons
     W[S_TMB * P + k] = sqrt(2.0 * (tb_x * tb_x + tb_y * tb_y));
 }
 
-static __global__ void __launch_bounds__(128) k_sgs_c(double* __restrict__ W, Geom G, SgsParams sp) {
+template <class St>
+__global__ void __launch_bounds__(128) k_sgs_c(SgsGrids<St> S, Geom G, SgsParams sp) {
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iy = blockIdx.y * blockDim.y + threadIdx.y;
     if (ix >= G.nx || iy >= G.ny) return;
+    double* __restrict__ W = S.g[blockIdx.z].W;
     const long long P = G.plane;
     const int k = iy * G.pitch + ix;
     const Window w = box_window(G, ix, iy, sp.width);
@@ -230,12 +261,15 @@ static __global__ void __launch_bounds__(128) k_sgs_c(double* __restrict__ W, Ge
     W[S_KAPMIX * P + k] = kap_mix_g;
 }
 
-template <class A>
-__global__ void __launch_bounds__(128) k_sgs_d(double* __restrict__ W, A* __restrict__ nut_pre, A* __restrict__ at_pre,
-                                               Geom G, SgsParams sp) {
+template <class St>
+__global__ void __launch_bounds__(128) k_sgs_d(SgsGrids<St> S, Geom G, SgsParams sp) {
+    using A = typename Fmt<St>::A;
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iy = blockIdx.y * blockDim.y + threadIdx.y;
     if (ix >= G.nx || iy >= G.ny) return;
+    double* __restrict__ W = S.g[blockIdx.z].W;
+    A* __restrict__ nut_pre = S.g[blockIdx.z].nut;
+    A* __restrict__ at_pre = S.g[blockIdx.z].at;
     const long long P = G.plane;
     const int k = iy * G.pitch + ix;
     const Window w = box_window(G, ix, iy, sp.width);

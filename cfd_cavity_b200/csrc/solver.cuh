@@ -471,13 +471,13 @@ struct Impl final : Solver {
         sp.nu_mol = U.nu;
         sp.alpha_mol = U.alpha;
         sp.nu_sm_min = dyn_min;
-        k_sgs_a<A><<<grd, blk, 0, stream>>>(ux, uy, tt, sgs_w, G, sp);
+        SgsGrids<St> S{};
+        S.g[0] = SgsGrid<St>{pop[cur], rho, ux, uy, tt, sgs_w, nut_pre, at_pre};
+        k_sgs_b<St><<<grd, blk, 0, stream>>>(S, G, sp);
         check_launch();
-        k_sgs_b<St><<<grd, blk, 0, stream>>>(pop[cur], rho, ux, uy, tt, sgs_w, G, sp);
+        k_sgs_c<St><<<grd, blk, 0, stream>>>(S, G, sp);
         check_launch();
-        k_sgs_c<<<grd, blk, 0, stream>>>(sgs_w, G, sp);
-        check_launch();
-        k_sgs_d<A><<<grd, blk, 0, stream>>>(sgs_w, nut_pre, at_pre, G, sp);
+        k_sgs_d<St><<<grd, blk, 0, stream>>>(S, G, sp);
         check_launch();
         sgs_valid = true;
         k_collide_ref<St><<<grd, blk, 0, stream>>>(pop[cur], pop[cur ^ 1], rho, ux, uy, tt, fy, nut, G,
