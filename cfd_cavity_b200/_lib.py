@@ -183,6 +183,7 @@ def load(path: str | None = None):
         "cav_batch_set_tuning": (i32, [vp, ctypes.POINTER(CavBatchTuning)]),
         "cav_batch_autotune": (i32, [vp, i32, ctypes.POINTER(CavBatchTuning)]),
         "cav_batch_sync": (i32, [vp]),
+        "cav_batch_debug_stall_copies": (i32, [vp, i32]),
         "cav_batch_get_stream": (i32, [vp, ctypes.POINTER(vp)]),
         "cav_batch_launch_count": (i32, [vp, ctypes.POINTER(i64)]),
         "cav_octree_default_params": (i32, [ctypes.POINTER(CavOctreeParams)]),

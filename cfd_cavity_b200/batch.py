@@ -141,6 +141,11 @@ class CavityBatch:
         self._ck(L.load().cav_batch_autotune(self._b, int(trial_steps), ctypes.byref(t)))
         return {"rows_per_item": t.rows_per_item, "ctas_per_sm": t.ctas_per_sm, "tiles": t.tiles}
 
+    def debug_stall_copies(self, on):
+        """Test of the tile kernel's bounded waits: arm the barriers but issue
+        no copy (the next sync raises CAV_ERR_TIMEOUT)."""
+        self._ck(L.load().cav_batch_debug_stall_copies(self._b, int(bool(on))))
+
     def sync(self):
         self._ck(L.load().cav_batch_sync(self._b))
 

@@ -77,6 +77,7 @@ struct BatchBase {
     virtual void set_tuning(const BatchTuning& t) = 0;
     virtual double time_steps(int steps) = 0;  // ms for `steps` batched steps (advances the state)
     virtual void sync() = 0;
+    virtual void set_stall_copies(bool on) = 0;
     std::vector<Solver*> cavs;  // owned
     BatchTuning tun;
     cudaStream_t stream = nullptr;
@@ -105,6 +106,7 @@ struct Batch final : BatchBase {
     unsigned* d_err = nullptr;
     unsigned* h_err = nullptr;  // pinned copy of *d_err
     int n_titems[3] = {0, 0, 0}, tgrid = 0;
+    bool stall_copies = false;  // test of the bounded waits: arm the barriers, issue no copy
 
     ~Batch() override {
         if (graph) cudaGraphExecDestroy(graph);
@@ -272,7 +274,8 @@ struct Batch final : BatchBase {
         cfg.numAttrs = 1;
         CK(cudaLaunchKernelEx(&cfg, k_tile<St, V, WN, false>, (const TileCav<St>*)d_tcavs,
                               (const CUtensorMap*)d_maps[V], (const TileItem*)d_titems[V], n_titems[V],
-                              (const StepScalars<A>*)d_table, int(cv.size()), step, sdev, d_err));
+                              (const StepScalars<A>*)d_table, int(cv.size()), step, sdev, d_err,
+                              int(stall_copies)));
     }
 
     void launch(bool write_nut, const long long* sdev, long long step) {
@@ -364,11 +367,26 @@ struct Batch final : BatchBase {
         return ms;
     }
 
-    // A tile CTA that gave up waiting for its copies (k_tile) sets *d_err.
+    // A tile CTA that gave up waiting for its copies (k_tile) sets *d_err;
+    // reported once, then cleared (the steps of that launch are lost).
     void check_err() {
         CK(cudaMemcpyAsync(h_err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
         CK(cudaStreamSynchronize(stream));
-        if (*h_err) throw ArgError{CAV_ERR_TIMEOUT, "a tile copy did not complete within its bounded wait"};
+        if (*h_err) {
+            *h_err = 0;
+            CK(cudaMemsetAsync(d_err, 0, sizeof(unsigned), stream));
+            CK(cudaStreamSynchronize(stream));
+            throw ArgError{CAV_ERR_TIMEOUT, "a tile copy did not complete within its bounded wait"};
+        }
+    }
+
+    void set_stall_copies(bool on) override {
+        CK(cudaStreamSynchronize(stream));
+        stall_copies = on;
+        if (graph) {
+            CK(cudaGraphExecDestroy(graph));
+            graph = nullptr;
+        }
     }
 
     void sync() override { check_err(); }

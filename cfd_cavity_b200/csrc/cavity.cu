@@ -658,6 +658,10 @@ int cav_batch_autotune(cav_batch* b, int32_t trial_steps, cav_batch_tuning* chos
     });
 }
 
+int cav_batch_debug_stall_copies(cav_batch* b, int32_t on) {
+    return bguarded(b, [&](BatchBase& x) { x.set_stall_copies(on != 0); });
+}
+
 int cav_batch_sync(cav_batch* b) {
     return bguarded(b, [&](BatchBase& x) { x.sync(); });
 }

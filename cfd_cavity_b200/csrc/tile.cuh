@@ -14,7 +14,9 @@
 //
 // Every wait on an mbarrier is bounded (about one second of %globaltimer);
 // a CTA that gives up sets *err, finishes its loop without blocking and
-// waits (bounded again) for the copies it issued before returning.
+// waits (bounded again) for the copies it issued before returning.  With
+// `no_copy` (a test of that path) the barriers are armed but no copy is
+// issued, so every wait runs out and nothing is left in flight.
 #pragma once
 
 #include <cuda.h>
@@ -173,7 +175,8 @@ template <class St, int V, bool WRITE_NUT, bool ACC_NU>
 __global__ void __launch_bounds__(TileShape<St, V>::THREADS)
     k_tile(const TileCav<St>* __restrict__ cavs, const CUtensorMap* __restrict__ maps,
            const TileItem* __restrict__ items, int n_items, const StepScalars<typename Fmt<St>::A>* __restrict__ table,
-           int n_cav, long long step, const long long* __restrict__ step_dev, unsigned* __restrict__ err) {
+           int n_cav, long long step, const long long* __restrict__ step_dev, unsigned* __restrict__ err,
+           int no_copy) {
     using A = typename Fmt<St>::A;
     using TS = TileShape<St, V>;
     extern __shared__ __align__(128) unsigned char tile_smem[];
@@ -197,7 +200,8 @@ __global__ void __launch_bounds__(TileShape<St, V>::THREADS)
         const int b = (cavs[I.cav].parity + int(s & 1)) & 1;
         uint64_t* br = &bar[st];
         mbar_expect_tx(br, TS::STAGE_BYTES);
-        tma_load_3d(st ? stage1 : stage0, maps + 2 * I.cav + b, br, I.x0 - TILE_HX, I.y0 - TILE_HY, 0);
+        if (!no_copy)
+            tma_load_3d(st ? stage1 : stage0, maps + 2 * I.cav + b, br, I.x0 - TILE_HX, I.y0 - TILE_HY, 0);
     };
     if (threadIdx.x == 0 && int(blockIdx.x) < n_items) issue(blockIdx.x, 0);
     int k = 0;

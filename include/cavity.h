@@ -274,6 +274,12 @@ int cav_batch_get_tuning(cav_batch* b, cav_batch_tuning* t);
 int cav_batch_set_tuning(cav_batch* b, const cav_batch_tuning* t);
 int cav_batch_autotune(cav_batch* b, int32_t trial_steps, cav_batch_tuning* chosen);
 int cav_batch_sync(cav_batch* b);
+/* Test of the tile kernel's bounded waits (no counterpart in the reference):
+ * with on = 1 the tile kernel arms its barriers but issues no copy, every
+ * wait gives up after about a second and the next cav_batch_sync returns
+ * CAV_ERR_TIMEOUT (the steps of those launches are lost); on = 0 restores
+ * the copies.  Nothing is left in flight, the device stays usable. */
+int cav_batch_debug_stall_copies(cav_batch* b, int32_t on);
 int cav_batch_get_stream(cav_batch* b, void** stream);
 int cav_batch_launch_count(cav_batch* b, int64_t* n);
 
