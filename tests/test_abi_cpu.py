@@ -139,3 +139,40 @@ def test_octree_default_params_and_argument_checks():
         assert lib.cav_octree_create(ctypes.byref(q), ctypes.byref(h)) == L.CAV_ERR_ARG, field
         assert not h.value
         assert lib.cav_octree_last_error(None)
+
+
+# ---- struct layouts: the Python mirror of every public struct ----------------
+STRUCTS = [
+    ("cav_params", "CavParams"), ("cav_info", "CavInfo"), ("cav_diag_out", "CavDiag"),
+    ("cav_batch_tuning", "CavBatchTuning"), ("cav_adjoint_spec", "CavAdjointSpec"),
+    ("cav_adjoint_result", "CavAdjointResult"), ("cav_octree_params", "CavOctreeParams"),
+    ("cav_octree_info", "CavOctreeInfo"), ("cav_octree_diag_out", "CavOctreeDiag"),
+]
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """sizeof and every field's offset of the header's structs (compiled by
+    the C compiler) equal those of the ctypes mirrors in _lib.py."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "cavity.h"', "int main(void) {"]
+    for c_name, py_name in STRUCTS:
+        py = getattr(L, py_name)
+        lines.append(f'printf("{py_name} size %zu\\n", sizeof({c_name}));')
+        for f, _ in py._fields_:
+            lines.append(f'printf("{py_name} {f} %zu\\n", offsetof({c_name}, {f}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    for line in filter(None, out):
+        py_name, field, value = line.split()
+        py = getattr(L, py_name)
+        got = ctypes.sizeof(py) if field == "size" else getattr(py, field).offset
+        assert got == int(value), (py_name, field, got, value)
