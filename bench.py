@@ -305,10 +305,11 @@ def octree_c5(dev, chain=(30_000, 30_000, 60_000), window=40_000, sample_every=1
     return out
 
 
-def batch_only(precision, steps, tiles):
+def batch_only(precision, steps, kernel):
     """C3 batch timing alone (profiling runs): the 64-cavity sweep in one
     storage format with a fixed tuning (tile height 16, 4 CTAs per SM for
-    the global-memory kernel; the tile kernel's resident CTAs otherwise),
+    the persistent global-memory kernel; the tile kernel's resident CTAs
+    for kernels 1 / 2; one CTA per item for kernel 3),
     250 spin-up steps, then `steps` timed lattice steps."""
     import torch
 
@@ -317,7 +318,7 @@ def batch_only(precision, steps, tiles):
     cfg = sweep_configs(64)
     nodes = sum(c["nx"] * c["ny"] for c in cfg)
     bt = CavityBatch(cfg, precision=precision, device=0)
-    bt.set_tuning(16, 4 if tiles == 0 else 3, tiles=tiles)
+    bt.set_tuning(16, 4 if kernel == 0 else 3, kernel=kernel)
     bt.step(250)
     st = torch.cuda.ExternalStream(bt.stream_handle(), device=0)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -329,7 +330,7 @@ def batch_only(precision, steps, tiles):
     e1.synchronize()
     bt.sync()
     ms = e0.elapsed_time(e1)
-    print(json.dumps({"workload": f"batched sweep 64 cavities {precision}", "tiles": tiles, "steps": steps,
+    print(json.dumps({"workload": f"batched sweep 64 cavities {precision}", "kernel": kernel, "steps": steps,
                       "us_per_step": ms * 1e3 / steps, "mlups": nodes * steps / (ms * 1e-3) / 1e6}), flush=True)
     bt.close()
     return 0
@@ -427,14 +428,14 @@ def main():
                          "(FP32 / binary16) and print their device time (profiling runs)")
     ap.add_argument("--batch-only", default="", metavar="PRECISION",
                     help="only time the 64-cavity batched sweep in PRECISION for --steps lattice steps "
-                         "(profiling runs); --batch-tiles selects the kernel")
-    ap.add_argument("--batch-tiles", type=int, default=0, choices=[0, 1, 2])
+                         "(profiling runs); --batch-kernel selects the kernel")
+    ap.add_argument("--batch-kernel", type=int, default=0, choices=[0, 1, 2, 3])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.octree_only:
         return octree_only(args.octree_only)
     if args.batch_only:
-        return batch_only(args.batch_only, args.steps, args.batch_tiles)
+        return batch_only(args.batch_only, args.steps, args.batch_kernel)
     world, rank, local, dist = dist_setup(args)
     if args.impl == "reference":
         rc = run_reference(args, world, rank, dist)

@@ -65,7 +65,7 @@ class CavDiag(ctypes.Structure):
 
 
 class CavBatchTuning(ctypes.Structure):
-    _fields_ = [("rows_per_item", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32), ("tiles", ctypes.c_int32)]
+    _fields_ = [("rows_per_item", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32), ("kernel", ctypes.c_int32)]
 
 
 class CavAdjointSpec(ctypes.Structure):

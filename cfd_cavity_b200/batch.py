@@ -128,18 +128,19 @@ class CavityBatch:
     def tuning(self):
         t = L.CavBatchTuning()
         self._ck(L.load().cav_batch_get_tuning(self._b, ctypes.byref(t)))
-        return {"rows_per_item": t.rows_per_item, "ctas_per_sm": t.ctas_per_sm, "tiles": t.tiles}
+        return {"rows_per_item": t.rows_per_item, "ctas_per_sm": t.ctas_per_sm, "kernel": t.kernel}
 
-    def set_tuning(self, rows_per_item, ctas_per_sm, tiles=1):
-        """rows_per_item / ctas_per_sm of the global-memory kernel (tiles=0),
-        or the grid of the TMA tile kernel in tile shape 1 (the default) or 2."""
-        t = L.CavBatchTuning(rows_per_item, ctas_per_sm, int(tiles))
+    def set_tuning(self, rows_per_item, ctas_per_sm, kernel=3):
+        """kernel 0: the persistent global-memory kernel (rows_per_item,
+        ctas_per_sm); 1 / 2: the TMA tile kernel in tile shape 1 or 2
+        (ctas_per_sm); 3: one CTA per 32 x 4 item (the default)."""
+        t = L.CavBatchTuning(rows_per_item, ctas_per_sm, int(kernel))
         self._ck(L.load().cav_batch_set_tuning(self._b, ctypes.byref(t)))
 
     def autotune(self, trial_steps=64):
         t = L.CavBatchTuning()
         self._ck(L.load().cav_batch_autotune(self._b, int(trial_steps), ctypes.byref(t)))
-        return {"rows_per_item": t.rows_per_item, "ctas_per_sm": t.ctas_per_sm, "tiles": t.tiles}
+        return {"rows_per_item": t.rows_per_item, "ctas_per_sm": t.ctas_per_sm, "kernel": t.kernel}
 
     def debug_stall_copies(self, on):
         """Test of the tile kernel's bounded waits: arm the barriers but issue

@@ -64,10 +64,41 @@ __global__ void __launch_bounds__(BATCH_THREADS)
     }
 }
 
+// The same node body with one CTA per (cavity, 32-column x 4-row) item and
+// one node per thread (no persistent loop): the per-cavity pointers and
+// scalars are not kept live across items, so the kernel needs the
+// registers of k_fused, not of k_batch.
+constexpr int NP_ROWS = BATCH_THREADS / 32;
+template <class St, bool WRITE_NUT>
+__global__ void __launch_bounds__(BATCH_THREADS)
+    k_batch_np(const BatchCav<St>* __restrict__ cavs, const BatchItem* __restrict__ items,
+               const StepScalars<typename Fmt<St>::A>* __restrict__ table, int n_cav, long long step,
+               const long long* __restrict__ step_dev) {
+    using A = typename Fmt<St>::A;
+    pdl_wait();
+    pdl_trigger();
+    const long long s = step_dev ? *step_dev + step : step;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const BatchItem item = items[blockIdx.x];
+    const BatchCav<St>& cv = cavs[item.cav];
+    const int row = s < cv.spin_up ? int(s) : cv.spin_up;
+    StepScalars<A> c = table[(long long)row * n_cav + item.cav];
+    c.step = s;
+    c.step_dev = nullptr;
+    const int cur = (cv.parity + int(s & 1)) & 1;
+    const int ix = item.tx0 + lane;
+    if (ix < cv.G.nx && w < item.rows)
+        fused_node<St, WRITE_NUT, false, false>(cv.pop[cur], cv.pop[cur ^ 1], cv.fy, cv.nut, nullptr, nullptr, cv.G,
+                                                ix, item.ty0 + w, c);
+}
+
 struct BatchTuning {
     int rows_per_item = 8;
     int ctas_per_sm = 8;
-    int tiles = 1;  // 1, 2: the TMA tile kernel (k_tile) in tile shape 1 or 2; 0: k_batch
+    // 0: k_batch (persistent, one thread per node); 1, 2: k_tile (TMA-staged
+    // tiles, shape 1 or 2); 3: k_batch_np (one CTA per 32 x 4 item, the
+    // fastest on a B200 in every storage format)
+    int kernel = 3;
 };
 
 struct BatchBase {
@@ -103,6 +134,8 @@ struct Batch final : BatchBase {
     TileCav<St>* d_tcavs = nullptr;
     CUtensorMap* d_maps[3] = {nullptr, nullptr, nullptr};   // per tile shape
     TileItem* d_titems[3] = {nullptr, nullptr, nullptr};
+    BatchItem* d_np_items = nullptr;
+    int n_np_items = 0;
     unsigned* d_err = nullptr;
     unsigned* h_err = nullptr;  // pinned copy of *d_err
     int n_titems[3] = {0, 0, 0}, tgrid = 0;
@@ -111,8 +144,8 @@ struct Batch final : BatchBase {
     ~Batch() override {
         if (graph) cudaGraphExecDestroy(graph);
         if (h_err) cudaFreeHost(h_err);
-        void* bufs[] = {d_cavs,     d_items,     d_table,     step_dev,    d_tcavs, d_maps[1],
-                        d_maps[2], d_titems[1], d_titems[2], d_err};
+        void* bufs[] = {d_cavs,      d_items,     d_table, step_dev, d_tcavs,   d_maps[1],
+                        d_maps[2],   d_titems[1], d_titems[2], d_err,  d_np_items};
         for (void* b : bufs)
             if (b) cudaFree(b);
         for (Solver* s : cavs) delete s;
@@ -147,6 +180,17 @@ struct Batch final : BatchBase {
         *h_err = 0;
         setup_tiles<1>();
         setup_tiles<2>();
+        {
+            std::vector<BatchItem> ni;
+            for (int i = 0; i < n; ++i)
+                for (int y0 = 0; y0 < cv[i]->p.ny; y0 += NP_ROWS)
+                    for (int x0 = 0; x0 < cv[i]->p.nx; x0 += 32)
+                        ni.push_back({i, x0, y0, std::min(NP_ROWS, cv[i]->p.ny - y0)});
+            n_np_items = int(ni.size());
+            CK(cudaMalloc(&d_np_items, sizeof(BatchItem) * ni.size()));
+            CK(cudaMemcpyAsync(d_np_items, ni.data(), sizeof(BatchItem) * ni.size(), cudaMemcpyHostToDevice,
+                               stream));
+        }
         set_tuning(tun);
         CK(cudaStreamSynchronize(stream));
     }
@@ -186,7 +230,7 @@ struct Batch final : BatchBase {
 
     void set_tuning(const BatchTuning& t) override {
         if (t.rows_per_item < 1 || t.rows_per_item > 1024 || t.ctas_per_sm < 1 || t.ctas_per_sm > 32 ||
-            t.tiles < 0 || t.tiles > 2)
+            t.kernel < 0 || t.kernel > 3)
             throw ArgError{CAV_ERR_ARG, "tuning out of range"};
         tun = t;
         std::vector<BatchItem> items;
@@ -201,8 +245,8 @@ struct Batch final : BatchBase {
         CK(cudaMemcpyAsync(d_items, items.data(), sizeof(BatchItem) * items.size(), cudaMemcpyHostToDevice,
                            stream));
         grid = std::max(1, std::min(n_items, t.ctas_per_sm * n_sm));
-        if (t.tiles == 1) tgrid = tile_grid<1>(t.ctas_per_sm);
-        if (t.tiles == 2) tgrid = tile_grid<2>(t.ctas_per_sm);
+        if (t.kernel == 1) tgrid = tile_grid<1>(t.ctas_per_sm);
+        if (t.kernel == 2) tgrid = tile_grid<2>(t.ctas_per_sm);
         if (graph) {
             cudaGraphExecDestroy(graph);
             graph = nullptr;
@@ -278,9 +322,31 @@ struct Batch final : BatchBase {
                               int(stall_copies)));
     }
 
+    template <bool WN>
+    void launch_np(const long long* sdev, long long step) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(n_np_items);
+        cfg.blockDim = dim3(BATCH_THREADS);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CK(cudaLaunchKernelEx(&cfg, k_batch_np<St, WN>, (const BatchCav<St>*)d_cavs, (const BatchItem*)d_np_items,
+                              (const StepScalars<A>*)d_table, int(cv.size()), step, sdev));
+    }
+
     void launch(bool write_nut, const long long* sdev, long long step) {
-        if (tun.tiles) {
-            if (tun.tiles == 1)
+        if (tun.kernel == 3) {
+            write_nut ? launch_np<true>(sdev, step) : launch_np<false>(sdev, step);
+            ++launches;
+            CK(cudaGetLastError());
+            return;
+        }
+        if (tun.kernel == 1 || tun.kernel == 2) {
+            if (tun.kernel == 1)
                 write_nut ? launch_tiles<1, true>(sdev, step) : launch_tiles<1, false>(sdev, step);
             else
                 write_nut ? launch_tiles<2, true>(sdev, step) : launch_tiles<2, false>(sdev, step);

@@ -589,7 +589,7 @@ int cav_batch_get_tuning(cav_batch* b, cav_batch_tuning* t) {
     return bguarded(b, [&](BatchBase& x) {
         t->rows_per_item = x.tun.rows_per_item;
         t->ctas_per_sm = x.tun.ctas_per_sm;
-        t->tiles = x.tun.tiles;
+        t->kernel = x.tun.kernel;
     });
 }
 
@@ -599,7 +599,7 @@ int cav_batch_set_tuning(cav_batch* b, const cav_batch_tuning* t) {
         BatchTuning bt;
         bt.rows_per_item = t->rows_per_item;
         bt.ctas_per_sm = t->ctas_per_sm;
-        bt.tiles = t->tiles;
+        bt.kernel = t->kernel;
         x.set_tuning(bt);
     });
 }
@@ -616,23 +616,31 @@ int cav_batch_autotune(cav_batch* b, int32_t trial_steps, cav_batch_tuning* chos
             ps.push_back(p);
         }
         std::unique_ptr<BatchBase> twin(build_batch(ps.data(), int(ps.size())));
-        // candidates: the global-memory kernel over tile heights and grid
-        // sizes, then the shared-memory tile kernel over its grid sizes
+        // candidates: the persistent global-memory kernel over tile heights
+        // and grid sizes, the one-CTA-per-item kernel, then the shared-memory
+        // tile kernel over its shapes and grid sizes
         std::vector<BatchTuning> cand;
         for (int r : {2, 4, 8, 16, 32})
             for (int c : {4, 8, 12, 16}) {
                 BatchTuning t;
                 t.rows_per_item = r;
                 t.ctas_per_sm = c;
-                t.tiles = 0;
+                t.kernel = 0;
                 cand.push_back(t);
             }
+        {
+            BatchTuning t;
+            t.rows_per_item = x.tun.rows_per_item;
+            t.ctas_per_sm = x.tun.ctas_per_sm;
+            t.kernel = 3;
+            cand.push_back(t);
+        }
         for (int v : {1, 2})
             for (int c : {1, 2, 3, 4}) {
                 BatchTuning t;
                 t.rows_per_item = x.tun.rows_per_item;
                 t.ctas_per_sm = c;
-                t.tiles = v;
+                t.kernel = v;
                 cand.push_back(t);
             }
         BatchTuning best = x.tun;
@@ -653,7 +661,7 @@ int cav_batch_autotune(cav_batch* b, int32_t trial_steps, cav_batch_tuning* chos
         if (chosen) {
             chosen->rows_per_item = best.rows_per_item;
             chosen->ctas_per_sm = best.ctas_per_sm;
-            chosen->tiles = best.tiles;
+            chosen->kernel = best.kernel;
         }
     });
 }

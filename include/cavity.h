@@ -253,9 +253,10 @@ typedef struct cav_batch_tuning {
     int32_t rows_per_item; /* tile height of k_batch (tiles are 32 columns wide) */
     int32_t ctas_per_sm;   /* persistent grid = ctas_per_sm x #SMs CTAs (the tile
                               kernel: at most its resident CTAs per SM)          */
-    int32_t tiles;         /* 1, 2: TMA-staged shared-memory tiles in shape 1
-                              (default) or 2 (taller); 0: one thread per node
-                              from global memory                                 */
+    int32_t kernel;        /* 0: persistent, one thread per node from global
+                              memory; 1, 2: TMA-staged shared-memory tiles in
+                              shape 1 or 2 (taller); 3: one CTA per 32 x 4 item,
+                              one thread per node (default)                      */
 } cav_batch_tuning;
 int cav_batch_create(const cav_params* params, int32_t n, cav_batch** out);
 int cav_batch_destroy(cav_batch* b);

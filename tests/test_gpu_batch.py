@@ -42,17 +42,17 @@ def test_batch_is_bitwise_equal_to_single_cavities(precision):
 
 @pytest.mark.parametrize("precision", ["f64", "f32", "f16sr", "bf16", "f16gsr"])
 def test_batch_tuning_does_not_change_results(precision):
-    """Tile heights, grid sizes and the kernel (TMA-staged shared-memory tiles
-    or one thread per node from global memory) change no bit."""
+    """Tile heights, grid sizes and the kernel (persistent or one CTA per item
+    from global memory, TMA-staged shared-memory tiles) change no bit."""
     a = CavityBatch(MIXED, precision=precision)
     b = CavityBatch(MIXED, precision=precision)
-    a.set_tuning(3, 2, tiles=0)
-    b.set_tuning(32, 16, tiles=1)
+    a.set_tuning(3, 2, kernel=0)
+    b.set_tuning(32, 16, kernel=1)
     a.step(90)
     b.step(40)
-    b.set_tuning(5, 7, tiles=0)
+    b.set_tuning(5, 7, kernel=3)
     b.step(20)
-    b.set_tuning(5, 1, tiles=2)
+    b.set_tuning(5, 1, kernel=2)
     b.step(30)
     for i in range(len(MIXED)):
         fa, fb = a.fields(i), b.fields(i)
@@ -68,10 +68,10 @@ def test_autotune_picks_a_candidate_and_leaves_the_state_alone():
     b.step(10)
     ref.step(10)
     t = b.autotune(trial_steps=16)
-    assert t["tiles"] in (0, 1, 2)
-    if t["tiles"] == 0:
+    assert t["kernel"] in (0, 1, 2, 3)
+    if t["kernel"] == 0:
         assert t["rows_per_item"] in (2, 4, 8, 16, 32) and t["ctas_per_sm"] in (4, 8, 12, 16)
-    else:
+    elif t["kernel"] in (1, 2):
         assert t["ctas_per_sm"] in (1, 2, 3, 4)
     assert b.tuning() == t
     assert b.info()["time_step"] == 10
@@ -104,7 +104,7 @@ def test_tile_kernel_bounded_wait_reports_timeout_and_device_stays_usable():
     import time
 
     b = CavityBatch(MIXED[:2], precision="f16sr")
-    b.set_tuning(16, 2, tiles=1)
+    b.set_tuning(16, 2, kernel=1)
     b.step(3)
     b.sync()
     b.debug_stall_copies(True)
