@@ -130,10 +130,11 @@ class CavityBatch:
         self._ck(L.load().cav_batch_get_tuning(self._b, ctypes.byref(t)))
         return {"rows_per_item": t.rows_per_item, "ctas_per_sm": t.ctas_per_sm, "kernel": t.kernel}
 
-    def set_tuning(self, rows_per_item, ctas_per_sm, kernel=3):
+    def set_tuning(self, rows_per_item, ctas_per_sm, kernel=4):
         """kernel 0: the persistent global-memory kernel (rows_per_item,
         ctas_per_sm); 1 / 2: the TMA tile kernel in tile shape 1 or 2
-        (ctas_per_sm); 3: one CTA per 32 x 4 item (the default)."""
+        (ctas_per_sm); 3: one CTA per 32 x 4 item; 4: the same items, two
+        nodes per thread on packed FP32x2 arithmetic (the default)."""
         t = L.CavBatchTuning(rows_per_item, ctas_per_sm, int(kernel))
         self._ck(L.load().cav_batch_set_tuning(self._b, ctypes.byref(t)))
 

@@ -92,13 +92,41 @@ __global__ void __launch_bounds__(BATCH_THREADS)
                                                 ix, item.ty0 + w, c);
 }
 
+// k_batch_np with two rows per thread (fused_pair: the arithmetic of both
+// nodes on packed FP32x2 lanes): NP_ROWS / 2 warps per item.  FP32-arithmetic
+// formats only.  Register budget for 10 resident CTAs per SM (96 registers,
+// a few words spilled to L1): more warps to hide the loads' latency beat the
+// spill traffic on a B200.
+template <class St, bool WRITE_NUT>
+__global__ void __launch_bounds__(BATCH_THREADS / 2, 10)
+    k_batch_np2(const BatchCav<St>* __restrict__ cavs, const BatchItem* __restrict__ items,
+                const StepScalars<float>* __restrict__ table, int n_cav, long long step,
+                const long long* __restrict__ step_dev) {
+    pdl_wait();
+    pdl_trigger();
+    const long long s = step_dev ? *step_dev + step : step;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const BatchItem item = items[blockIdx.x];
+    const BatchCav<St>& cv = cavs[item.cav];
+    const int row = s < cv.spin_up ? int(s) : cv.spin_up;
+    StepScalars<float> c = table[(long long)row * n_cav + item.cav];
+    c.step = s;
+    c.step_dev = nullptr;
+    const int cur = (cv.parity + int(s & 1)) & 1;
+    const int ix = item.tx0 + lane;
+    if (ix < cv.G.nx && 2 * w < item.rows)
+        fused_pair<St, WRITE_NUT, false>(cv.pop[cur], cv.pop[cur ^ 1], cv.fy, cv.nut, nullptr, nullptr, cv.G, ix,
+                                         item.ty0 + 2 * w, 2 * w + 1 < item.rows, c);
+}
+
 struct BatchTuning {
     int rows_per_item = 8;
     int ctas_per_sm = 8;
     // 0: k_batch (persistent, one thread per node); 1, 2: k_tile (TMA-staged
-    // tiles, shape 1 or 2); 3: k_batch_np (one CTA per 32 x 4 item, the
-    // fastest on a B200 in every storage format)
-    int kernel = 3;
+    // tiles, shape 1 or 2); 3: k_batch_np (one CTA per 32 x 4 item);
+    // 4: k_batch_np2 (the same items, two nodes per thread on packed FP32x2
+    // lanes; the FP64 format has no such lanes and runs kernel 3)
+    int kernel = 4;
 };
 
 struct BatchBase {
@@ -230,7 +258,7 @@ struct Batch final : BatchBase {
 
     void set_tuning(const BatchTuning& t) override {
         if (t.rows_per_item < 1 || t.rows_per_item > 1024 || t.ctas_per_sm < 1 || t.ctas_per_sm > 32 ||
-            t.kernel < 0 || t.kernel > 3)
+            t.kernel < 0 || t.kernel > 4)
             throw ArgError{CAV_ERR_ARG, "tuning out of range"};
         tun = t;
         std::vector<BatchItem> items;
@@ -334,12 +362,21 @@ struct Batch final : BatchBase {
         attr[0].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
+        if constexpr (Fmt<St>::SHIFT) {
+            if (tun.kernel == 4) {
+                cfg.blockDim = dim3(BATCH_THREADS / 2);
+                CK(cudaLaunchKernelEx(&cfg, k_batch_np2<St, WN>, (const BatchCav<St>*)d_cavs,
+                                      (const BatchItem*)d_np_items, (const StepScalars<float>*)d_table, int(cv.size()),
+                                      step, sdev));
+                return;
+            }
+        }
         CK(cudaLaunchKernelEx(&cfg, k_batch_np<St, WN>, (const BatchCav<St>*)d_cavs, (const BatchItem*)d_np_items,
                               (const StepScalars<A>*)d_table, int(cv.size()), step, sdev));
     }
 
     void launch(bool write_nut, const long long* sdev, long long step) {
-        if (tun.kernel == 3) {
+        if (tun.kernel == 3 || tun.kernel == 4) {
             write_nut ? launch_np<true>(sdev, step) : launch_np<false>(sdev, step);
             ++launches;
             CK(cudaGetLastError());

@@ -617,8 +617,9 @@ int cav_batch_autotune(cav_batch* b, int32_t trial_steps, cav_batch_tuning* chos
         }
         std::unique_ptr<BatchBase> twin(build_batch(ps.data(), int(ps.size())));
         // candidates: the persistent global-memory kernel over tile heights
-        // and grid sizes, the one-CTA-per-item kernel, then the shared-memory
-        // tile kernel over its shapes and grid sizes
+        // and grid sizes, the one-CTA-per-item kernels (one or two nodes per
+        // thread), then the shared-memory tile kernel over its shapes and
+        // grid sizes
         std::vector<BatchTuning> cand;
         for (int r : {2, 4, 8, 16, 32})
             for (int c : {4, 8, 12, 16}) {
@@ -628,11 +629,11 @@ int cav_batch_autotune(cav_batch* b, int32_t trial_steps, cav_batch_tuning* chos
                 t.kernel = 0;
                 cand.push_back(t);
             }
-        {
+        for (int k : {3, 4}) {
             BatchTuning t;
             t.rows_per_item = x.tun.rows_per_item;
             t.ctas_per_sm = x.tun.ctas_per_sm;
-            t.kernel = 3;
+            t.kernel = k;
             cand.push_back(t);
         }
         for (int v : {1, 2})

@@ -30,7 +30,8 @@ __device__ __forceinline__ void stp(St* __restrict__ buf, const Geom& G, int q, 
 // Stores the 18 populations of one node (32-bit offsets, like pull_node);
 // the stochastically rounded formats draw their random bits from the
 // (seed, step, node) stream, two 16-bit draws per generator step.
-template <class St>
+// LANE: f and g in lane units (Fmt::lstore).
+template <class St, bool LANE = false>
 __device__ __forceinline__ void store_node(St* __restrict__ dst, const Geom& G, int iy, int ix,
                                            const typename Fmt<St>::A (&f)[Q], const typename Fmt<St>::A (&g)[Q],
                                            const StepScalars<typename Fmt<St>::A>& c) {
@@ -45,11 +46,41 @@ __device__ __forceinline__ void store_node(St* __restrict__ dst, const Geom& G, 
             // high half of an LCG output, then its bits 0..15 shifted up
             if ((q & 1) == 0) r = rng.next();
             const uint32_t bits = (q & 1) == 0 ? (r & 0xffff0000u) : (r << 16);
-            dst[q * P + k] = Fmt<St>::store_sr(q < Q ? f[q] : g[q - Q], q, bits);
+            const auto x = q < Q ? f[q] : g[q - Q];
+            dst[q * P + k] = LANE ? Fmt<St>::lstore_sr(x, q, bits) : Fmt<St>::store_sr(x, q, bits);
         }
     } else {
 #pragma unroll
-        for (int q = 0; q < NPLANES; ++q) dst[q * P + k] = Fmt<St>::store(q < Q ? f[q] : g[q - Q], q, RN_BITS);
+        for (int q = 0; q < NPLANES; ++q) {
+            const auto x = q < Q ? f[q] : g[q - Q];
+            dst[q * P + k] = LANE ? Fmt<St>::lstore(x, q, RN_BITS) : Fmt<St>::store(x, q, RN_BITS);
+        }
+    }
+}
+
+// Stores the 9 planes Q0..Q0+8 (Q0 = 0: f, Q0 = 9: g) of one node from lane
+// units, drawing the same random bits per plane as store_node.
+template <class St, int Q0>
+__device__ __forceinline__ void store_planes(St* __restrict__ dst, const Geom& G, int iy, int ix,
+                                             const typename Fmt<St>::A (&v)[Q],
+                                             const StepScalars<typename Fmt<St>::A>& c) {
+    const int P = int(G.plane);
+    const int k = iy * G.pitch + ix;
+    if constexpr (Fmt<St>::SR) {
+        const long long step = c.step_dev ? *c.step_dev + c.step : c.step;
+        NodeRng rng(c.sr_seed, step, (long long)iy * G.nx + ix);
+#pragma unroll
+        for (int j = 0; j < Q0 / 2; ++j) rng.next();  // the draws of planes 0..Q0-1
+        uint32_t r = (Q0 & 1) ? rng.next() : 0u;
+#pragma unroll
+        for (int q = Q0; q < Q0 + Q; ++q) {
+            if ((q & 1) == 0) r = rng.next();
+            const uint32_t bits = (q & 1) == 0 ? (r & 0xffff0000u) : (r << 16);
+            dst[q * P + k] = Fmt<St>::lstore_sr(v[q - Q0], q, bits);
+        }
+    } else {
+#pragma unroll
+        for (int q = Q0; q < Q0 + Q; ++q) dst[q * P + k] = Fmt<St>::lstore(v[q - Q0], q, RN_BITS);
     }
 }
 
@@ -72,7 +103,8 @@ static __global__ void k_add_step(long long* p, long long d) { *p += d; }
 //  row, as the vertical loop runs first).  Every other g source is inside
 //  the domain, so the reference's "keep g at out-of-domain sources" value
 //  is always overwritten and never needed here.
-template <class St>
+// LANE: values in lane units (Fmt::lload).
+template <class St, bool LANE = false>
 __device__ __forceinline__ void pull_f(const St* __restrict__ src, const Geom& G, int ix, int iy,
                                        typename Fmt<St>::A (&f)[Q]) {
     // 32-bit element offsets: 18 * plane < 2^31 is checked at allocation.
@@ -84,11 +116,11 @@ __device__ __forceinline__ void pull_f(const St* __restrict__ src, const Geom& G
         const int cx = CX(i), cy = CY(i);
         const bool ok = (cx > 0 ? xm : (cx < 0 ? xp : true)) && (cy > 0 ? ym : (cy < 0 ? yp : true));
         const int idx = ok ? i * P + k - cx - cy * W : OPP(i) * P + k;  // else bounce-back
-        f[i] = Fmt<St>::load(src[idx], i);
+        f[i] = LANE ? Fmt<St>::lload(src[idx], i) : Fmt<St>::load(src[idx], i);
     }
 }
 
-template <class St>
+template <class St, bool LANE = false>
 __device__ __forceinline__ void pull_g(const St* __restrict__ src, const Geom& G, int ix, int iy,
                                        const StepScalars<typename Fmt<St>::A>& c, typename Fmt<St>::A (&g)[Q]) {
     using A = typename Fmt<St>::A;
@@ -96,23 +128,24 @@ __device__ __forceinline__ void pull_g(const St* __restrict__ src, const Geom& G
     const int k = iy * W + ix;
     const int gy = iy == 0 ? 1 : (iy == G.ny - 1 ? G.ny - 2 : iy);
     const bool wall_col = (ix == 0) || (ix == G.nx - 1);
-    const A tw = ix == 0 ? c.t_hot[gy] : c.t_cold;
+    // (w_i T scaled by a power of two is w_i T rounded, scaled)
+    const A tw = (ix == 0 ? c.t_hot[gy] : c.t_cold) * A(LANE ? p2(Fmt<St>::EG) : 1.0f);
     const int kg = wall_col ? k : gy * W + ix;
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
         // wall columns read their own node (a valid address) and discard it
         const int idx = (Q + i) * P + (wall_col ? kg : kg - CX(i) - CY(i) * W);
-        const A v = Fmt<St>::load(src[idx], Q + i);
+        const A v = LANE ? Fmt<St>::lload(src[idx], Q + i) : Fmt<St>::load(src[idx], Q + i);
         g[i] = wall_col ? geq_rest<A>(i, tw, c.geq_order) : v;
     }
 }
 
-template <class St>
+template <class St, bool LANE = false>
 __device__ __forceinline__ void pull_node(const St* __restrict__ src, const Geom& G, int ix, int iy,
                                           const StepScalars<typename Fmt<St>::A>& c,
                                           typename Fmt<St>::A (&f)[Q], typename Fmt<St>::A (&g)[Q]) {
-    pull_f<St>(src, G, ix, iy, f);
-    pull_g<St>(src, G, ix, iy, c, g);
+    pull_f<St, LANE>(src, G, ix, iy, f);
+    pull_g<St, LANE>(src, G, ix, iy, c, g);
 }
 
 // Temperature of node (ix, iy) of the streamed state, gathered from a PC
@@ -133,10 +166,7 @@ __device__ __forceinline__ typename Fmt<St>::A gather_t(const St* __restrict__ s
 #pragma unroll
         for (int i = 0; i < Q; ++i) g[i] = ldp(src, G, Q + i, gy - CY(i), ix - CX(i));
     }
-    A t = g[0];
-#pragma unroll
-    for (int j = 1; j < Q; ++j) t = t + g[j];
-    return t;
+    return sum_g<A>(g);
 }
 
 __device__ __forceinline__ bool is_wall(const Geom& G, int ix, int iy) {
@@ -158,7 +188,8 @@ __device__ __forceinline__ bool is_wall(const Geom& G, int ix, int iy) {
 // macroscopic, no-slip, the Nusselt accumulation (t_at(x) gives T of the
 // streamed state at column x of the same row), the collision, the stores.
 // Shared by the global-memory pull (fused_node_io) and the shared-memory
-// tiles (tile.cuh), so both give the same bits.
+// tiles (tile.cuh), so both give the same bits.  f and g arrive in lane units
+// (pull with LANE); t_at returns T unscaled.
 template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE, class TAt>
 __device__ __forceinline__ void fused_core(typename Fmt<St>::A (&f)[Q], typename Fmt<St>::A (&g)[Q],
                                            St* __restrict__ dst, const typename Fmt<St>::A* fy_in,
@@ -168,26 +199,37 @@ __device__ __forceinline__ void fused_core(typename Fmt<St>::A (&f)[Q], typename
                                            TAt&& t_at) {
     using A = typename Fmt<St>::A;
     constexpr bool SH = Fmt<St>::SHIFT;
+    constexpr int EF = Fmt<St>::EF, EG = Fmt<St>::EG;
     const int k = iy * G.pitch + ix;
     const bool wall = is_wall(G, ix, iy);
-    Macro<A, SH> m = macro_node<A, SH>(f, g, fy_in[k], wall);
+    Macro<A, SH> m;
+    if constexpr (SH) {
+        m = macro_f_lane<A, EF>(f, fy_in[k], wall);
+        m.t = sum_g<A>(g);
+    } else {
+        m = macro_node<A, SH>(f, g, fy_in[k], wall);
+    }
     if (ACC_NU) {
+        const A t = m.t * A(p2(-EG));
         if (ix == 1) {
             A t2 = t_at(2);
-            acc_hot[iy] += fabs(double(m.t) - double(t2));
+            acc_hot[iy] += fabs(double(t) - double(t2));
         }
         if (ix == G.nx - 2) {
             A t0 = t_at(G.nx - 3);
-            acc_cold[iy] += fabs(double(m.t) - double(t0));
+            acc_cold[iy] += fabs(double(t) - double(t0));
         }
     }
     A fyv, nutv;
     if (!NO_COLLIDE) {
-        collide_node<A, SH>(f, g, m, c, fyv, nutv);
+        if constexpr (SH)
+            collide_node_lane<A, EF, EG>(f, g, m, c, fyv, nutv);
+        else
+            collide_node<A, SH>(f, g, m, c, fyv, nutv);
         fy_out[k] = fyv;
         if (WRITE_NUT) nut[k] = nutv;
     }
-    store_node<St>(dst, G, iy, ix, f, g, c);
+    store_node<St, true>(dst, G, iy, ix, f, g, c);
 }
 
 template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE>
@@ -198,7 +240,7 @@ __device__ __forceinline__ void fused_node_io(const St* __restrict__ src, St* __
                                               const StepScalars<typename Fmt<St>::A>& c) {
     using A = typename Fmt<St>::A;
     A f[Q], g[Q];
-    pull_node<St>(src, G, ix, iy, c, f, g);
+    pull_node<St, true>(src, G, ix, iy, c, f, g);
     fused_core<St, WRITE_NUT, ACC_NU, NO_COLLIDE>(f, g, dst, fy_in, fy_out, nut, acc_hot, acc_cold, G, ix, iy, c,
                                                   [&](int x) { return gather_t<St>(src, G, x, iy, c); });
 }
@@ -209,6 +251,72 @@ __device__ __forceinline__ void fused_node(const St* __restrict__ src, St* __res
                                            double* __restrict__ acc_hot, double* __restrict__ acc_cold,
                                            const Geom& G, int ix, int iy, const StepScalars<typename Fmt<St>::A>& c) {
     fused_node_io<St, WRITE_NUT, ACC_NU, NO_COLLIDE>(src, dst, fy, fy, nut, acc_hot, acc_cold, G, ix, iy, c);
+}
+
+// Two nodes of one column, (ix, iy) and (ix, iy + 1), in one thread: the
+// pulls, boundary conditions and stores per node, the macroscopic update and
+// the collision of both on packed FP32x2 lanes (one add / mul / fma
+// instruction for the two nodes).  The lane arithmetic rounds every operation
+// once, so each node gets the bits fused_node gives it.  hi: whether
+// (ix, iy + 1) is in the grid (else the upper lane recomputes (ix, iy) and
+// is not stored).
+template <class St, bool WRITE_NUT, bool ACC_NU>
+__device__ __forceinline__ void fused_pair(const St* __restrict__ src, St* __restrict__ dst, float* fy,
+                                           float* __restrict__ nut, double* __restrict__ acc_hot,
+                                           double* __restrict__ acc_cold, const Geom& G, int ix, int iy, bool hi,
+                                           const StepScalars<float>& c) {
+    static_assert(Fmt<St>::SHIFT, "the two-node lanes carry the FP32 arithmetic");
+    constexpr int EF = Fmt<St>::EF, EG = Fmt<St>::EG;
+    const int iy1 = hi ? iy + 1 : iy;
+    float fa[Q], ga[Q], fb[Q], gb[Q];
+    pull_node<St, true>(src, G, ix, iy, c, fa, ga);
+    pull_node<St, true>(src, G, ix, iy1, c, fb, gb);
+    float2 f[Q], g[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        f[i] = make_float2(fa[i], fb[i]);
+        g[i] = make_float2(ga[i], gb[i]);
+    }
+    const int k0 = iy * G.pitch + ix, k1 = iy1 * G.pitch + ix;
+    Macro<float2, true> m = macro_f_lane<float2, EF>(f, make_float2(fy[k0], fy[k1]),
+                                                     Mask2{is_wall(G, ix, iy), is_wall(G, ix, iy1)});
+    m.t = sum_g<float2>(g);
+    if (ACC_NU) {
+        const float ta = m.t.x * p2(-EG), tb = m.t.y * p2(-EG);
+        if (ix == 1) {
+            acc_hot[iy] += fabs(double(ta) - double(gather_t<St>(src, G, 2, iy, c)));
+            if (hi) acc_hot[iy1] += fabs(double(tb) - double(gather_t<St>(src, G, 2, iy1, c)));
+        }
+        if (ix == G.nx - 2) {
+            acc_cold[iy] += fabs(double(ta) - double(gather_t<St>(src, G, G.nx - 3, iy, c)));
+            if (hi) acc_cold[iy1] += fabs(double(tb) - double(gather_t<St>(src, G, G.nx - 3, iy1, c)));
+        }
+    }
+    // the collision in the order that frees registers soonest: the f
+    // coefficients, then g (collided and stored), then f
+    const CollF<float2> o = collide_f_pre_lane<float2, EF>(f, m, c, nullptr);
+    collide_g_lane<float2>(g, m.t, m.ux, m.uy, o.nut, o.q, c, nullptr);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        ga[i] = g[i].x;
+        gb[i] = g[i].y;
+    }
+    store_planes<St, Q>(dst, G, iy, ix, ga, c);
+    if (hi) store_planes<St, Q>(dst, G, iy1, ix, gb, c);
+    const float2 fyv = collide_f_post_lane<float2, EF, EG>(f, o, m, c, m.t);
+    fy[k0] = fyv.x;
+    if (WRITE_NUT) nut[k0] = o.nut.x;
+    if (hi) {
+        fy[k1] = fyv.y;
+        if (WRITE_NUT) nut[k1] = o.nut.y;
+    }
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        fa[i] = f[i].x;
+        fb[i] = f[i].y;
+    }
+    store_planes<St, 0>(dst, G, iy, ix, fa, c);
+    if (hi) store_planes<St, 0>(dst, G, iy1, ix, fb, c);
 }
 
 // One full reference step, PC(src) -> PC(dst), one thread per node.

@@ -22,6 +22,8 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <type_traits>
+
 namespace cav {
 
 constexpr int Q = 9;
@@ -52,6 +54,16 @@ constexpr double LAMBDA_TRT = 3.0 / 16.0;
 // ---------------------------------------------------------------------------
 constexpr uint32_t RN_BITS = 0x80000000u;
 
+// 2^e as a float constant (|e| < 64).
+__host__ __device__ constexpr float p2(int e) {
+    return e >= 0 ? float(1ull << e) : 1.0f / float(1ull << -e);
+}
+
+// Lane units.  The fused step works on the f planes scaled by 2^EF and the g
+// planes by 2^EG (the formats' own power-of-two scales, so that lload is a
+// bare decode and lstore a bare encode); power-of-two scaling commutes with
+// rounding, and the physics folds the factors into its constants.
+
 template <class St>
 struct Fmt;
 
@@ -59,32 +71,39 @@ template <>
 struct Fmt<double> {
     using A = double;
     static constexpr bool SHIFT = false, SR = false;
+    static constexpr int EF = 0, EG = 0;
     __host__ __device__ static A load(double v, int) { return v; }
     __host__ __device__ static double store(A v, int, uint32_t) { return v; }
+    __host__ __device__ static A lload(double v, int) { return v; }
+    __host__ __device__ static double lstore(A v, int, uint32_t) { return v; }
 };
 template <>
 struct Fmt<float> {
     using A = float;
     static constexpr bool SHIFT = true, SR = false;
+    static constexpr int EF = 0, EG = 0;
     __host__ __device__ static A load(float v, int) { return v; }
     __host__ __device__ static float store(A v, int, uint32_t) { return v; }
+    __host__ __device__ static A lload(float v, int) { return v; }
+    __host__ __device__ static float lstore(A v, int, uint32_t) { return v; }
 };
 
 // binary16 of x * 2^15 (the 2^15 keeps |f - w| >= 2e-9 out of the subnormals).
 constexpr float H_SCALE = 32768.0f, H_INV = 1.0f / 32768.0f;
 
-__host__ __device__ __forceinline__ float h16_load(unsigned short bits) {
+__host__ __device__ __forceinline__ float h16_raw(unsigned short bits) {
     __half_raw r;
     r.x = bits;
-    return __half2float(__half(r)) * H_INV;
+    return __half2float(__half(r));
 }
+__host__ __device__ __forceinline__ float h16_load(unsigned short bits) { return h16_raw(bits) * H_INV; }
 // Round to nearest (ties to even), or stochastically: add 13 random bits
 // below binary16's last mantissa bit to the binary32 magnitude, then
 // truncate (Croci et al., "Stochastic rounding: implementation, error
 // analysis and applications", R. Soc. open sci. 2022).  Unbiased:
 // E[round(x)] = x.
-__host__ __device__ __forceinline__ unsigned short h16_store(float x, bool sr, uint32_t r) {
-    float s = x * H_SCALE;
+// h16_enc takes x already scaled by 2^15.
+__host__ __device__ __forceinline__ unsigned short h16_enc(float s, bool sr, uint32_t r) {
     __half h;
     if (sr) {
         // (a non-finite input stays non-finite: inf + dither becomes NaN)
@@ -97,6 +116,9 @@ __host__ __device__ __forceinline__ unsigned short h16_store(float x, bool sr, u
         h = __float2half_rn(s);
     }
     return __half_raw(h).x;
+}
+__host__ __device__ __forceinline__ unsigned short h16_store(float x, bool sr, uint32_t r) {
+    return h16_enc(x * H_SCALE, sr, r);
 }
 
 __host__ __device__ __forceinline__ float bf16_load(unsigned short bits) {
@@ -151,6 +173,28 @@ struct Fmt<P16<KIND, SRND>> {
     using A = float;
     using St = P16<KIND, SRND>;
     static constexpr bool SHIFT = true, SR = SRND;
+    static constexpr int EF = KIND == K_BF16 ? 0 : 15, EG = KIND == K_HALF ? 15 : 0;
+    // lane units: binary16 planes undecoded by the 2^15 (see EF / EG)
+    __host__ __device__ static A lload(St v, int q) {
+        if (KIND == K_BF16) return bf16_load(v.bits);
+        if (KIND == K_MIX && q >= 9) return fx_load(v.bits, q);
+        return h16_raw(v.bits);
+    }
+    __host__ __device__ static St lstore(A x, int q, uint32_t r) {
+        const bool sr = SRND && r != RN_BITS;
+        St o;
+        if (KIND == K_BF16) o.bits = bf16_store(x, sr, r);
+        else if (KIND == K_MIX && q >= 9) o.bits = fx_store(x, q, sr, r);
+        else o.bits = h16_enc(x, sr, r);
+        return o;
+    }
+    __host__ __device__ static St lstore_sr(A x, int q, uint32_t r) {
+        St o;
+        if (KIND == K_BF16) o.bits = bf16_store(x, true, r);
+        else if (KIND == K_MIX && q >= 9) o.bits = fx_store(x, q, true, r);
+        else o.bits = h16_enc(x, true, r);
+        return o;
+    }
     __host__ __device__ static A load(St v, int q) {
         if (KIND == K_BF16) return bf16_load(v.bits);
         if (KIND == K_MIX && q >= 9) return fx_load(v.bits, q);
@@ -251,19 +295,76 @@ __host__ __device__ __forceinline__ A geq_full(int i, A t, A ux, A uy, int order
     return A(WD(i)) * t * (A(1.0) + eu / cs2 + eu * eu / (A(2.0) * cs2 * cs2) - u2 / (A(2.0) * cs2));
 }
 
-// FP32 shifted equilibrium: feq_i - w_i = w_i*(drho + rho*P_i),
-// P_i = 3 e.u + 4.5 (e.u)^2 - 1.5 u^2.
-__device__ __forceinline__ float feq_shift_f32(int i, float drho, float rho, float ux, float uy) {
-    float eu = float(CX(i)) * ux + float(CY(i)) * uy;
-    float u2 = ux * ux + uy * uy;
-    float P = 3.0f * eu + 4.5f * eu * eu - 1.5f * u2;
-    return float(WD(i)) * (drho + rho * P);
+// ---------------------------------------------------------------------------
+// Lane arithmetic of the FP32 physics.  The FP32 macroscopic update and
+// collision are written once over a lane type L: float (one node) or float2
+// (two nodes in one thread, on Blackwell's packed FP32x2 add / mul / fma:
+// one instruction for both nodes).  Every operation is an explicitly rounded
+// intrinsic, so the compiler contracts nothing and a node gets the same bits
+// from either lane type, in whichever kernel it runs.
+// ---------------------------------------------------------------------------
+struct Mask2 {
+    bool x, y;
+};
+template <class L>
+struct LaneMask;
+template <>
+struct LaneMask<float> {
+    using T = bool;
+};
+template <>
+struct LaneMask<float2> {
+    using T = Mask2;
+};
+
+__device__ __forceinline__ float ladd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float lsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float lmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float lfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float2 ladd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+// a - b as fma(b, -1, a): b * -1 is exact, so this is the one rounding of
+// a - b that __fsub_rn gives.
+__device__ __forceinline__ float2 lsub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
+__device__ __forceinline__ float2 lmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 lfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+template <class L>
+__device__ __forceinline__ L lbc(float s);
+template <>
+__device__ __forceinline__ float lbc<float>(float s) {
+    return s;
 }
-__device__ __forceinline__ float geq_f32(int i, float t, float ux, float uy, int order) {
-    float eu = float(CX(i)) * ux + float(CY(i)) * uy;
-    if (order == 1) return float(WD(i)) * t * (1.0f + 3.0f * eu);
-    float u2 = ux * ux + uy * uy;
-    return float(WD(i)) * t * (1.0f + 3.0f * eu + 4.5f * eu * eu - 1.5f * u2);
+template <>
+__device__ __forceinline__ float2 lbc<float2>(float s) {
+    return make_float2(s, s);
+}
+
+// 1/x and sqrt(x) from the special-function unit (rcp.approx / sqrt.approx,
+// about one ulp); the arguments here are normal numbers or zero.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float lrcp(float x) { return rcp_approx(x); }
+__device__ __forceinline__ float2 lrcp(float2 x) { return make_float2(rcp_approx(x.x), rcp_approx(x.y)); }
+__device__ __forceinline__ float lsqrt(float x) { return sqrt_approx(x); }
+__device__ __forceinline__ float2 lsqrt(float2 x) { return make_float2(sqrt_approx(x.x), sqrt_approx(x.y)); }
+__device__ __forceinline__ float lsel(bool m, float a, float b) { return m ? a : b; }
+__device__ __forceinline__ float2 lsel(Mask2 m, float2 a, float2 b) {
+    return make_float2(m.x ? a.x : b.x, m.y ? a.y : b.y);
+}
+
+// c_i . u for the directions p = 1..4 of the (p, p + 4) pairs:
+// E (1, 0), N (0, 1), NE (1, 1), NW (-1, 1).
+template <class L>
+__device__ __forceinline__ L eu_pair(int p, L u, L v) {
+    return p == 1 ? u : (p == 2 ? v : (p == 3 ? ladd(u, v) : lsub(v, u)));
 }
 
 // ---------------------------------------------------------------------------
@@ -276,47 +377,75 @@ struct Macro {
     A rho, drho, ux, uy, t, inv_rho;
 };
 
+// T = sum of g: the reference's order in FP64; a balanced tree in the FP32
+// lane arithmetic.
 template <class A>
 __device__ __forceinline__ A sum_g(const A (&g)[Q]) {
-    A tn = g[0];
+    if constexpr (std::is_same<A, double>::value) {
+        A tn = g[0];
 #pragma unroll
-    for (int j = 1; j < Q; ++j) tn = tn + g[j];
-    return tn;
+        for (int j = 1; j < Q; ++j) tn = tn + g[j];
+        return tn;
+    } else {
+        return ladd(ladd(g[0], ladd(ladd(g[1], g[5]), ladd(g[2], g[6]))), ladd(ladd(g[3], g[7]), ladd(g[4], g[8])));
+    }
+}
+
+// FP32 rho and u on the shifted populations h_i = f_i - w_i, from the pair
+// sums a_p = h_p + h_opp and differences d_p = h_p - h_opp (p = 1..4; the
+// collision reuses them): rho - 1 = h_0 + sum a_p, rho u_x = d_E + d_NE - d_NW,
+// rho u_y = d_N + d_NE + d_NW, plus half the previous Guo force in u_y.
+// f in lane units (h 2^EF): drho comes out scaled by 2^EF, rho and u not.
+template <class L, int EF = 0>
+__device__ __forceinline__ Macro<L, true> macro_f_lane(const L (&f)[Q], L fy_prev, typename LaneMask<L>::T wall) {
+    L a[5], d[5];
+#pragma unroll
+    for (int p = 1; p <= 4; ++p) {
+        a[p] = ladd(f[p], f[p + 4]);
+        d[p] = lsub(f[p], f[p + 4]);
+    }
+    Macro<L, true> m;
+    m.drho = ladd(ladd(f[0], ladd(a[1], a[2])), ladd(a[3], a[4]));
+    if constexpr (EF == 0)
+        m.rho = ladd(lbc<L>(1.0f), m.drho);
+    else
+        m.rho = lfma(m.drho, lbc<L>(p2(-EF)), lbc<L>(1.0f));
+    m.inv_rho = lrcp(m.rho);
+    const L inv_s = EF == 0 ? m.inv_rho : lmul(m.inv_rho, lbc<L>(p2(-EF)));
+    const L un = lmul(lsub(ladd(d[1], d[3]), d[4]), inv_s);
+    const L vn = lmul(lfma(lbc<L>(0.5f * p2(EF)), fy_prev, ladd(ladd(d[2], d[3]), d[4])), inv_s);
+    m.ux = lsel(wall, lbc<L>(0.0f), un);
+    m.uy = lsel(wall, lbc<L>(0.0f), vn);
+    m.t = lbc<L>(0.0f);
+    return m;
 }
 
 // rho and u of the node (t left 0): the f part of macro_node.
 template <class A, bool SHIFT>
 __device__ __forceinline__ Macro<A, SHIFT> macro_f(const A (&f)[Q], A fy_prev, bool wall) {
-    Macro<A, SHIFT> m;
-    A s = f[0];
-#pragma unroll
-    for (int j = 1; j < Q; ++j) s = s + f[j];
-    A un = ((((f[1] + f[3]) - f[4]) - f[5]) - f[7]) + f[8];
-    A vn = ((((f[2] + f[3]) + f[4]) - f[6]) - f[7]) - f[8];
-    A r;
-    m.inv_rho = A(0.0);
-    if (SHIFT) {
-        m.drho = s;
-        r = A(1.0) + s;
-    } else {
-        r = s;
-        m.drho = s - A(1.0);
-    }
     if constexpr (SHIFT) {
-        const A inv = __fdividef(1.0f, r);
-        m.inv_rho = inv;
-        un = un * inv;
-        vn = (vn + A(0.5) * fy_prev) * inv;
-    } else if (r > A(2.220446049250313e-16)) {
-        un = un / r;
-        vn = vn / r;
-        vn = vn + A(0.5) * fy_prev / r;
+        return macro_f_lane<A>(f, fy_prev, wall);
+    } else {
+        Macro<A, SHIFT> m;
+        A s = f[0];
+#pragma unroll
+        for (int j = 1; j < Q; ++j) s = s + f[j];
+        A un = ((((f[1] + f[3]) - f[4]) - f[5]) - f[7]) + f[8];
+        A vn = ((((f[2] + f[3]) + f[4]) - f[6]) - f[7]) - f[8];
+        const A r = s;
+        m.drho = s - A(1.0);
+        m.inv_rho = A(0.0);
+        if (r > A(2.220446049250313e-16)) {
+            un = un / r;
+            vn = vn / r;
+            vn = vn + A(0.5) * fy_prev / r;
+        }
+        m.rho = r;
+        m.ux = wall ? A(0.0) : un;
+        m.uy = wall ? A(0.0) : vn;
+        m.t = A(0.0);
+        return m;
     }
-    m.rho = r;
-    m.ux = wall ? A(0.0) : un;
-    m.uy = wall ? A(0.0) : vn;
-    m.t = A(0.0);
-    return m;
 }
 
 template <class A, bool SHIFT>
@@ -341,8 +470,113 @@ template <class A>
 struct CollF {
     A d[Q];                // FP64: f - feq
     A d0, dS[5], dD[5];    // FP32: rest part, symmetric / antisymmetric pair parts
+    A q[5];                // FP32: 4.5 (c_p.u)^2 - 1.5 u^2 (shared with the g equilibrium)
     A nut, w1, w2, k1, k2; // FP64 a_f, b_f, k-, k+;  FP32 om+, om-, k+, k-
 };
+
+// ---- FP32 collision over a lane type (float: one node, float2: two) --------
+// On h_i = f_i - w_i, pairwise: for each pair p = (i, i+4), i = 1..4, split
+// populations and equilibria into symmetric / antisymmetric parts.  The TRT
+// update f_i += -a d_i - b d_opp + (1 - 1/2tau-) S-_i + (1 - 1/2tau+) S+_i
+// with a = (w+ + w-)/2, b = (w+ - w-)/2 is exactly
+//   f_p += E + O, f_opp += E - O,
+//   E = -w+ (d_p + d_opp)/2 + k+ S+_p,  O = -w- (d_p - d_opp)/2 + k- S-_p,
+// and pi_neq only needs the symmetric parts.  Same arithmetic as the
+// reference up to rounding, a third of the operations.  f, drho and the
+// non-equilibrium parts in lane units (scaled by 2^EF).
+template <class L, int EF = 0>
+__device__ __forceinline__ CollF<L> collide_f_pre_lane(const L (&f)[Q], const Macro<L, true>& m,
+                                                       const StepScalars<float>& c, const L* nut_ovr) {
+    CollF<L> o;
+    const L u = m.ux, v = m.uy;
+    const L r = EF == 0 ? m.rho : lmul(m.rho, lbc<L>(p2(EF)));  // rho 2^EF
+    const L u2 = lfma(u, u, lmul(v, v));
+    const L m15u2 = lmul(lbc<L>(-1.5f), u2);
+    // rest: h_0 - (feq_0 - w_0) = h_0 - w_0 (drho - 1.5 rho u^2)
+    o.d0 = lfma(lbc<L>(-float(WD(0))), lfma(r, m15u2, m.drho), f[0]);
+#pragma unroll
+    for (int p = 1; p <= 4; ++p) {
+        const float w = float(WD(p));
+        const L eu = eu_pair<L>(p, u, v);
+        o.q[p] = lfma(lbc<L>(4.5f), lmul(eu, eu), m15u2);
+        // (h_p + h_opp) - 2 w (drho + rho q),  (h_p - h_opp) - 2 w rho 3 e.u
+        o.dS[p] = lfma(lbc<L>(-2.0f * w), lfma(r, o.q[p], m.drho), ladd(f[p], f[p + 4]));
+        o.dD[p] = lfma(lbc<L>(-6.0f * w), lmul(r, eu), lsub(f[p], f[p + 4]));
+    }
+    // pi_neq (solver.rs:1096-1106) from the symmetric parts.
+    const L s34 = ladd(o.dS[3], o.dS[4]);
+    const L pxx = ladd(o.dS[1], s34), pyy = ladd(o.dS[2], s34), pxy = lsub(o.dS[3], o.dS[4]);
+    const L pi2 = lfma(pxx, pxx, lfma(lmul(lbc<L>(2.0f), pxy), pxy, lmul(pyy, pyy)));
+    // nu_t = Cs^2 |S|, |S| = sqrt(pi:pi) / (2 cs^2 tau rho) = sqrt(pi:pi) (1.5 / tau) / rho
+    const float kS = c.cs * c.cs * (1.5f * c.inv_tau_s) * p2(-EF);
+    o.nut = nut_ovr ? *nut_ovr : lmul(lmul(lsqrt(pi2), lbc<L>(kS)), m.inv_rho);
+    const L e = lfma(lbc<L>(3.0f), o.nut, lbc<L>(3.0f * c.nu));          // tau+ - 1/2
+    o.w1 = lrcp(ladd(lbc<L>(0.5f), e));                                     // 1/tau+
+    o.w2 = lmul(e, lrcp(lfma(lbc<L>(0.5f), e, lbc<L>(float(LAMBDA_TRT)))));  // 1/tau-, tau- = 1/2 + Lambda/e
+    o.k1 = lfma(lbc<L>(-0.5f), o.w1, lbc<L>(1.0f));
+    o.k2 = lfma(lbc<L>(-0.5f), o.w2, lbc<L>(1.0f));
+    return o;
+}
+
+// The f update with the Guo force fy = rho beta T: S+_p = w_p (-3 u_y +
+// 9 (c_p.u) c_py) fy, S-_p = w_p 3 c_py fy.  f in lane units (2^EF), temp
+// in g lane units (2^EG); returns fy unscaled.
+template <class L, int EF = 0, int EG = 0>
+__device__ __forceinline__ L collide_f_post_lane(L (&f)[Q], const CollF<L>& o, const Macro<L, true>& m,
+                                                 const StepScalars<float>& c, L temp) {
+    const L u = m.ux, v = m.uy;
+    const L fyv = lmul(lmul(m.rho, lbc<L>(c.beta * p2(-EG))), temp);
+    const L fys = EF == 0 ? fyv : lmul(fyv, lbc<L>(p2(EF)));
+    const L gp = lmul(o.k1, fys), gm = lmul(o.k2, fys);       // k+ fy, k- fy
+    const L hp = lmul(lbc<L>(-0.5f), o.w1), hm = lmul(lbc<L>(-0.5f), o.w2);
+    const L m3v = lmul(lbc<L>(-3.0f), v);
+    f[0] = lfma(lmul(lbc<L>(float(WD(0))), m3v), gp, lsub(f[0], lmul(o.w1, o.d0)));
+    const L sa = lmul(lbc<L>(float(WD(1))), m3v), sd = lmul(lbc<L>(float(WD(3))), m3v);
+    const L oa = lmul(lbc<L>(3.0f * float(WD(2))), gm), od = lmul(lbc<L>(3.0f * float(WD(3))), gm);
+#pragma unroll
+    for (int p = 1; p <= 4; ++p) {
+        const float w = float(WD(p));
+        const L w3v = p <= 2 ? sa : sd;
+        const L sp = p == 1 ? w3v : lfma(lbc<L>(9.0f * w), eu_pair<L>(p, u, v), w3v);
+        const L E = lfma(sp, gp, lmul(hp, o.dS[p]));
+        const L O = p == 1 ? lmul(hm, o.dD[p]) : lfma(hm, o.dD[p], p == 2 ? oa : od);
+        f[p] = ladd(f[p], ladd(E, O));
+        f[p + 4] = ladd(f[p + 4], lsub(E, O));
+    }
+    return fyv;
+}
+
+// BGK of g towards geq (quadratic, or linear in u when c.geq_order == 1).
+// q_p = 4.5 (c_p.u)^2 - 1.5 u^2 comes from the f collision (same u).  g and
+// temp in the same (lane) units: the update is linear in both.
+template <class L, bool LINEAR>
+__device__ __forceinline__ void collide_g_lane_o(L (&g)[Q], L temp, L u, L v, L om, const L (&q)[5]) {
+    const L one_m = lsub(lbc<L>(1.0f), om);
+    const L B = lmul(om, temp);
+    const L b0 = lmul(B, lbc<L>(float(WD(0))));
+    const L ba = lmul(B, lbc<L>(float(WD(1)))), bd = lmul(B, lbc<L>(float(WD(3))));
+    const L ba3 = lmul(lbc<L>(3.0f), ba), bd3 = lmul(lbc<L>(3.0f), bd);
+    const L u2 = lfma(u, u, lmul(v, v));
+    g[0] = lfma(one_m, g[0], LINEAR ? b0 : lfma(b0, lmul(lbc<L>(-1.5f), u2), b0));
+#pragma unroll
+    for (int p = 1; p <= 4; ++p) {
+        const L bw = p <= 2 ? ba : bd;
+        const L gS = LINEAR ? bw : lfma(bw, q[p], bw);
+        const L gA = lmul(p <= 2 ? ba3 : bd3, eu_pair<L>(p, u, v));
+        g[p] = lfma(one_m, g[p], ladd(gS, gA));
+        g[p + 4] = lfma(one_m, g[p + 4], lsub(gS, gA));
+    }
+}
+template <class L>
+__device__ __forceinline__ void collide_g_lane(L (&g)[Q], L temp, L u, L v, L nut, const L (&q)[5],
+                                               const StepScalars<float>& c, const L* at_ovr) {
+    const L at = at_ovr ? *at_ovr : lmul(nut, lbc<L>(c.inv_pr_t));
+    const L om = lrcp(lfma(lbc<L>(3.0f), at, lbc<L>(0.5f + 3.0f * c.alpha)));
+    if (c.geq_order == 1)
+        collide_g_lane_o<L, true>(g, temp, u, v, om, q);
+    else
+        collide_g_lane_o<L, false>(g, temp, u, v, om, q);
+}
 
 // nut_ovr: nu_t given per node (the dynamic subgrid model, solver.rs:1118-1121)
 // instead of Cs^2 |S|.
@@ -373,42 +607,7 @@ __device__ __forceinline__ CollF<A> collide_f_pre(const A (&f)[Q], const Macro<A
         o.k1 = 1.0 - 0.5 / tau_minus;
         o.k2 = 1.0 - 0.5 / tau_plus;
     } else {
-        // ---- FP32 on h_i = f_i - w_i, pairwise (i, opp(i)) form --------------
-        // For each pair p = (i, i+4), i = 1..4, split populations and
-        // equilibria into symmetric / antisymmetric parts: the TRT update
-        //   f_i += -a d_i - b d_opp + (1 - 1/2tau-) S-_i + (1 - 1/2tau+) S+_i
-        // with a = (w+ + w-)/2, b = (w+ - w-)/2 is exactly
-        //   f_p += E + O, f_opp += E - O,
-        //   E = -w+ (d_p + d_opp)/2 + k+ S+_p,  O = -w- (d_p - d_opp)/2 + k- S-_p,
-        // and pi_neq only needs the symmetric parts.  Same arithmetic as the
-        // reference up to rounding (FP32), a third of the operations.
-        const float u2 = u * u + v * v;
-        const float inv_r = m.inv_rho;
-        const float feq0 = float(WD(0)) * (m.drho - 1.5f * r * u2);
-        o.d0 = f[0] - feq0;
-#pragma unroll
-        for (int p = 1; p <= 4; ++p) {
-            const float cx = CX(p), cy = CY(p);
-            const float eu = cx * u + cy * v;
-            const float feS = float(WD(p)) * (m.drho + r * (4.5f * eu * eu - 1.5f * u2));
-            const float feA = float(WD(p)) * (r * 3.0f * eu);
-            o.dS[p] = (f[p] + f[p + 4]) - 2.0f * feS;
-            o.dD[p] = (f[p] - f[p + 4]) - 2.0f * feA;
-        }
-        // pi_neq (solver.rs:1096-1106) from the symmetric parts.
-        const float pxx = o.dS[1] + o.dS[3] + o.dS[4];
-        const float pxy = o.dS[3] - o.dS[4];
-        const float pyy = o.dS[2] + o.dS[3] + o.dS[4];
-        const float pi2 = pxx * pxx + 2.0f * pxy * pxy + pyy * pyy;
-        // |S| = sqrt(pi:pi) / (2 cs^2 tau rho) = sqrt(pi:pi) * (1.5 / tau) / rho
-        const float s_mag = __fsqrt_rn(pi2) * (1.5f * c.inv_tau_s) * inv_r;
-        const float nut = nut_ovr ? float(*nut_ovr) : c.cs * c.cs * s_mag;
-        o.nut = nut;
-        const float e = 3.0f * (c.nu + nut);             // tau+ - 1/2
-        o.w1 = __fdividef(1.0f, 0.5f + e);                // 1/tau+
-        o.w2 = __fdividef(e, 0.5f * e + float(LAMBDA_TRT));  // 1/tau-, tau- = 1/2 + Lambda/e
-        o.k1 = 1.0f - 0.5f * o.w1;
-        o.k2 = 1.0f - 0.5f * o.w2;
+        o = collide_f_pre_lane<A>(f, m, c, nut_ovr);
     }
     return o;
 }
@@ -434,20 +633,7 @@ __device__ __forceinline__ A collide_f_post(A (&f)[Q], const CollF<A>& o, const 
         }
         return fyv;
     } else {
-        const float fyv = r * c.beta * temp;
-        const float om_p = o.w1, om_m = o.w2, k_p = o.k1, k_m = o.k2;
-        // Guo source: S+_p = w_p (-3 u_y + 9 (e.u) c_y) fy, S-_p = w_p 3 c_y fy.
-        f[0] = f[0] - om_p * o.d0 + k_p * float(WD(0)) * (-3.0f * v) * fyv;
-#pragma unroll
-        for (int p = 1; p <= 4; ++p) {
-            const float cx = CX(p), cy = CY(p);
-            const float eu = cx * u + cy * v;
-            const float E = -0.5f * om_p * o.dS[p] + k_p * float(WD(p)) * (-3.0f * v + 9.0f * eu * cy) * fyv;
-            const float O = -0.5f * om_m * o.dD[p] + k_m * float(WD(p)) * (3.0f * cy) * fyv;
-            f[p] = f[p] + (E + O);
-            f[p + 4] = f[p + 4] + (E - O);
-        }
-        return fyv;
+        return collide_f_post_lane<A>(f, o, m, c, temp);
     }
 }
 
@@ -468,22 +654,14 @@ __device__ __forceinline__ void collide_g(A (&g)[Q], A temp, A u, A v, A nut, co
 #pragma unroll
         for (int i = 0; i < Q; ++i) g[i] = g[i] + (-a_g * d_g[i] - b_g * d_g[OPP(i)]);
     } else {
-        const float u2 = u * u + v * v;
-        const float alpha_t = at_ovr ? float(*at_ovr) : nut * c.inv_pr_t;
-        const float om_g = __fdividef(1.0f, 0.5f + 3.0f * (c.alpha + alpha_t));  // BGK g
-        // g: BGK towards geq (quadratic or linear in u).
-        const float one_m = 1.0f - om_g;
-        const float q2 = c.geq_order == 1 ? 0.0f : 1.0f;
-        g[0] = one_m * g[0] + om_g * float(WD(0)) * temp * (1.0f - q2 * 1.5f * u2);
+        A q[5];
+        const A m15u2 = lmul(lbc<A>(-1.5f), lfma(u, u, lmul(v, v)));
 #pragma unroll
         for (int p = 1; p <= 4; ++p) {
-            const float cx = CX(p), cy = CY(p);
-            const float eu = cx * u + cy * v;
-            const float gS = om_g * float(WD(p)) * temp * (1.0f + q2 * (4.5f * eu * eu - 1.5f * u2));
-            const float gA = om_g * float(WD(p)) * temp * (3.0f * eu);
-            g[p] = one_m * g[p] + (gS + gA);
-            g[p + 4] = one_m * g[p + 4] + (gS - gA);
+            const A eu = eu_pair<A>(p, u, v);
+            q[p] = lfma(lbc<A>(4.5f), lmul(eu, eu), m15u2);
         }
+        collide_g_lane<A>(g, temp, u, v, nut, q, c, at_ovr);
     }
 }
 
@@ -501,7 +679,21 @@ __device__ __forceinline__ void collide_node(A (&f)[Q], A (&g)[Q], const Macro<A
     const CollF<A> o = collide_f_pre<A, SHIFT>(f, m, c, nut_ovr);
     nut_out = o.nut;
     fy_out = collide_f_post<A, SHIFT>(f, o, m, c, m.t);
-    collide_g<A, SHIFT>(g, m.t, m.ux, m.uy, o.nut, c, at_ovr);
+    if constexpr (SHIFT)
+        collide_g_lane<A>(g, m.t, m.ux, m.uy, o.nut, o.q, c, at_ovr);
+    else
+        collide_g<A, SHIFT>(g, m.t, m.ux, m.uy, o.nut, c, at_ovr);
+}
+
+// The same collision on a lane type and in lane units (f scaled by 2^EF,
+// g and m.t by 2^EG, m.drho by 2^EF).
+template <class L, int EF, int EG>
+__device__ __forceinline__ void collide_node_lane(L (&f)[Q], L (&g)[Q], const Macro<L, true>& m,
+                                                  const StepScalars<float>& c, L& fy_out, L& nut_out) {
+    const CollF<L> o = collide_f_pre_lane<L, EF>(f, m, c, nullptr);
+    nut_out = o.nut;
+    fy_out = collide_f_post_lane<L, EF, EG>(f, o, m, c, m.t);
+    collide_g_lane<L>(g, m.t, m.ux, m.uy, o.nut, o.q, c, nullptr);
 }
 
 // Wall-node equilibrium of g (apply_thermal_boundary_conditions,

@@ -116,7 +116,8 @@ __device__ __forceinline__ typename Fmt<St>::A tile_at(const St* __restrict__ S,
     return Fmt<St>::load(S[(q * BY + row) * TILE_BX + col], q);
 }
 
-// pull_f / pull_g (kernels.cuh) with the sources taken from the stage.
+// pull_f / pull_g (kernels.cuh) with the sources taken from the stage, in
+// lane units (Fmt::lload).
 template <class St, int BY>
 __device__ __forceinline__ void pull_tile(const St* __restrict__ S, const Geom& G, int ix, int iy, int row, int col,
                                           const StepScalars<typename Fmt<St>::A>& c, typename Fmt<St>::A (&f)[Q],
@@ -128,17 +129,17 @@ __device__ __forceinline__ void pull_tile(const St* __restrict__ S, const Geom& 
         const int cx = CX(i), cy = CY(i);
         const bool ok = (cx > 0 ? xm : (cx < 0 ? xp : true)) && (cy > 0 ? ym : (cy < 0 ? yp : true));
         const int off = ok ? (i * BY + row - cy) * TILE_BX + col - cx : (OPP(i) * BY + row) * TILE_BX + col;
-        f[i] = Fmt<St>::load(S[off], i);
+        f[i] = Fmt<St>::lload(S[off], i);
     }
     const int gy = iy == 0 ? 1 : (iy == G.ny - 1 ? G.ny - 2 : iy);
     const int grow = row + (gy - iy);
     const bool wall_col = (ix == 0) || (ix == G.nx - 1);
-    const A tw = ix == 0 ? c.t_hot[gy] : c.t_cold;
+    const A tw = (ix == 0 ? c.t_hot[gy] : c.t_cold) * p2(Fmt<St>::EG);
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
         const int off = wall_col ? ((Q + i) * BY + row) * TILE_BX + col
                                  : ((Q + i) * BY + grow - CY(i)) * TILE_BX + col - CX(i);
-        const A v = Fmt<St>::load(S[off], Q + i);
+        const A v = Fmt<St>::lload(S[off], Q + i);
         g[i] = wall_col ? geq_rest<A>(i, tw, c.geq_order) : v;
     }
 }

@@ -256,7 +256,9 @@ typedef struct cav_batch_tuning {
     int32_t kernel;        /* 0: persistent, one thread per node from global
                               memory; 1, 2: TMA-staged shared-memory tiles in
                               shape 1 or 2 (taller); 3: one CTA per 32 x 4 item,
-                              one thread per node (default)                      */
+                              one thread per node; 4: the same items, two nodes
+                              per thread on packed FP32x2 arithmetic (default;
+                              FP64 batches run it as 3)                          */
 } cav_batch_tuning;
 int cav_batch_create(const cav_params* params, int32_t n, cav_batch** out);
 int cav_batch_destroy(cav_batch* b);

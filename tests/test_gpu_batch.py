@@ -43,7 +43,8 @@ def test_batch_is_bitwise_equal_to_single_cavities(precision):
 @pytest.mark.parametrize("precision", ["f64", "f32", "f16sr", "bf16", "f16gsr"])
 def test_batch_tuning_does_not_change_results(precision):
     """Tile heights, grid sizes and the kernel (persistent or one CTA per item
-    from global memory, TMA-staged shared-memory tiles) change no bit."""
+    from global memory, TMA-staged shared-memory tiles, two nodes per thread
+    on packed FP32x2 lanes) change no bit."""
     a = CavityBatch(MIXED, precision=precision)
     b = CavityBatch(MIXED, precision=precision)
     a.set_tuning(3, 2, kernel=0)
@@ -53,7 +54,9 @@ def test_batch_tuning_does_not_change_results(precision):
     b.set_tuning(5, 7, kernel=3)
     b.step(20)
     b.set_tuning(5, 1, kernel=2)
-    b.step(30)
+    b.step(15)
+    b.set_tuning(5, 1, kernel=4)
+    b.step(15)
     for i in range(len(MIXED)):
         fa, fb = a.fields(i), b.fields(i)
         for k in fa:
@@ -68,7 +71,7 @@ def test_autotune_picks_a_candidate_and_leaves_the_state_alone():
     b.step(10)
     ref.step(10)
     t = b.autotune(trial_steps=16)
-    assert t["kernel"] in (0, 1, 2, 3)
+    assert t["kernel"] in (0, 1, 2, 3, 4)
     if t["kernel"] == 0:
         assert t["rows_per_item"] in (2, 4, 8, 16, 32) and t["ctas_per_sm"] in (4, 8, 12, 16)
     elif t["kernel"] in (1, 2):
