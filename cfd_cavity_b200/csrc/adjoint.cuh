@@ -25,6 +25,8 @@
 
 namespace cav {
 
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // P-buffer: adjoints of the pulled inputs of every node, 19 planes of type A
 // in the population geometry: f 0..8, g 9..17, previous Guo force 18.
 constexpr int APLANES = 19;
@@ -103,7 +105,8 @@ __global__ void __launch_bounds__(128) k_adj_step(const St* __restrict__ X, cons
                                                   double* __restrict__ acc_theta, Geom G,
                                                   const StepScalars<typename Fmt<St>::A>* __restrict__ table, int S,
                                                   const long long* step_dev, long long j,
-                                                  AdjObj<typename Fmt<St>::A> obj) {
+                                                  AdjObj<typename Fmt<St>::A> obj, const St* __restrict__ Xpre,
+                                                  const typename Fmt<St>::A* __restrict__ Xfy_pre) {
     using A = typename Fmt<St>::A;
     pdl_wait();
     pdl_trigger();
@@ -115,9 +118,21 @@ __global__ void __launch_bounds__(128) k_adj_step(const St* __restrict__ X, cons
     const int W = G.pitch, Pp = int(G.plane);
     const int k = iy * W + ix;
     const int nx = G.nx, ny = G.ny;
+    // The next kernel of the sweep reads the previous state of the segment
+    // (recomputed earlier, usually evicted to HBM): bring this node's part
+    // of it into L2 now, so that its loads are L2 hits.
+    if (Xpre) {
+#pragma unroll
+        for (int q = 0; q < NPLANES; ++q) prefetch_l2(Xpre + (q * Pp + k));
+        prefetch_l2(Xfy_pre + k);
+    }
     // 1. adjoint of this node's outputs X_{s+1}(x), gathered from its readers.
     // Branch-free: every load reads a valid address and the unused ones are
     // discarded by selects, so all of a node's loads are in flight together.
+    // Rows 1 / ny-2 were copied to the wall rows 0 / ny-1, so their readers'
+    // adjoints add up; only rows within two of a wall read those (a row of a
+    // block is one warp, so the branch is uniform).
+    const bool near_wall = iy <= 2 || iy >= ny - 3;
     A af[Q], ag[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
@@ -126,12 +141,18 @@ __global__ void __launch_bounds__(128) k_adj_step(const St* __restrict__ X, cons
         const int kr = in ? ry * W + rx : k;
         af[q] = Pin[(in ? q : OPP(q)) * Pp + kr];
         const bool gin = in && rx >= 1 && rx <= nx - 2 && ry >= 1 && ry <= ny - 2;
-        const A v0 = Pin[(Q + q) * Pp + kr];
-        // rows 1 / ny-2 were copied to the wall rows 0 / ny-1: their readers add up
-        const int kw = ry == 1 ? rx : (ry == ny - 2 ? (ny - 1) * W + rx : kr);
-        const A vw = Pin[(Q + q) * Pp + (gin ? kw : kr)];
-        const bool wrow = gin && (ry == 1 || ry == ny - 2);
-        ag[q] = gin ? (wrow ? v0 + vw : v0) : A(0.0);
+        ag[q] = gin ? Pin[(Q + q) * Pp + kr] : A(0.0);
+    }
+    if (near_wall) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int rx = ix + CX(q), ry = iy + CY(q);
+            const bool gin = rx >= 1 && rx <= nx - 2 && ry >= 1 && ry <= ny - 2;
+            if (gin && (ry == 1 || ry == ny - 2)) {
+                const int kw = ry == 1 ? rx : (ny - 1) * W + rx;
+                ag[q] = ag[q] + Pin[(Q + q) * Pp + kw];
+            }
+        }
     }
     const A afy = Pin[18 * Pp + k];
     // 2. recompute the node's pulled inputs from X_s.

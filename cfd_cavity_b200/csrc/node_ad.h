@@ -44,6 +44,18 @@ template <class T>
 __host__ __device__ __forceinline__ T sqrt_(T x) {
     return sqrt(x);
 }
+// FP32 on the device: the special-function unit's square root, as the FP32
+// forward step uses.
+template <>
+__host__ __device__ __forceinline__ float sqrt_<float>(float x) {
+#ifdef __CUDA_ARCH__
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+#else
+    return sqrtf(x);
+#endif
+}
 
 // Division; FP32 on the device uses the fast approximate division (2 ulp),
 // as the FP32 forward step does.
