@@ -268,18 +268,23 @@ __device__ __forceinline__ void fused_pair(const St* __restrict__ src, St* __res
     static_assert(Fmt<St>::SHIFT, "the two-node lanes carry the FP32 arithmetic");
     constexpr int EF = Fmt<St>::EF, EG = Fmt<St>::EG;
     const int iy1 = hi ? iy + 1 : iy;
+    // f first: rho, u and the f collision's coefficients need no g, so the
+    // g populations are pulled only once those are formed (fewer values
+    // live at once: more resident warps)
     float fa[Q], ga[Q], fb[Q], gb[Q];
-    pull_node<St, true>(src, G, ix, iy, c, fa, ga);
-    pull_node<St, true>(src, G, ix, iy1, c, fb, gb);
+    pull_f<St, true>(src, G, ix, iy, fa);
+    pull_f<St, true>(src, G, ix, iy1, fb);
     float2 f[Q], g[Q];
 #pragma unroll
-    for (int i = 0; i < Q; ++i) {
-        f[i] = make_float2(fa[i], fb[i]);
-        g[i] = make_float2(ga[i], gb[i]);
-    }
+    for (int i = 0; i < Q; ++i) f[i] = make_float2(fa[i], fb[i]);
     const int k0 = iy * G.pitch + ix, k1 = iy1 * G.pitch + ix;
     Macro<float2, true> m = macro_f_lane<float2, EF>(f, make_float2(fy[k0], fy[k1]),
                                                      Mask2{is_wall(G, ix, iy), is_wall(G, ix, iy1)});
+    const CollF<float2> o = collide_f_pre_lane<float2, EF>(f, m, c, nullptr);
+    pull_g<St, true>(src, G, ix, iy, c, ga);
+    pull_g<St, true>(src, G, ix, iy1, c, gb);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) g[i] = make_float2(ga[i], gb[i]);
     m.t = sum_g<float2>(g);
     if (ACC_NU) {
         const float ta = m.t.x * p2(-EG), tb = m.t.y * p2(-EG);
@@ -292,9 +297,7 @@ __device__ __forceinline__ void fused_pair(const St* __restrict__ src, St* __res
             if (hi) acc_cold[iy1] += fabs(double(tb) - double(gather_t<St>(src, G, G.nx - 3, iy1, c)));
         }
     }
-    // the collision in the order that frees registers soonest: the f
-    // coefficients, then g (collided and stored), then f
-    const CollF<float2> o = collide_f_pre_lane<float2, EF>(f, m, c, nullptr);
+    // then g (collided and stored), then the f update
     collide_g_lane<float2>(g, m.t, m.ux, m.uy, o.nut, o.q, c, nullptr);
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
