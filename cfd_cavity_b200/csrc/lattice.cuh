@@ -70,7 +70,7 @@ struct Fmt;
 template <>
 struct Fmt<double> {
     using A = double;
-    static constexpr bool SHIFT = false, SR = false;
+    static constexpr bool SHIFT = false, SR = false, HW_SR = false;
     static constexpr int EF = 0, EG = 0;
     __host__ __device__ static A load(double v, int) { return v; }
     __host__ __device__ static double store(A v, int, uint32_t) { return v; }
@@ -80,7 +80,7 @@ struct Fmt<double> {
 template <>
 struct Fmt<float> {
     using A = float;
-    static constexpr bool SHIFT = true, SR = false;
+    static constexpr bool SHIFT = true, SR = false, HW_SR = false;
     static constexpr int EF = 0, EG = 0;
     __host__ __device__ static A load(float v, int) { return v; }
     __host__ __device__ static float store(A v, int, uint32_t) { return v; }
@@ -120,6 +120,20 @@ __host__ __device__ __forceinline__ unsigned short h16_enc(float s, bool sr, uin
 __host__ __device__ __forceinline__ unsigned short h16_store(float x, bool sr, uint32_t r) {
     return h16_enc(x * H_SCALE, sr, r);
 }
+#ifdef __CUDACC__
+// Two h16_enc stochastic roundings in one instruction (cvt.rs.f16x2.f32):
+// the hardware adds the low 13 bits of rbits[31:16] (for a) and of
+// rbits[15:0] (for b) below binary16's last mantissa bit and truncates (the
+// layout checked on a B200 with an in-bounds probe).  With rbits = r >> 3
+// those are r's bits 31..19 and 15..3, the bits h16_enc takes from the
+// draws r & 0xffff0000 and r << 16: the same results for normal binary16
+// values.  Returns (a << 16) | b.
+__device__ __forceinline__ uint32_t h16x2_enc_sr(float a, float b, uint32_t r) {
+    uint32_t d;
+    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(a), "f"(b), "r"(r >> 3));
+    return d;
+}
+#endif
 
 __host__ __device__ __forceinline__ float bf16_load(unsigned short bits) {
     uint32_t u = uint32_t(bits) << 16;
@@ -173,6 +187,9 @@ struct Fmt<P16<KIND, SRND>> {
     using A = float;
     using St = P16<KIND, SRND>;
     static constexpr bool SHIFT = true, SR = SRND;
+    // every plane binary16 with stochastic rounding: pairs of planes are
+    // rounded by one cvt.rs (h16x2_enc_sr)
+    static constexpr bool HW_SR = SRND && KIND == K_HALF;
     static constexpr int EF = KIND == K_BF16 ? 0 : 15, EG = KIND == K_HALF ? 15 : 0;
     // lane units: binary16 planes undecoded by the 2^15 (see EF / EG)
     __host__ __device__ static A lload(St v, int q) {
