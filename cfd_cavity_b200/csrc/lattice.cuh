@@ -126,8 +126,11 @@ __host__ __device__ __forceinline__ unsigned short h16_store(float x, bool sr, u
 // rbits[15:0] (for b) below binary16's last mantissa bit and truncates (the
 // layout checked on a B200 with an in-bounds probe).  With rbits = r >> 3
 // those are r's bits 31..19 and 15..3, the bits h16_enc takes from the
-// draws r & 0xffff0000 and r << 16: the same results for normal binary16
-// values.  Returns (a << 16) | b.
+// draws r & 0xffff0000 and r << 16.  Checked against h16_enc on 2^21 random
+// values: the same bits for normal binary16 results (33 differences, all at
+// the overflow edge above 65504); results in the subnormal range differ,
+// where the hardware dithers at the subnormal's last bit (unbiased) and the
+// 13-bit software dither does not.  Returns (a << 16) | b.
 __device__ __forceinline__ uint32_t h16x2_enc_sr(float a, float b, uint32_t r) {
     uint32_t d;
     asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(a), "f"(b), "r"(r >> 3));
