@@ -41,10 +41,10 @@ __device__ __forceinline__ void store_node(St* __restrict__ dst, const Geom& G, 
         // pairs of planes (q, q + 1) from one draw: the bits of the path below
         const long long step = c.step_dev ? *c.step_dev + c.step : c.step;
         NodeRng rng(c.sr_seed, step, (long long)iy * G.nx + ix);
-        const float sc = LANE ? 1.0f : H_SCALE;
+        const float sc = LANE ? 1.0f : p2(Fmt<St>::EF);  // binary16: 2^15, bfloat16: 1
 #pragma unroll
         for (int q = 0; q < NPLANES; q += 2) {
-            const uint32_t d = h16x2_enc_sr((q < Q ? f[q] : g[q - Q]) * sc, (q + 1 < Q ? f[q + 1] : g[q + 1 - Q]) * sc,
+            const uint32_t d = Fmt<St>::enc2_sr((q < Q ? f[q] : g[q - Q]) * sc, (q + 1 < Q ? f[q + 1] : g[q + 1 - Q]) * sc,
                                             rng.next());
             dst[q * P + k].bits = (unsigned short)(d >> 16);
             dst[(q + 1) * P + k].bits = (unsigned short)(d & 0xffffu);
@@ -85,17 +85,17 @@ __device__ __forceinline__ void store_planes(St* __restrict__ dst, const Geom& G
         for (int j = 0; j < Q0 / 2; ++j) rng.next();  // the draws of planes 0..Q0-1
         int q = Q0;
         if (Q0 & 1) {  // plane Q0 is the low half of its draw
-            dst[q * P + k].bits = (unsigned short)(h16x2_enc_sr(0.0f, v[0], rng.next()) & 0xffffu);
+            dst[q * P + k].bits = (unsigned short)(Fmt<St>::enc2_sr(0.0f, v[0], rng.next()) & 0xffffu);
             ++q;
         }
 #pragma unroll
         for (; q + 1 < Q0 + Q; q += 2) {
-            const uint32_t d = h16x2_enc_sr(v[q - Q0], v[q + 1 - Q0], rng.next());
+            const uint32_t d = Fmt<St>::enc2_sr(v[q - Q0], v[q + 1 - Q0], rng.next());
             dst[q * P + k].bits = (unsigned short)(d >> 16);
             dst[(q + 1) * P + k].bits = (unsigned short)(d & 0xffffu);
         }
         if (q < Q0 + Q)  // the last plane is the high half of its draw
-            dst[q * P + k].bits = (unsigned short)(h16x2_enc_sr(v[q - Q0], 0.0f, rng.next()) >> 16);
+            dst[q * P + k].bits = (unsigned short)(Fmt<St>::enc2_sr(v[q - Q0], 0.0f, rng.next()) >> 16);
     } else if constexpr (Fmt<St>::SR) {
         const long long step = c.step_dev ? *c.step_dev + c.step : c.step;
         NodeRng rng(c.sr_seed, step, (long long)iy * G.nx + ix);

@@ -151,6 +151,17 @@ __host__ __device__ __forceinline__ unsigned short bf16_store(float x, bool sr, 
     if (sr) return (unsigned short)((u + (r >> 16)) >> 16);
     return (unsigned short)((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);        // nearest, ties to even
 }
+#ifdef __CUDACC__
+// Two bf16_store stochastic roundings in one instruction
+// (cvt.rs.bf16x2.f32): r[31:16] dithers a, r[15:0] dithers b, the bits
+// bf16_store takes from the draws r & 0xffff0000 and r << 16.  Returns
+// (a << 16) | b.
+__device__ __forceinline__ uint32_t bf16x2_enc_sr(float a, float b, uint32_t r) {
+    uint32_t d;
+    asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(a), "f"(b), "r"(r));
+    return d;
+}
+#endif
 
 // 16-bit fixed point of g_i with a power-of-two scale per direction class:
 // 2^16 on the rest population (|g_0| <= 4/9 |T| < 0.5), 2^17 on the axes
@@ -190,9 +201,17 @@ struct Fmt<P16<KIND, SRND>> {
     using A = float;
     using St = P16<KIND, SRND>;
     static constexpr bool SHIFT = true, SR = SRND;
-    // every plane binary16 with stochastic rounding: pairs of planes are
-    // rounded by one cvt.rs (h16x2_enc_sr)
-    static constexpr bool HW_SR = SRND && KIND == K_HALF;
+    // every plane binary16 (bfloat16) with stochastic rounding: pairs of
+    // planes are rounded by one cvt.rs (enc2_sr)
+    static constexpr bool HW_SR = SRND && (KIND == K_HALF || KIND == K_BF16);
+#ifdef __CUDACC__
+    __device__ static uint32_t enc2_sr(float a, float b, uint32_t r) {
+        if constexpr (KIND == K_BF16)
+            return bf16x2_enc_sr(a, b, r);
+        else
+            return h16x2_enc_sr(a, b, r);
+    }
+#endif
     static constexpr int EF = KIND == K_BF16 ? 0 : 15, EG = KIND == K_HALF ? 15 : 0;
     // lane units: binary16 planes undecoded by the 2^15 (see EF / EG)
     __host__ __device__ static A lload(St v, int q) {

@@ -1,13 +1,14 @@
-// The hardware stochastic rounding of binary16 pairs (h16x2_enc_sr, cvt.rs)
-// against the software h16_enc on 2^21 deterministic pseudo-random values
-// (magnitudes 2^-20 .. 2^16, both signs): prints the differences in the
-// normal and in the subnormal binary16 range.  Built and run by
+// The hardware stochastic rounding of binary16 and bfloat16 pairs
+// (h16x2_enc_sr, bf16x2_enc_sr: cvt.rs) against the software h16_enc /
+// bf16_store on 2^21 deterministic pseudo-random values (magnitudes
+// 2^-20 .. 2^16, both signs): prints the binary16 differences in the normal
+// and in the subnormal range, and the bfloat16 differences.  Built and run by
 // tests/test_gpu_sr.py.
 #include <cstdio>
 #include "lattice.cuh"
 using namespace cav;
 constexpr int N = 1 << 20;
-__global__ void k(unsigned* mism, unsigned* sub) {
+__global__ void k(unsigned* mism, unsigned* sub, unsigned* bmism) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     uint32_t s = mix32(uint32_t(i) * 2654435761u + 12345u);
@@ -21,13 +22,19 @@ __global__ void k(unsigned* mism, unsigned* sub) {
     const bool sa = fabsf(a) < 6.103515625e-05f, sb = fabsf(b) < 6.103515625e-05f;  // binary16 subnormal range
     if ((d >> 16) != ha) atomicAdd(sa ? sub : mism, 1u);
     if ((d & 0xffffu) != hb) atomicAdd(sb ? sub : mism, 1u);
+    const uint32_t db = bf16x2_enc_sr(a, b, r);
+    if ((db >> 16) != bf16_store(a, true, r & 0xffff0000u)) atomicAdd(bmism, 1u);
+    if ((db & 0xffffu) != bf16_store(b, true, r << 16)) atomicAdd(bmism, 1u);
 }
 int main() {
-    unsigned *m, *s, hm = 0, hs = 0;
-    cudaMalloc(&m, 4); cudaMalloc(&s, 4); cudaMemset(m, 0, 4); cudaMemset(s, 0, 4);
-    k<<<N / 256, 256>>>(m, s);
+    unsigned *m, *s, *bm, hm = 0, hs = 0, hb = 0;
+    cudaMalloc(&m, 4); cudaMalloc(&s, 4); cudaMalloc(&bm, 4);
+    cudaMemset(m, 0, 4); cudaMemset(s, 0, 4); cudaMemset(bm, 0, 4);
+    k<<<N / 256, 256>>>(m, s, bm);
     cudaError_t e = cudaDeviceSynchronize();
     cudaMemcpy(&hm, m, 4, cudaMemcpyDeviceToHost); cudaMemcpy(&hs, s, 4, cudaMemcpyDeviceToHost);
-    printf("err %d  mismatches (normal range) %u  (subnormal range) %u  of %d\n", int(e), hm, hs, 2 * N);
+    cudaMemcpy(&hb, bm, 4, cudaMemcpyDeviceToHost);
+    printf("err %d  mismatches (normal range) %u  (subnormal range) %u  of %d  bf16 %u\n", int(e), hm, hs, 2 * N,
+           hb);
     return e == cudaSuccess ? 0 : 1;
 }

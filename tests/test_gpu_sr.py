@@ -1,6 +1,7 @@
-"""The binary16 stochastic rounding of the 16-bit storage formats runs on the
-hardware's cvt.rs.f16x2.f32 for pairs of planes (h16x2_enc_sr), fed the
-bits that the software rounding h16_enc takes from the same draws.  A
+"""The binary16 and bfloat16 stochastic rounding of the 16-bit storage formats
+runs on the hardware's cvt.rs for pairs of planes (h16x2_enc_sr,
+bf16x2_enc_sr), fed the bits that the software roundings h16_enc /
+bf16_store take from the same draws.  bfloat16 must agree everywhere.  A
 native check (tests/native/sr_check.cu) converts 2^21 deterministic
 pseudo-random values both ways: the results must agree for normal binary16
 results (the only differences sit at the overflow edge above 65504); in the
@@ -29,6 +30,8 @@ def test_hardware_stochastic_rounding_matches_software_in_the_normal_range(tmp_p
                    check=True, capture_output=True, timeout=300)
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
-    m = re.search(r"err (\d+)\s+mismatches \(normal range\) (\d+)\s+\(subnormal range\) (\d+)", r.stdout)
+    m = re.search(r"err (\d+)\s+mismatches \(normal range\) (\d+)\s+\(subnormal range\) (\d+)\s+of \d+\s+"
+                  r"bf16 (\d+)", r.stdout)
     assert m and int(m.group(1)) == 0, r.stdout
     assert int(m.group(2)) <= 64, r.stdout  # overflow edge only (33 on a B200)
+    assert int(m.group(4)) == 0, r.stdout
