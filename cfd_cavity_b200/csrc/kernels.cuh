@@ -37,17 +37,31 @@ __device__ __forceinline__ void store_node(St* __restrict__ dst, const Geom& G, 
                                            const StepScalars<typename Fmt<St>::A>& c) {
     const int P = int(G.plane);
     const int k = iy * G.pitch + ix;
-    if constexpr (Fmt<St>::HW_SR) {
-        // pairs of planes (q, q + 1) from one draw: the bits of the path below
+    if constexpr (Fmt<St>::HW_SR_F) {
+        // pairs of planes (q, q + 1) from one draw, rounded by one cvt.rs
+        // where both are binary16 / bfloat16: the bits of the path below
         const long long step = c.step_dev ? *c.step_dev + c.step : c.step;
         NodeRng rng(c.sr_seed, step, (long long)iy * G.nx + ix);
-        const float sc = LANE ? 1.0f : p2(Fmt<St>::EF);  // binary16: 2^15, bfloat16: 1
+        const float sf = LANE ? 1.0f : p2(Fmt<St>::EF), sg = LANE ? 1.0f : p2(Fmt<St>::EG);
 #pragma unroll
         for (int q = 0; q < NPLANES; q += 2) {
-            const uint32_t d = Fmt<St>::enc2_sr((q < Q ? f[q] : g[q - Q]) * sc, (q + 1 < Q ? f[q + 1] : g[q + 1 - Q]) * sc,
-                                            rng.next());
-            dst[q * P + k].bits = (unsigned short)(d >> 16);
-            dst[(q + 1) * P + k].bits = (unsigned short)(d & 0xffffu);
+            const uint32_t r = rng.next();
+            const auto xa = q < Q ? f[q] : g[q - Q];
+            const auto xb = q + 1 < Q ? f[q + 1] : g[q + 1 - Q];
+            const bool ha = q < Q || Fmt<St>::HW_SR_G, hb = q + 1 < Q || Fmt<St>::HW_SR_G;
+            if (ha && hb) {
+                const uint32_t d = Fmt<St>::enc2_sr(xa * (q < Q ? sf : sg), xb * (q + 1 < Q ? sf : sg), r);
+                dst[q * P + k].bits = (unsigned short)(d >> 16);
+                dst[(q + 1) * P + k].bits = (unsigned short)(d & 0xffffu);
+            } else {
+                if (ha)
+                    dst[q * P + k].bits = (unsigned short)(Fmt<St>::enc2_sr(xa * sf, 0.0f, r) >> 16);
+                else
+                    dst[q * P + k] = LANE ? Fmt<St>::lstore_sr(xa, q, r & 0xffff0000u)
+                                          : Fmt<St>::store_sr(xa, q, r & 0xffff0000u);
+                dst[(q + 1) * P + k] = LANE ? Fmt<St>::lstore_sr(xb, q + 1, r << 16)
+                                            : Fmt<St>::store_sr(xb, q + 1, r << 16);
+            }
         }
     } else if constexpr (Fmt<St>::SR) {
         const long long step = c.step_dev ? *c.step_dev + c.step : c.step;
@@ -78,7 +92,7 @@ __device__ __forceinline__ void store_planes(St* __restrict__ dst, const Geom& G
                                              const StepScalars<typename Fmt<St>::A>& c) {
     const int P = int(G.plane);
     const int k = iy * G.pitch + ix;
-    if constexpr (Fmt<St>::HW_SR) {
+    if constexpr (Q0 == 0 ? Fmt<St>::HW_SR_F : Fmt<St>::HW_SR_G) {
         const long long step = c.step_dev ? *c.step_dev + c.step : c.step;
         NodeRng rng(c.sr_seed, step, (long long)iy * G.nx + ix);
 #pragma unroll

@@ -70,7 +70,7 @@ struct Fmt;
 template <>
 struct Fmt<double> {
     using A = double;
-    static constexpr bool SHIFT = false, SR = false, HW_SR = false;
+    static constexpr bool SHIFT = false, SR = false, HW_SR_F = false, HW_SR_G = false;
     static constexpr int EF = 0, EG = 0;
     __host__ __device__ static A load(double v, int) { return v; }
     __host__ __device__ static double store(A v, int, uint32_t) { return v; }
@@ -80,7 +80,7 @@ struct Fmt<double> {
 template <>
 struct Fmt<float> {
     using A = float;
-    static constexpr bool SHIFT = true, SR = false, HW_SR = false;
+    static constexpr bool SHIFT = true, SR = false, HW_SR_F = false, HW_SR_G = false;
     static constexpr int EF = 0, EG = 0;
     __host__ __device__ static A load(float v, int) { return v; }
     __host__ __device__ static float store(A v, int, uint32_t) { return v; }
@@ -201,9 +201,10 @@ struct Fmt<P16<KIND, SRND>> {
     using A = float;
     using St = P16<KIND, SRND>;
     static constexpr bool SHIFT = true, SR = SRND;
-    // every plane binary16 (bfloat16) with stochastic rounding: pairs of
-    // planes are rounded by one cvt.rs (enc2_sr)
-    static constexpr bool HW_SR = SRND && (KIND == K_HALF || KIND == K_BF16);
+    // stochastic rounding of the binary16 (bfloat16) planes by the hardware,
+    // two planes per cvt.rs (enc2_sr): the f planes of every 16-bit format,
+    // the g planes unless they are fixed point
+    static constexpr bool HW_SR_F = SRND, HW_SR_G = SRND && KIND != K_MIX;
 #ifdef __CUDACC__
     __device__ static uint32_t enc2_sr(float a, float b, uint32_t r) {
         if constexpr (KIND == K_BF16)
