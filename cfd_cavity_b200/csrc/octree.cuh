@@ -238,7 +238,40 @@ template <class St, bool BACK = false>
 __device__ __forceinline__ void store_pops(St* __restrict__ dst, int n, int k, typename Fmt<St>::A (&f)[Q],
                                            typename Fmt<St>::A (&g)[Q], bool sr, uint32_t seed, long long key,
                                            long long node) {
-    if constexpr (Fmt<St>::SR) {
+    if constexpr (Fmt<St>::HW_SR_F) {
+        // pairs of binary16 / bfloat16 planes by one cvt.rs (enc2_sr), fed
+        // the bits the software rounding below takes from the same draw
+        if (sr) {
+            NodeRng rng(seed, key, node);
+            const float sf = p2(Fmt<St>::EF), sg = p2(Fmt<St>::EG);
+#pragma unroll
+            for (int q = 0; q < NPLANES; q += 2) {
+                const uint32_t r = rng.next();
+                typename Fmt<St>::A& xa = q < Q ? f[q] : g[q - Q];
+                typename Fmt<St>::A& xb = q + 1 < Q ? f[q + 1] : g[q + 1 - Q];
+                const bool ha = q < Q || Fmt<St>::HW_SR_G, hb = q + 1 < Q || Fmt<St>::HW_SR_G;
+                St va, vb;
+                if (ha && hb) {
+                    const uint32_t d = Fmt<St>::enc2_sr(xa * (q < Q ? sf : sg), xb * (q + 1 < Q ? sf : sg), r);
+                    va.bits = (unsigned short)(d >> 16);
+                    vb.bits = (unsigned short)(d & 0xffffu);
+                } else {
+                    if (ha)
+                        va.bits = (unsigned short)(Fmt<St>::enc2_sr(xa * sf, 0.0f, r) >> 16);
+                    else
+                        va = Fmt<St>::store_sr(xa, q, r & 0xffff0000u);
+                    vb = Fmt<St>::store_sr(xb, q + 1, r << 16);
+                }
+                dst[q * n + k] = va;
+                dst[(q + 1) * n + k] = vb;
+                if (BACK) {
+                    xa = Fmt<St>::load(va, q);
+                    xb = Fmt<St>::load(vb, q + 1);
+                }
+            }
+            return;
+        }
+    } else if constexpr (Fmt<St>::SR) {
         if (sr) {
             NodeRng rng(seed, key, node);
             uint32_t r = 0;
