@@ -67,10 +67,12 @@ __global__ void __launch_bounds__(BATCH_THREADS)
 // The same node body with one CTA per (cavity, 32-column x 4-row) item and
 // one node per thread (no persistent loop): the per-cavity pointers and
 // scalars are not kept live across items, so the kernel needs the
-// registers of k_fused, not of k_batch.
+// registers of k_fused, not of k_batch; capped at 56 for 9 resident CTAs
+// per SM (a word or three spilled to L1; on a B200 +3 % binary16, +15 %
+// bfloat16 with stochastic rounding against 64 registers and 8 CTAs).
 constexpr int NP_ROWS = BATCH_THREADS / 32;
 template <class St, bool WRITE_NUT>
-__global__ void __launch_bounds__(BATCH_THREADS)
+__global__ void __launch_bounds__(BATCH_THREADS, 9)
     k_batch_np(const BatchCav<St>* __restrict__ cavs, const BatchItem* __restrict__ items,
                const StepScalars<typename Fmt<St>::A>* __restrict__ table, int n_cav, long long step,
                const long long* __restrict__ step_dev) {
