@@ -163,7 +163,7 @@ def batched_sweep(precisions, dev, steps=300):
     return out
 
 
-def c2_nusselt_error(dev, precisions=("f32", "f16sr", "f16gsr", "bf16sr")):
+def c2_nusselt_error(dev, precisions=("f32", "f16sr", "f16", "f16gsr", "bf16sr")):
     """The accuracy half of the headline: configs[1] (128x512, Ra = 1e8,
     theta = 0 + 1e-4 noise) for 200 000 steps, the per-step hot / cold wall
     Nu (post.rs:68-111) averaged over steps 150 001-200 000 on the device,
@@ -523,21 +523,23 @@ def main():
 
     extras = {}
     if not args.no_extras and world == 1:  # single-GPU workloads: reported at N = 1
-        # FP32 storage on the same single cavity, same timing method
-        s32 = CavitySolver(NX, NY, RA, PHYS["pr"], PHYS["cs"], PHYS["pr_t"], PHYS["utarget"],
-                           PHYS["seed"], precision="f32", init_mode=L.CAV_INIT_ZERO, noise_amp=1e-4,
-                           device=dev)
-        st32 = torch.cuda.ExternalStream(s32.stream_handle(), device=dev)
-        s32.step(s32.info()["spin_up_steps"] + 64 + args.chunk)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(st32):
-            e0.record(st32)
-        s32.step(args.chunk * 3)
-        with torch.cuda.stream(st32):
-            e1.record(st32)
-        e1.synchronize()
-        extras["fp32_single_cavity_mlups"] = nodes * args.chunk * 3 / (e0.elapsed_time(e1) * 1e-3) / 1e6
-        s32.close()
+        # FP32 and round-to-nearest binary16 storage on the same single
+        # cavity, same timing method
+        for other, key in (("f32", "fp32_single_cavity_mlups"), ("f16", "f16_single_cavity_mlups")):
+            s32 = CavitySolver(NX, NY, RA, PHYS["pr"], PHYS["cs"], PHYS["pr_t"], PHYS["utarget"],
+                               PHYS["seed"], precision=other, init_mode=L.CAV_INIT_ZERO, noise_amp=1e-4,
+                               device=dev)
+            st32 = torch.cuda.ExternalStream(s32.stream_handle(), device=dev)
+            s32.step(s32.info()["spin_up_steps"] + 64 + args.chunk)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(st32):
+                e0.record(st32)
+            s32.step(args.chunk * 3)
+            with torch.cuda.stream(st32):
+                e1.record(st32)
+            e1.synchronize()
+            extras[key] = nodes * args.chunk * 3 / (e0.elapsed_time(e1) * 1e-3) / 1e6
+            s32.close()
         extras["c2_nusselt"] = c2_nusselt_error(dev)
         extras["batched_sweep"] = batched_sweep(["f32", "f16sr", "f16gsr", "bf16sr", "f16"], dev)
         extras["adjoint_c4"] = adjoint_c4(dev)
