@@ -45,6 +45,9 @@ BYTES_PER_NODE = {"f64": 304, "f32": 152, "f16": 80, "bf16": 80, "f16g": 80, "f1
                   "bf16sr": 80, "f16gsr": 80}
 PRECISION = "f16sr"
 L2_FLUSH_BYTES = 256 << 20
+# B200 HBM3e nominal bandwidth (the north star's "~8 TB/s peak"), reported
+# beside the measured copy peak
+SPEC_HBM_GBS = 8000.0
 
 
 def measured_peaks():
@@ -307,12 +310,12 @@ def octree_c5(dev, chain=(30_000, 30_000, 60_000), window=40_000, sample_every=1
     return out
 
 
-def batch_only(precision, steps, kernel):
+def batch_only(precision, steps, kernel, rows):
     """C3 batch timing alone (profiling runs): the 64-cavity sweep in one
-    storage format with a fixed tuning (tile height 16, 4 CTAs per SM for
-    the persistent global-memory kernel; the tile kernel's resident CTAs
-    for kernels 1 / 2; one CTA per item for kernels 3 / 4),
-    250 spin-up steps, then `steps` timed lattice steps."""
+    storage format with a fixed tuning (kernel `kernel`, `rows` rows per
+    tile or item; 4 CTAs per SM for the persistent global-memory kernel, 3
+    for the tile kernel), 250 spin-up steps, then `steps` timed lattice
+    steps."""
     import torch
 
     from cfd_cavity_b200 import CavityBatch, sweep_configs
@@ -320,7 +323,7 @@ def batch_only(precision, steps, kernel):
     cfg = sweep_configs(64)
     nodes = sum(c["nx"] * c["ny"] for c in cfg)
     bt = CavityBatch(cfg, precision=precision, device=0)
-    bt.set_tuning(16, 4 if kernel == 0 else 3, kernel=kernel)
+    bt.set_tuning(rows, 4 if kernel == 0 else 3, kernel=kernel)
     bt.step(250)
     st = torch.cuda.ExternalStream(bt.stream_handle(), device=0)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -332,7 +335,8 @@ def batch_only(precision, steps, kernel):
     e1.synchronize()
     bt.sync()
     ms = e0.elapsed_time(e1)
-    print(json.dumps({"workload": f"batched sweep 64 cavities {precision}", "kernel": kernel, "steps": steps,
+    print(json.dumps({"workload": f"batched sweep 64 cavities {precision}", "kernel": kernel, "rows": rows,
+                      "steps": steps,
                       "us_per_step": ms * 1e3 / steps, "mlups": nodes * steps / (ms * 1e-3) / 1e6}), flush=True)
     bt.close()
     return 0
@@ -431,13 +435,15 @@ def main():
     ap.add_argument("--batch-only", default="", metavar="PRECISION",
                     help="only time the 64-cavity batched sweep in PRECISION for --steps lattice steps "
                          "(profiling runs); --batch-kernel selects the kernel")
-    ap.add_argument("--batch-kernel", type=int, default=4, choices=[0, 1, 2, 3, 4])
+    ap.add_argument("--batch-kernel", type=int, default=5, choices=[0, 1, 2, 3, 4, 5])
+    ap.add_argument("--batch-rows", type=int, default=4,
+                    help="tile / item height of --batch-only (kernels 3 and 5: 1, 2, 4 or 8)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.octree_only:
         return octree_only(args.octree_only)
     if args.batch_only:
-        return batch_only(args.batch_only, args.steps, args.batch_kernel)
+        return batch_only(args.batch_only, args.steps, args.batch_kernel, args.batch_rows)
     world, rank, local, dist = dist_setup(args)
     if args.impl == "reference":
         rc = run_reference(args, world, rank, dist)
@@ -523,23 +529,35 @@ def main():
 
     extras = {}
     if not args.no_extras and world == 1:  # single-GPU workloads: reported at N = 1
+        def single_mlups(other, nx, ny, ra, n_steps):
+            """Device MLUPS of one cavity in storage `other`, steady-state
+            steps (same timing method as the headline)."""
+            s2 = CavitySolver(nx, ny, ra, PHYS["pr"], PHYS["cs"], PHYS["pr_t"], PHYS["utarget"],
+                              PHYS["seed"], precision=other, init_mode=L.CAV_INIT_ZERO, noise_amp=1e-4,
+                              device=dev)
+            st2 = torch.cuda.ExternalStream(s2.stream_handle(), device=dev)
+            s2.step(s2.info()["spin_up_steps"] + 64 + n_steps // 3)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(st2):
+                e0.record(st2)
+            s2.step(n_steps)
+            with torch.cuda.stream(st2):
+                e1.record(st2)
+            e1.synchronize()
+            s2.close()
+            return nx * ny * n_steps / (e0.elapsed_time(e1) * 1e-3) / 1e6
+
         # FP32 and round-to-nearest binary16 storage on the same single
         # cavity, same timing method
-        for other, key in (("f32", "fp32_single_cavity_mlups"), ("f16", "f16_single_cavity_mlups")):
-            s32 = CavitySolver(NX, NY, RA, PHYS["pr"], PHYS["cs"], PHYS["pr_t"], PHYS["utarget"],
-                               PHYS["seed"], precision=other, init_mode=L.CAV_INIT_ZERO, noise_amp=1e-4,
-                               device=dev)
-            st32 = torch.cuda.ExternalStream(s32.stream_handle(), device=dev)
-            s32.step(s32.info()["spin_up_steps"] + 64 + args.chunk)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            with torch.cuda.stream(st32):
-                e0.record(st32)
-            s32.step(args.chunk * 3)
-            with torch.cuda.stream(st32):
-                e1.record(st32)
-            e1.synchronize()
-            extras[key] = nodes * args.chunk * 3 / (e0.elapsed_time(e1) * 1e-3) / 1e6
-            s32.close()
+        extras["fp32_single_cavity_mlups"] = single_mlups("f32", NX, NY, RA, args.chunk * 3)
+        extras["f16_single_cavity_mlups"] = single_mlups("f16", NX, NY, RA, args.chunk * 3)
+        # like-for-like with the reference's FP64 arithmetic: the FP64 GPU
+        # path (bit-identical to the FP64 oracle) on configs[0] (64x256,
+        # Ra = 1e6) and on this workload
+        extras["fp64_single_cavity"] = {
+            "c1_64x256_ra1e6_mlups": single_mlups("f64", 64, 256, 1e6, 2000),
+            "c2_128x512_ra1e8_mlups": single_mlups("f64", NX, NY, RA, 2000),
+        }
         extras["c2_nusselt"] = c2_nusselt_error(dev)
         extras["batched_sweep"] = batched_sweep(["f32", "f16sr", "f16gsr", "bf16sr", "f16"], dev)
         extras["adjoint_c4"] = adjoint_c4(dev)
@@ -565,6 +583,7 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
+                         "peak_spec": SPEC_HBM_GBS, "frac_spec": achieved / SPEC_HBM_GBS,
                          "traffic": profile_traffic(prec),
                          "kernel": "k_fused", "algorithmic_bytes_per_node": bpn,
                          "avg_launch_us": kernel_us},

@@ -27,8 +27,9 @@ PRECISIONS = {"f64": CAV_PREC_F64, "f32": CAV_PREC_F32, "f16": CAV_PREC_F16, "bf
               "f16g": CAV_PREC_F16G, "f16sr": CAV_PREC_F16SR, "bf16sr": CAV_PREC_BF16SR,
               "f16gsr": CAV_PREC_F16GSR}
 CAV_INIT_LINEAR, CAV_INIT_ZERO = 0, 1
+CAV_STEP_NODE, CAV_STEP_PAIR = 0, 1
 (CAV_PHASE_COLLIDE, CAV_PHASE_STREAM, CAV_PHASE_BOUNCE_BACK, CAV_PHASE_THERMAL_BC,
- CAV_PHASE_MACRO, CAV_PHASE_NOSLIP, CAV_PHASE_FUSED_IDENTITY) = range(7)
+ CAV_PHASE_MACRO, CAV_PHASE_NOSLIP, CAV_PHASE_FUSED_IDENTITY, CAV_PHASE_CHANNEL) = range(8)
 
 _dp = ctypes.POINTER(ctypes.c_double)
 
@@ -160,6 +161,8 @@ def load(path: str | None = None):
         "cav_sync": (i32, [vp]),
         "cav_get_stream": (i32, [vp, ctypes.POINTER(vp)]),
         "cav_launch_count": (i32, [vp, ctypes.POINTER(i64)]),
+        "cav_set_step_kernel": (i32, [vp, i32]),
+        "cav_get_step_kernel": (i32, [vp, ctypes.POINTER(i32)]),
         "cav_set_dynamic_sgs": (i32, [vp, i32, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
         "cav_snapshot_write_fields": (i32, [ctypes.c_char_p, i64, i64, _dp, _dp, _dp, _dp]),
         "cav_snapshot_read_fields": (i32, [ctypes.c_char_p, ctypes.POINTER(i64), ctypes.POINTER(i64), _dp, _dp,

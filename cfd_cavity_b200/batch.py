@@ -125,23 +125,39 @@ class CavityBatch:
         self._ck(L.load().cav_batch_info(self._b, ctypes.byref(n), ctypes.byref(nodes), ctypes.byref(t)))
         return {"n_cavities": n.value, "total_nodes": nodes.value, "time_step": t.value}
 
+    @staticmethod
+    def _used(t):
+        """The kernel and the tuning fields it uses (cav_batch_tuning)."""
+        k = t.kernel
+        if k == 0:
+            return {"kernel": 0, "rows_per_item": t.rows_per_item, "ctas_per_sm": t.ctas_per_sm}
+        if k in (1, 2):
+            return {"kernel": k, "ctas_per_sm": t.ctas_per_sm}
+        return {"kernel": k, "rows_per_item": t.rows_per_item}
+
     def tuning(self):
+        """The current kernel and the tuning fields it uses."""
         t = L.CavBatchTuning()
         self._ck(L.load().cav_batch_get_tuning(self._b, ctypes.byref(t)))
-        return {"rows_per_item": t.rows_per_item, "ctas_per_sm": t.ctas_per_sm, "kernel": t.kernel}
+        return self._used(t)
 
-    def set_tuning(self, rows_per_item, ctas_per_sm, kernel=4):
+    def set_tuning(self, rows_per_item, ctas_per_sm, kernel=3):
         """kernel 0: the persistent global-memory kernel (rows_per_item,
         ctas_per_sm); 1 / 2: the TMA tile kernel in tile shape 1 or 2
-        (ctas_per_sm); 3: one CTA per 32 x 4 item; 4: the same items, two
-        nodes per thread on packed FP32x2 arithmetic (the default)."""
+        (ctas_per_sm); 3: one CTA per 32-column x rows_per_item item, one
+        node per thread (1, 2, 4 or 8 rows); 4: the same items, two rows per
+        thread on packed FP32x2 arithmetic (2, 4 or 8 rows); 5: one CTA per
+        64-column x rows_per_item item, two x-adjacent nodes per thread
+        (16-bit formats; 1, 2, 4 or 8 rows)."""
         t = L.CavBatchTuning(rows_per_item, ctas_per_sm, int(kernel))
         self._ck(L.load().cav_batch_set_tuning(self._b, ctypes.byref(t)))
 
     def autotune(self, trial_steps=64):
+        """Times every candidate kernel / parameter set three times on a twin
+        batch (median kept), applies the fastest; returns it as tuning()."""
         t = L.CavBatchTuning()
         self._ck(L.load().cav_batch_autotune(self._b, int(trial_steps), ctypes.byref(t)))
-        return {"rows_per_item": t.rows_per_item, "ctas_per_sm": t.ctas_per_sm, "kernel": t.kernel}
+        return self._used(t)
 
     def debug_stall_copies(self, on):
         """Test of the tile kernel's bounded waits: arm the barriers but issue

@@ -17,6 +17,7 @@
 
 #include "solver.cuh"
 #include "tile.cuh"
+#include "xpair.cuh"
 
 namespace cav {
 
@@ -64,15 +65,14 @@ __global__ void __launch_bounds__(BATCH_THREADS)
     }
 }
 
-// The same node body with one CTA per (cavity, 32-column x 4-row) item and
-// one node per thread (no persistent loop): the per-cavity pointers and
-// scalars are not kept live across items, so the kernel needs the
-// registers of k_fused, not of k_batch; capped at 56 for 9 resident CTAs
-// per SM (a word or three spilled to L1; on a B200 +3 % binary16, +15 %
+// The same node body with one CTA per (cavity, 32-column x rows) item, one
+// node per thread (no persistent loop): the per-cavity pointers and scalars
+// are not kept live across items, so the kernel needs the registers of
+// k_fused, not of k_batch; capped at 56 (with 128-thread CTAs, 9 resident
+// per SM; a word or three spilled to L1; on a B200 +3 % binary16, +15 %
 // bfloat16 with stochastic rounding against 64 registers and 8 CTAs).
-constexpr int NP_ROWS = BATCH_THREADS / 32;
 template <class St, bool WRITE_NUT>
-__global__ void __launch_bounds__(BATCH_THREADS, 9)
+__global__ void __maxnreg__(56)
     k_batch_np(const BatchCav<St>* __restrict__ cavs, const BatchItem* __restrict__ items,
                const StepScalars<typename Fmt<St>::A>* __restrict__ table, int n_cav, long long step,
                const long long* __restrict__ step_dev) {
@@ -95,12 +95,12 @@ __global__ void __launch_bounds__(BATCH_THREADS, 9)
 }
 
 // k_batch_np with two rows per thread (fused_pair: the arithmetic of both
-// nodes on packed FP32x2 lanes): NP_ROWS / 2 warps per item.  FP32-arithmetic
-// formats only.  Register budget for 10 resident CTAs per SM (96 registers,
-// a few words spilled to L1): more warps to hide the loads' latency beat the
+// nodes on packed FP32x2 lanes): rows / 2 warps per item.  FP32-arithmetic
+// formats only.  Register budget 96 (10 resident 64-thread CTAs per SM, a
+// few words spilled to L1): more warps to hide the loads' latency beat the
 // spill traffic on a B200.
 template <class St, bool WRITE_NUT>
-__global__ void __launch_bounds__(BATCH_THREADS / 2, 10)
+__global__ void __maxnreg__(96)
     k_batch_np2(const BatchCav<St>* __restrict__ cavs, const BatchItem* __restrict__ items,
                 const StepScalars<float>* __restrict__ table, int n_cav, long long step,
                 const long long* __restrict__ step_dev) {
@@ -121,14 +121,49 @@ __global__ void __launch_bounds__(BATCH_THREADS / 2, 10)
                                          item.ty0 + 2 * w, 2 * w + 1 < item.rows, c);
 }
 
+// The node-pair body of k_fused_x (xpair.cuh: two x-adjacent nodes per
+// thread, every plane one 32-bit word) with one CTA per (cavity, 64-column x
+// rows) item: warp w takes row ty0 + w.  16-bit formats only.
+template <class St, bool WRITE_NUT>
+__global__ void __maxnreg__(XPAIR_MAXNREG)
+    k_batch_x(const BatchCav<St>* __restrict__ cavs, const BatchItem* __restrict__ items,
+              const StepScalars<float>* __restrict__ table, int n_cav, long long step,
+              const long long* __restrict__ step_dev) {
+    pdl_wait();
+    pdl_trigger();
+    const long long s = step_dev ? *step_dev + step : step;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const BatchItem item = items[blockIdx.x];
+    const BatchCav<St>& cv = cavs[item.cav];
+    const int row = s < cv.spin_up ? int(s) : cv.spin_up;
+    StepScalars<float> c = table[(long long)row * n_cav + item.cav];
+    c.step = s;
+    c.step_dev = nullptr;
+    const int cur = (cv.parity + int(s & 1)) & 1;
+    const int ix = item.tx0 + 2 * lane;
+    if (ix < cv.G.nx && w < item.rows)
+        fused_xpair<St, WRITE_NUT, false>(cv.pop[cur], cv.pop[cur ^ 1], cv.fy, cv.fy, cv.nut, nullptr, nullptr, cv.G,
+                                          ix, item.ty0 + w, c);
+}
+
+// Which kernel runs a batched step, and the parameters it uses:
+//   0  k_batch      persistent grid of ctas_per_sm x #SMs CTAs over
+//                   32-column x rows_per_item tiles, one thread per node;
+//   1, 2  k_tile    TMA-staged shared-memory tiles of shape 1 or 2,
+//                   ctas_per_sm persistent CTAs per SM;
+//   3  k_batch_np   one CTA per 32-column x rows_per_item item (rows_per_item
+//                   in {1, 2, 4, 8}), one node per thread;
+//   4  k_batch_np2  the same items, two rows per thread on packed FP32x2
+//                   lanes (rows_per_item in {2, 4, 8}; FP32-arithmetic formats);
+//   5  k_batch_x    one CTA per 64-column x rows_per_item item (rows_per_item
+//                   in {1, 2, 4, 8}), two x-adjacent nodes per thread, every
+//                   plane one 32-bit word (16-bit formats).
+// A kernel a format has no version of runs as kernel 3 (FP64: 4 and 5; FP32:
+// 5).  Parameters a kernel does not use are ignored.
 struct BatchTuning {
-    int rows_per_item = 8;
+    int rows_per_item = 4;
     int ctas_per_sm = 8;
-    // 0: k_batch (persistent, one thread per node); 1, 2: k_tile (TMA-staged
-    // tiles, shape 1 or 2); 3: k_batch_np (one CTA per 32 x 4 item);
-    // 4: k_batch_np2 (the same items, two nodes per thread on packed FP32x2
-    // lanes; the FP64 format has no such lanes and runs kernel 3)
-    int kernel = 4;
+    int kernel = 3;
 };
 
 struct BatchBase {
@@ -164,8 +199,6 @@ struct Batch final : BatchBase {
     TileCav<St>* d_tcavs = nullptr;
     CUtensorMap* d_maps[3] = {nullptr, nullptr, nullptr};   // per tile shape
     TileItem* d_titems[3] = {nullptr, nullptr, nullptr};
-    BatchItem* d_np_items = nullptr;
-    int n_np_items = 0;
     unsigned* d_err = nullptr;
     unsigned* h_err = nullptr;  // pinned copy of *d_err
     int n_titems[3] = {0, 0, 0}, tgrid = 0;
@@ -175,7 +208,7 @@ struct Batch final : BatchBase {
         if (graph) cudaGraphExecDestroy(graph);
         if (h_err) cudaFreeHost(h_err);
         void* bufs[] = {d_cavs,      d_items,     d_table, step_dev, d_tcavs,   d_maps[1],
-                        d_maps[2],   d_titems[1], d_titems[2], d_err,  d_np_items};
+                        d_maps[2],   d_titems[1], d_titems[2], d_err};
         for (void* b : bufs)
             if (b) cudaFree(b);
         for (Solver* s : cavs) delete s;
@@ -210,17 +243,6 @@ struct Batch final : BatchBase {
         *h_err = 0;
         setup_tiles<1>();
         setup_tiles<2>();
-        {
-            std::vector<BatchItem> ni;
-            for (int i = 0; i < n; ++i)
-                for (int y0 = 0; y0 < cv[i]->p.ny; y0 += NP_ROWS)
-                    for (int x0 = 0; x0 < cv[i]->p.nx; x0 += 32)
-                        ni.push_back({i, x0, y0, std::min(NP_ROWS, cv[i]->p.ny - y0)});
-            n_np_items = int(ni.size());
-            CK(cudaMalloc(&d_np_items, sizeof(BatchItem) * ni.size()));
-            CK(cudaMemcpyAsync(d_np_items, ni.data(), sizeof(BatchItem) * ni.size(), cudaMemcpyHostToDevice,
-                               stream));
-        }
         set_tuning(tun);
         CK(cudaStreamSynchronize(stream));
     }
@@ -258,16 +280,31 @@ struct Batch final : BatchBase {
         return std::max(1, std::min(n_titems[V], std::max(1, std::min(ctas_per_sm, occ)) * n_sm));
     }
 
+    // The kernel this format runs for a requested one (see BatchTuning).
+    static int effective_kernel(int k) {
+        if (k == 5 && !is_p16<St>::value) k = 3;
+        if (k == 4 && !Fmt<St>::SHIFT) k = 3;
+        return k;
+    }
+
     void set_tuning(const BatchTuning& t) override {
         if (t.rows_per_item < 1 || t.rows_per_item > 1024 || t.ctas_per_sm < 1 || t.ctas_per_sm > 32 ||
-            t.kernel < 0 || t.kernel > 4)
+            t.kernel < 0 || t.kernel > 5)
             throw ArgError{CAV_ERR_ARG, "tuning out of range"};
+        const int k = effective_kernel(t.kernel);
+        const int r = t.rows_per_item;
+        if ((k == 3 || k == 5) && !(r == 1 || r == 2 || r == 4 || r == 8))
+            throw ArgError{CAV_ERR_ARG, "rows_per_item of kernels 3 and 5 must be 1, 2, 4 or 8"};
+        if (k == 4 && !(r == 2 || r == 4 || r == 8))
+            throw ArgError{CAV_ERR_ARG, "rows_per_item of kernel 4 must be 2, 4 or 8"};
         tun = t;
+        // work items: 64 columns for the node-pair kernel, 32 otherwise
+        const int width = k == 5 ? 64 : 32;
         std::vector<BatchItem> items;
         for (int i = 0; i < int(cv.size()); ++i) {
             const int nx = cv[i]->p.nx, ny = cv[i]->p.ny;
-            for (int y0 = 0; y0 < ny; y0 += t.rows_per_item)
-                for (int x0 = 0; x0 < nx; x0 += 32) items.push_back({i, x0, y0, std::min(t.rows_per_item, ny - y0)});
+            for (int y0 = 0; y0 < ny; y0 += r)
+                for (int x0 = 0; x0 < nx; x0 += width) items.push_back({i, x0, y0, std::min(r, ny - y0)});
         }
         if (d_items) CK(cudaFree(d_items));
         n_items = int(items.size());
@@ -352,11 +389,12 @@ struct Batch final : BatchBase {
                               int(stall_copies)));
     }
 
+    // The one-CTA-per-item kernels (3, 4, 5) over d_items.
     template <bool WN>
-    void launch_np(const long long* sdev, long long step) {
+    void launch_np(int k, const long long* sdev, long long step) {
         cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(n_np_items);
-        cfg.blockDim = dim3(BATCH_THREADS);
+        cfg.gridDim = dim3(n_items);
+        cfg.blockDim = dim3(32 * tun.rows_per_item);
         cfg.dynamicSmemBytes = 0;
         cfg.stream = stream;
         cudaLaunchAttribute attr[1];
@@ -364,22 +402,30 @@ struct Batch final : BatchBase {
         attr[0].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
+        if constexpr (is_p16<St>::value) {
+            if (k == 5) {
+                CK(cudaLaunchKernelEx(&cfg, k_batch_x<St, WN>, (const BatchCav<St>*)d_cavs, (const BatchItem*)d_items,
+                                      (const StepScalars<float>*)d_table, int(cv.size()), step, sdev));
+                return;
+            }
+        }
         if constexpr (Fmt<St>::SHIFT) {
-            if (tun.kernel == 4) {
-                cfg.blockDim = dim3(BATCH_THREADS / 2);
+            if (k == 4) {
+                cfg.blockDim = dim3(16 * tun.rows_per_item);
                 CK(cudaLaunchKernelEx(&cfg, k_batch_np2<St, WN>, (const BatchCav<St>*)d_cavs,
-                                      (const BatchItem*)d_np_items, (const StepScalars<float>*)d_table, int(cv.size()),
+                                      (const BatchItem*)d_items, (const StepScalars<float>*)d_table, int(cv.size()),
                                       step, sdev));
                 return;
             }
         }
-        CK(cudaLaunchKernelEx(&cfg, k_batch_np<St, WN>, (const BatchCav<St>*)d_cavs, (const BatchItem*)d_np_items,
+        CK(cudaLaunchKernelEx(&cfg, k_batch_np<St, WN>, (const BatchCav<St>*)d_cavs, (const BatchItem*)d_items,
                               (const StepScalars<A>*)d_table, int(cv.size()), step, sdev));
     }
 
     void launch(bool write_nut, const long long* sdev, long long step) {
-        if (tun.kernel == 3 || tun.kernel == 4) {
-            write_nut ? launch_np<true>(sdev, step) : launch_np<false>(sdev, step);
+        const int k = effective_kernel(tun.kernel);
+        if (k >= 3) {
+            write_nut ? launch_np<true>(k, sdev, step) : launch_np<false>(k, sdev, step);
             ++launches;
             CK(cudaGetLastError());
             return;

@@ -299,6 +299,15 @@ int cav_get_stream(cav_handle* h, void** stream) {
     return guarded(h, [&](Solver& s) { *stream = (void*)s.stream; });
 }
 
+int cav_set_step_kernel(cav_handle* h, int32_t kernel) {
+    return guarded(h, [&](Solver& s) { s.set_step_kernel(kernel); });
+}
+
+int cav_get_step_kernel(cav_handle* h, int32_t* kernel) {
+    if (!kernel) return fail(h, CAV_ERR_ARG, "null output");
+    return guarded(h, [&](Solver& s) { *kernel = s.step_kernel(); });
+}
+
 int cav_snapshot_write_fields(const char* path, int64_t nx, int64_t ny, const double* rho, const double* ux,
                               const double* uy, const double* t) {
     if (!path || !rho || !ux || !uy || !t || nx < 1 || ny < 1) return fail(nullptr, CAV_ERR_ARG, "bad arguments");
@@ -616,41 +625,41 @@ int cav_batch_autotune(cav_batch* b, int32_t trial_steps, cav_batch_tuning* chos
             ps.push_back(p);
         }
         std::unique_ptr<BatchBase> twin(build_batch(ps.data(), int(ps.size())));
-        // candidates: the persistent global-memory kernel over tile heights
-        // and grid sizes, the one-CTA-per-item kernels (one or two nodes per
-        // thread), then the shared-memory tile kernel over its shapes and
-        // grid sizes
+        // candidates: every kernel the format has, over the parameters that
+        // kernel uses (BatchTuning): the persistent global-memory kernel over
+        // tile heights and grid sizes, the shared-memory tile kernel over its
+        // shapes and resident CTAs, the one-CTA-per-item kernels over item
+        // heights
+        const int prec = x.cavs[0]->p.precision;
+        const bool p16 = prec >= CAV_PREC_F16;
         std::vector<BatchTuning> cand;
-        for (int r : {2, 4, 8, 16, 32})
-            for (int c : {4, 8, 12, 16}) {
-                BatchTuning t;
-                t.rows_per_item = r;
-                t.ctas_per_sm = c;
-                t.kernel = 0;
-                cand.push_back(t);
-            }
-        for (int k : {3, 4}) {
+        auto add = [&](int k, int r, int c) {
             BatchTuning t;
-            t.rows_per_item = x.tun.rows_per_item;
-            t.ctas_per_sm = x.tun.ctas_per_sm;
             t.kernel = k;
+            t.rows_per_item = r;
+            t.ctas_per_sm = c;
             cand.push_back(t);
-        }
+        };
+        for (int r : {4, 8, 16})
+            for (int c : {4, 8, 16}) add(0, r, c);
         for (int v : {1, 2})
-            for (int c : {1, 2, 3, 4}) {
-                BatchTuning t;
-                t.rows_per_item = x.tun.rows_per_item;
-                t.ctas_per_sm = c;
-                t.kernel = v;
-                cand.push_back(t);
-            }
+            for (int c : {1, 2, 3, 4}) add(v, 4, c);
+        for (int r : {1, 2, 4, 8}) add(3, r, 8);
+        if (prec != CAV_PREC_F64)
+            for (int r : {2, 4, 8}) add(4, r, 8);
+        if (p16)
+            for (int r : {1, 2, 4, 8}) add(5, r, 8);
+        // each candidate timed three times (after its warm-up steps), the
+        // median kept: one-off noise cannot pick the winner
         BatchTuning best = x.tun;
         double best_ms = 1e300;
         for (const BatchTuning& t : cand) {
             twin->set_tuning(t);
-            double ms = twin->time_steps(trial_steps);
-            if (ms < best_ms) {
-                best_ms = ms;
+            double ms[3];
+            for (double& m : ms) m = twin->time_steps(trial_steps);
+            std::sort(ms, ms + 3);
+            if (ms[1] < best_ms) {
+                best_ms = ms[1];
                 best = t;
             }
         }

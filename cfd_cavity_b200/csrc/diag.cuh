@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(DIAG_THREADS) k_diag_final(const double* __res
         out[6] = res[3];
         out[7] = res[4];
         out[8] = res[DIAG_NPART + 3] / double(G.ny - 2);
-        out[9] = 1.0 + res[6] / double((G.nx - 2) * (G.ny - 2)) * lz / dT;
+        out[9] = 1.0 + res[6] / (double(G.nx - 2) * double(G.ny - 2)) * lz / dT;
         out[10] = res[5];
     }
 }

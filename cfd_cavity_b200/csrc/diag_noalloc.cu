@@ -14,18 +14,24 @@
 // file-scope device array of CAV_NOALLOC_MAX_ROWS x 8 doubles (512 KiB) that
 // every GPU loading this library holds until the process exits.  In host
 // code the name g_row_scratch is only a host-side stand-in for the symbol,
-// not a device address: the first call on each device, with that device
-// current, asks the runtime for the real address (cudaGetSymbolAddress) and
-// caches it; that first call should therefore come before any stream
-// capture on that device.  Every row's partials are rewritten by each call
-// before they are read, so nothing has to be cleared between calls; but the
-// array keeps the last call's contents and is shared by all calls on a
-// device, so two calls whose kernels overlap on the GPU (different streams,
-// no ordering between them) race on it and must be serialised by the caller.
+// not a device address: every call, with the caller's device current, asks
+// the runtime for the real address (cudaGetSymbolAddress, cheap once the
+// module is loaded) and passes it to the kernels.  Nothing is cached, so a
+// cudaDeviceReset or another context between calls cannot leave a stale
+// address behind.  The first call on a device may load the library's device
+// code there, so it should come before any stream capture on that device.
+// Every row's partials are rewritten by each call before they are read, so
+// nothing has to be cleared between calls; but the array keeps the last
+// call's contents and is shared by all calls on a device, so two calls whose
+// kernels overlap on the GPU (different streams, no ordering between them)
+// race on it and must be serialised by the caller.
+//
+// Errors.  A CUDA error already pending when the call starts (left by the
+// caller's own work) is reported as CAV_ERR_CUDA without launching anything
+// and is not cleared: the caller still finds it with cudaGetLastError.
 #include <cuda_runtime.h>
 
 #include <cstdio>
-#include <mutex>
 
 #include "../../include/cavity.h"
 #include "diag.cuh"
@@ -33,12 +39,8 @@
 namespace {
 
 constexpr int NPART = 8;  // per row: sum rho, sum f, max u, max uy, max nu_t, non-finite, sum vol, spare
-constexpr int MAX_DEVICES = 64;
 
 static __device__ __align__(256) double g_row_scratch[CAV_NOALLOC_MAX_ROWS * NPART];
-
-std::mutex g_setup_mutex;
-double* g_scratch_addr[MAX_DEVICES] = {};
 
 // Pass 1: one block per row of a dense FP64 state, row-partials into scratch.
 __global__ void __launch_bounds__(cav::DIAG_THREADS)
@@ -107,7 +109,7 @@ k_final(const double* __restrict__ scratch, const double* __restrict__ uy, const
         out[6] = res[3];
         out[7] = res[4];
         out[8] = res[NPART + 3] / double(ny - 2);
-        out[9] = 1.0 + res[6] / double((nx - 2) * (ny - 2)) * lz;
+        out[9] = 1.0 + res[6] / (double(nx - 2) * double(ny - 2)) * lz;
         out[10] = res[5] == 0.0 ? 1.0 : 0.0;
     }
 }
@@ -134,26 +136,23 @@ int cav_diag_noalloc(const double* rho, const double* ux, const double* uy, cons
         return err(CAV_ERR_ARG, buf);
     }
     if (!(nu > 0.0)) return err(CAV_ERR_ARG, "nu must be positive");
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES)
-        return err(CAV_ERR_CUDA, "cudaGetDevice failed");
-    double* scratch;
-    {
-        // One-time set-up per device, with that device current: the device
-        // address of the static scratch array.
-        std::lock_guard<std::mutex> lk(g_setup_mutex);
-        if (!g_scratch_addr[dev]) {
-            void* p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, g_row_scratch);
-            if (e != cudaSuccess || !p) return err(CAV_ERR_CUDA, cudaGetErrorString(e));
-            g_scratch_addr[dev] = static_cast<double*>(p);
-        }
-        scratch = g_scratch_addr[dev];
+    // an error the caller left pending is reported, not consumed
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) return err(CAV_ERR_CUDA, cudaGetErrorString(pending));
+    // the device address of the static scratch on the current device
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_row_scratch);
+    if (e != cudaSuccess || !p) {
+        if (e != cudaSuccess) cudaGetLastError();  // this call's own failure
+        return err(CAV_ERR_CUDA, e != cudaSuccess ? cudaGetErrorString(e) : "null scratch address");
     }
+    double* scratch = static_cast<double*>(p);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     k_rows<<<ny, cav::DIAG_THREADS, 0, s>>>(rho, ux, uy, t, nu_t, f, nx, ny, scratch);
+    e = cudaGetLastError();  // nothing was pending, so a failure here is this launch's
+    if (e != cudaSuccess) return err(CAV_ERR_CUDA, cudaGetErrorString(e));
     k_final<<<1, cav::DIAG_THREADS, 0, s>>>(scratch, uy, t, nu_t, nx, ny, nu, lz, out);
-    cudaError_t e = cudaGetLastError();
+    e = cudaGetLastError();
     if (e != cudaSuccess) return err(CAV_ERR_CUDA, cudaGetErrorString(e));
     return CAV_OK;
 }

@@ -2,8 +2,9 @@
 // over the C ABI of libcavity_b200.so.
 //
 //   command line   parse_args (src/cli.rs:185-384): the same flags, aliases,
-//                  defaults, checks and exit codes; --precision and --device
-//                  are additions (storage format, CUDA device);
+//                  defaults, checks and exit codes; --precision, --device
+//                  and --geq-order are additions (storage format, CUDA
+//                  device, form of the g equilibrium);
 //   run_uniform    src/main.rs:42-443;
 //   run_octree     src/main.rs:447-720.
 //
@@ -65,6 +66,7 @@ struct Args {
     // additions of this build
     std::string precision = "f64";
     int device = 0;
+    int geq_order = 2;
 };
 
 const char* USAGE =
@@ -107,7 +109,8 @@ const char* USAGE =
     "GPU:\n"
     "  --precision <p>           uniform: f64 f32 f16 bf16 f16g f16sr bf16sr f16gsr;\n"
     "                            octree: f64 f32 f32_f16 f32_f16g  [f64]\n"
-    "  --device <n>              CUDA device ordinal              [0]\n";
+    "  --device <n>              CUDA device ordinal              [0]\n"
+    "  --geq-order <1|2>         uniform: g equilibrium linear / quadratic in u [2]\n";
 
 struct ArgError {
     std::string msg;
@@ -223,6 +226,12 @@ Args parse_args(int argc, char** argv, bool& help) {
         else if (key == "bl-width" || key == "bl_width") uint_of(a.bl_width, "bl-width");
         else if (key == "levels") uint_of(a.levels, "levels");
         else if (key == "precision") a.precision = value;
+        else if (key == "geq-order" || key == "geq_order") {
+            long long o;
+            uint_of(o, "geq-order");
+            if (o != 1 && o != 2) throw ArgError{"--geq-order: 1 or 2 expected"};
+            a.geq_order = int(o);
+        }
         else if (key == "device") {
             long long d;
             uint_of(d, "device");
@@ -411,6 +420,7 @@ int run_uniform(const Args& args) {
     p.nu_override = args.nu;
     p.init_mode = CAV_INIT_LINEAR;
     p.noise_amp = 1.0e-3;
+    p.geq_order = args.geq_order;
     p.precision = prec;
     p.device = args.device;
     cav_handle* h = nullptr;

@@ -27,9 +27,57 @@ __device__ __forceinline__ void stp(St* __restrict__ buf, const Geom& G, int q, 
     buf[(long long)q * G.plane + (long long)iy * G.pitch + ix] = Fmt<St>::store(v, q, r);
 }
 
+// Stochastic rounding draws.  The two x-adjacent nodes (2j, iy) and
+// (2j + 1, iy) share one generator, seeded by the seed, the step and the pair
+// index iy * ceil(nx / 2) + j (NodeRng), and one 32-bit draw r per plane,
+// planes 0..17 in order: node 2j takes its dither from r's high bits, node
+// 2j + 1 from its low bits (binary16: r[31:19] / r[15:3]; bfloat16:
+// r[31:16] / r[15:0]; 16-bit fixed point: r[31:16] / r[15:0]).  The x-pair
+// kernels round a plane of both nodes with one cvt.rs (the draw rotated so
+// that the hardware takes those bits); the one-node kernels compute the
+// pair's draws and use their half, so every kernel gives a node the same bits.
+__device__ __forceinline__ uint32_t sr_bits_f16(uint32_t r) { return __funnelshift_r(r, r, 19); }
+__device__ __forceinline__ uint32_t sr_bits_bf16(uint32_t r) { return __funnelshift_r(r, r, 16); }
+__host__ __device__ __forceinline__ uint32_t sr_bits_fx(uint32_t r, int half) {
+    return half ? r << 16 : r & 0xffff0000u;
+}
+// The software rounding's draw for node half h (h16_enc / bf16_store take
+// their dither from the top bits of the word they are given).
+__host__ __device__ __forceinline__ uint32_t sr_bits_sw(uint32_t r, int half) { return half ? r << 16 : r; }
+template <class A>
+__device__ __forceinline__ NodeRng sr_pair_rng(const StepScalars<A>& c, const Geom& G, int ix, int iy) {
+    const long long step = c.step_dev ? *c.step_dev + c.step : c.step;
+    return NodeRng(c.sr_seed, step, (long long)iy * ((G.nx + 1) >> 1) + (ix >> 1));
+}
+
+// Rounds x (in the plane's stored units) to the 16 bits of node half h of
+// plane q, from the pair's draw r for that plane.
+template <class St, bool LANE>
+__device__ __forceinline__ St store_sr_pairdraw(typename Fmt<St>::A x, int q, uint32_t r, int h) {
+    if constexpr (Fmt<St>::HW_SR_F) {
+        const bool hw = q < Q || Fmt<St>::HW_SR_G;
+        if (hw) {
+            const float s = LANE ? 1.0f : (q < Q ? p2(Fmt<St>::EF) : p2(Fmt<St>::EG));
+            const float v = x * s;
+            uint32_t d;
+            if constexpr (Fmt<St>::KIND_BF16)
+                asm("cvt.rs.bf16x2.f32 %0, %1, %1, %2;" : "=r"(d) : "f"(v), "r"(sr_bits_bf16(r)));
+            else
+                asm("cvt.rs.f16x2.f32 %0, %1, %1, %2;" : "=r"(d) : "f"(v), "r"(sr_bits_f16(r)));
+            St o;
+            o.bits = (unsigned short)(h ? d >> 16 : d & 0xffffu);
+            return o;
+        }
+        return LANE ? Fmt<St>::lstore_sr(x, q, sr_bits_fx(r, h)) : Fmt<St>::store_sr(x, q, sr_bits_fx(r, h));
+    } else {
+        const uint32_t b = (Fmt<St>::FIXED_G && q >= Q) ? sr_bits_fx(r, h) : sr_bits_sw(r, h);
+        return LANE ? Fmt<St>::lstore_sr(x, q, b) : Fmt<St>::store_sr(x, q, b);
+    }
+}
+
 // Stores the 18 populations of one node (32-bit offsets, like pull_node);
-// the stochastically rounded formats draw their random bits from the
-// (seed, step, node) stream, two 16-bit draws per generator step.
+// the stochastically rounded formats draw their random bits from the node
+// pair's (seed, step, pair) stream (sr_pair_rng).
 // LANE: f and g in lane units (Fmt::lstore).
 template <class St, bool LANE = false>
 __device__ __forceinline__ void store_node(St* __restrict__ dst, const Geom& G, int iy, int ix,
@@ -37,43 +85,13 @@ __device__ __forceinline__ void store_node(St* __restrict__ dst, const Geom& G, 
                                            const StepScalars<typename Fmt<St>::A>& c) {
     const int P = int(G.plane);
     const int k = iy * G.pitch + ix;
-    if constexpr (Fmt<St>::HW_SR_F) {
-        // pairs of planes (q, q + 1) from one draw, rounded by one cvt.rs
-        // where both are binary16 / bfloat16: the bits of the path below
-        const long long step = c.step_dev ? *c.step_dev + c.step : c.step;
-        NodeRng rng(c.sr_seed, step, (long long)iy * G.nx + ix);
-        const float sf = LANE ? 1.0f : p2(Fmt<St>::EF), sg = LANE ? 1.0f : p2(Fmt<St>::EG);
-#pragma unroll
-        for (int q = 0; q < NPLANES; q += 2) {
-            const uint32_t r = rng.next();
-            const auto xa = q < Q ? f[q] : g[q - Q];
-            const auto xb = q + 1 < Q ? f[q + 1] : g[q + 1 - Q];
-            const bool ha = q < Q || Fmt<St>::HW_SR_G, hb = q + 1 < Q || Fmt<St>::HW_SR_G;
-            if (ha && hb) {
-                const uint32_t d = Fmt<St>::enc2_sr(xa * (q < Q ? sf : sg), xb * (q + 1 < Q ? sf : sg), r);
-                dst[q * P + k].bits = (unsigned short)(d >> 16);
-                dst[(q + 1) * P + k].bits = (unsigned short)(d & 0xffffu);
-            } else {
-                if (ha)
-                    dst[q * P + k].bits = (unsigned short)(Fmt<St>::enc2_sr(xa * sf, 0.0f, r) >> 16);
-                else
-                    dst[q * P + k] = LANE ? Fmt<St>::lstore_sr(xa, q, r & 0xffff0000u)
-                                          : Fmt<St>::store_sr(xa, q, r & 0xffff0000u);
-                dst[(q + 1) * P + k] = LANE ? Fmt<St>::lstore_sr(xb, q + 1, r << 16)
-                                            : Fmt<St>::store_sr(xb, q + 1, r << 16);
-            }
-        }
-    } else if constexpr (Fmt<St>::SR) {
-        const long long step = c.step_dev ? *c.step_dev + c.step : c.step;
-        NodeRng rng(c.sr_seed, step, (long long)iy * G.nx + ix);
-        uint32_t r = 0;
+    if constexpr (Fmt<St>::SR) {
+        NodeRng rng = sr_pair_rng(c, G, ix, iy);
+        const int h = ix & 1;
 #pragma unroll
         for (int q = 0; q < NPLANES; ++q) {
-            // high half of an LCG output, then its bits 0..15 shifted up
-            if ((q & 1) == 0) r = rng.next();
-            const uint32_t bits = (q & 1) == 0 ? (r & 0xffff0000u) : (r << 16);
-            const auto x = q < Q ? f[q] : g[q - Q];
-            dst[q * P + k] = LANE ? Fmt<St>::lstore_sr(x, q, bits) : Fmt<St>::store_sr(x, q, bits);
+            const uint32_t r = rng.next();
+            dst[q * P + k] = store_sr_pairdraw<St, LANE>(q < Q ? f[q] : g[q - Q], q, r, h);
         }
     } else {
 #pragma unroll
@@ -92,36 +110,13 @@ __device__ __forceinline__ void store_planes(St* __restrict__ dst, const Geom& G
                                              const StepScalars<typename Fmt<St>::A>& c) {
     const int P = int(G.plane);
     const int k = iy * G.pitch + ix;
-    if constexpr (Q0 == 0 ? Fmt<St>::HW_SR_F : Fmt<St>::HW_SR_G) {
-        const long long step = c.step_dev ? *c.step_dev + c.step : c.step;
-        NodeRng rng(c.sr_seed, step, (long long)iy * G.nx + ix);
+    if constexpr (Fmt<St>::SR) {
+        NodeRng rng = sr_pair_rng(c, G, ix, iy);
 #pragma unroll
-        for (int j = 0; j < Q0 / 2; ++j) rng.next();  // the draws of planes 0..Q0-1
-        int q = Q0;
-        if (Q0 & 1) {  // plane Q0 is the low half of its draw
-            dst[q * P + k].bits = (unsigned short)(Fmt<St>::enc2_sr(0.0f, v[0], rng.next()) & 0xffffu);
-            ++q;
-        }
+        for (int j = 0; j < Q0; ++j) rng.next();  // the draws of planes 0..Q0-1
+        const int h = ix & 1;
 #pragma unroll
-        for (; q + 1 < Q0 + Q; q += 2) {
-            const uint32_t d = Fmt<St>::enc2_sr(v[q - Q0], v[q + 1 - Q0], rng.next());
-            dst[q * P + k].bits = (unsigned short)(d >> 16);
-            dst[(q + 1) * P + k].bits = (unsigned short)(d & 0xffffu);
-        }
-        if (q < Q0 + Q)  // the last plane is the high half of its draw
-            dst[q * P + k].bits = (unsigned short)(Fmt<St>::enc2_sr(v[q - Q0], 0.0f, rng.next()) >> 16);
-    } else if constexpr (Fmt<St>::SR) {
-        const long long step = c.step_dev ? *c.step_dev + c.step : c.step;
-        NodeRng rng(c.sr_seed, step, (long long)iy * G.nx + ix);
-#pragma unroll
-        for (int j = 0; j < Q0 / 2; ++j) rng.next();  // the draws of planes 0..Q0-1
-        uint32_t r = (Q0 & 1) ? rng.next() : 0u;
-#pragma unroll
-        for (int q = Q0; q < Q0 + Q; ++q) {
-            if ((q & 1) == 0) r = rng.next();
-            const uint32_t bits = (q & 1) == 0 ? (r & 0xffff0000u) : (r << 16);
-            dst[q * P + k] = Fmt<St>::lstore_sr(v[q - Q0], q, bits);
-        }
+        for (int q = Q0; q < Q0 + Q; ++q) dst[q * P + k] = store_sr_pairdraw<St, true>(v[q - Q0], q, rng.next(), h);
     } else {
 #pragma unroll
         for (int q = Q0; q < Q0 + Q; ++q) dst[q * P + k] = Fmt<St>::lstore(v[q - Q0], q, RN_BITS);
@@ -148,7 +143,9 @@ static __global__ void k_add_step(long long* p, long long d) { *p += d; }
 //  the domain, so the reference's "keep g at out-of-domain sources" value
 //  is always overwritten and never needed here.
 // LANE: values in lane units (Fmt::lload).
-template <class St, bool LANE = false>
+// CHANNEL: the plane-channel variant (periodic in y, bounce-back walls at
+// x = 0 and nx - 1), see k_fused.
+template <class St, bool LANE = false, bool CHANNEL = false>
 __device__ __forceinline__ void pull_f(const St* __restrict__ src, const Geom& G, int ix, int iy,
                                        typename Fmt<St>::A (&f)[Q]) {
     // 32-bit element offsets: 18 * plane < 2^31 is checked at allocation.
@@ -158,9 +155,35 @@ __device__ __forceinline__ void pull_f(const St* __restrict__ src, const Geom& G
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
         const int cx = CX(i), cy = CY(i);
-        const bool ok = (cx > 0 ? xm : (cx < 0 ? xp : true)) && (cy > 0 ? ym : (cy < 0 ? yp : true));
-        const int idx = ok ? i * P + k - cx - cy * W : OPP(i) * P + k;  // else bounce-back
-        f[i] = LANE ? Fmt<St>::lload(src[idx], i) : Fmt<St>::load(src[idx], i);
+        if constexpr (CHANNEL) {
+            const int sy = cy > 0 ? (ym ? iy - 1 : G.ny - 1) : (cy < 0 ? (yp ? iy + 1 : 0) : iy);
+            const bool ok = cx > 0 ? xm : (cx < 0 ? xp : true);
+            const int idx = ok ? i * P + sy * W + ix - cx : OPP(i) * P + k;
+            f[i] = LANE ? Fmt<St>::lload(src[idx], i) : Fmt<St>::load(src[idx], i);
+        } else {
+            const bool ok = (cx > 0 ? xm : (cx < 0 ? xp : true)) && (cy > 0 ? ym : (cy < 0 ? yp : true));
+            const int idx = ok ? i * P + k - cx - cy * W : OPP(i) * P + k;  // else bounce-back
+            f[i] = LANE ? Fmt<St>::lload(src[idx], i) : Fmt<St>::load(src[idx], i);
+        }
+    }
+}
+
+// g of the plane channel: periodic in y; an out-of-domain x source keeps the
+// node's own value (stream(), src/uniform/solver.rs:879-881); no thermal
+// boundary conditions.
+template <class St, bool LANE = false>
+__device__ __forceinline__ void pull_g_channel(const St* __restrict__ src, const Geom& G, int ix, int iy,
+                                               typename Fmt<St>::A (&g)[Q]) {
+    const int P = int(G.plane), W = G.pitch;
+    const int k = iy * W + ix;
+    const bool xm = ix > 0, xp = ix < G.nx - 1, ym = iy > 0, yp = iy < G.ny - 1;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const int cx = CX(i), cy = CY(i);
+        const int sy = cy > 0 ? (ym ? iy - 1 : G.ny - 1) : (cy < 0 ? (yp ? iy + 1 : 0) : iy);
+        const bool ok = cx > 0 ? xm : (cx < 0 ? xp : true);
+        const int idx = (Q + i) * P + (ok ? sy * W + ix - cx : k);
+        g[i] = LANE ? Fmt<St>::lload(src[idx], Q + i) : Fmt<St>::load(src[idx], Q + i);
     }
 }
 
@@ -234,7 +257,7 @@ __device__ __forceinline__ bool is_wall(const Geom& G, int ix, int iy) {
 // Shared by the global-memory pull (fused_node_io) and the shared-memory
 // tiles (tile.cuh), so both give the same bits.  f and g arrive in lane units
 // (pull with LANE); t_at returns T unscaled.
-template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE, class TAt>
+template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE, class TAt, bool CHANNEL = false>
 __device__ __forceinline__ void fused_core(typename Fmt<St>::A (&f)[Q], typename Fmt<St>::A (&g)[Q],
                                            St* __restrict__ dst, const typename Fmt<St>::A* fy_in,
                                            typename Fmt<St>::A* fy_out, typename Fmt<St>::A* __restrict__ nut,
@@ -245,7 +268,7 @@ __device__ __forceinline__ void fused_core(typename Fmt<St>::A (&f)[Q], typename
     constexpr bool SH = Fmt<St>::SHIFT;
     constexpr int EF = Fmt<St>::EF, EG = Fmt<St>::EG;
     const int k = iy * G.pitch + ix;
-    const bool wall = is_wall(G, ix, iy);
+    const bool wall = !CHANNEL && is_wall(G, ix, iy);
     Macro<A, SH> m;
     if constexpr (SH) {
         m = macro_f_lane<A, EF>(f, fy_in[k], wall);
@@ -265,7 +288,22 @@ __device__ __forceinline__ void fused_core(typename Fmt<St>::A (&f)[Q], typename
         }
     }
     A fyv, nutv;
-    if (!NO_COLLIDE) {
+    if (CHANNEL) {
+        // body force rho beta along +y (the temperature factor taken as 1)
+        if constexpr (SH) {
+            const CollF<A> o = collide_f_pre_lane<A, EF>(f, m, c, nullptr);
+            nutv = o.nut;
+            fyv = collide_f_post_lane<A, EF, EG>(f, o, m, c, A(p2(EG)));
+            collide_g_lane<A>(g, m.t, m.ux, m.uy, o.nut, o.q, c, nullptr);
+        } else {
+            const CollF<A> o = collide_f_pre<A, SH>(f, m, c);
+            nutv = o.nut;
+            fyv = collide_f_post<A, SH>(f, o, m, c, A(1.0));
+            collide_g<A, SH>(g, m.t, m.ux, m.uy, o.nut, c);
+        }
+        fy_out[k] = fyv;
+        if (WRITE_NUT) nut[k] = nutv;
+    } else if (!NO_COLLIDE) {
         if constexpr (SH)
             collide_node_lane<A, EF, EG>(f, g, m, c, fyv, nutv);
         else
@@ -276,7 +314,7 @@ __device__ __forceinline__ void fused_core(typename Fmt<St>::A (&f)[Q], typename
     store_node<St, true>(dst, G, iy, ix, f, g, c);
 }
 
-template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE>
+template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE, bool CHANNEL = false>
 __device__ __forceinline__ void fused_node_io(const St* __restrict__ src, St* __restrict__ dst,
                                               const typename Fmt<St>::A* fy_in, typename Fmt<St>::A* fy_out,
                                               typename Fmt<St>::A* __restrict__ nut, double* __restrict__ acc_hot,
@@ -284,17 +322,24 @@ __device__ __forceinline__ void fused_node_io(const St* __restrict__ src, St* __
                                               const StepScalars<typename Fmt<St>::A>& c) {
     using A = typename Fmt<St>::A;
     A f[Q], g[Q];
-    pull_node<St, true>(src, G, ix, iy, c, f, g);
-    fused_core<St, WRITE_NUT, ACC_NU, NO_COLLIDE>(f, g, dst, fy_in, fy_out, nut, acc_hot, acc_cold, G, ix, iy, c,
-                                                  [&](int x) { return gather_t<St>(src, G, x, iy, c); });
+    if constexpr (CHANNEL) {
+        pull_f<St, true, true>(src, G, ix, iy, f);
+        pull_g_channel<St, true>(src, G, ix, iy, g);
+    } else {
+        pull_node<St, true>(src, G, ix, iy, c, f, g);
+    }
+    auto t_at = [&](int x) { return gather_t<St>(src, G, x, iy, c); };
+    fused_core<St, WRITE_NUT, ACC_NU && !CHANNEL, NO_COLLIDE, decltype(t_at)&, CHANNEL>(
+        f, g, dst, fy_in, fy_out, nut, acc_hot, acc_cold, G, ix, iy, c, t_at);
 }
 
-template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE>
+template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE, bool CHANNEL = false>
 __device__ __forceinline__ void fused_node(const St* __restrict__ src, St* __restrict__ dst,
                                            typename Fmt<St>::A* fy, typename Fmt<St>::A* __restrict__ nut,
                                            double* __restrict__ acc_hot, double* __restrict__ acc_cold,
                                            const Geom& G, int ix, int iy, const StepScalars<typename Fmt<St>::A>& c) {
-    fused_node_io<St, WRITE_NUT, ACC_NU, NO_COLLIDE>(src, dst, fy, fy, nut, acc_hot, acc_cold, G, ix, iy, c);
+    fused_node_io<St, WRITE_NUT, ACC_NU, NO_COLLIDE, CHANNEL>(src, dst, fy, fy, nut, acc_hot, acc_cold, G, ix, iy,
+                                                              c);
 }
 
 // Two nodes of one column, (ix, iy) and (ix, iy + 1), in one thread: the
@@ -373,7 +418,13 @@ __device__ __forceinline__ void fused_pair(const St* __restrict__ src, St* __res
 //              to the per-row FP64 accumulators (nusselt_hot/cold, post.rs:68-111).
 //  NO_COLLIDE  identity collision: checks the streaming / bounce-back /
 //              boundary index maps bit for bit.
-template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE>
+//  CHANNEL     the same node body on a plane channel instead of the cavity:
+//              periodic in y, bounce-back walls at x = 0 and nx - 1 with no
+//              wall-velocity override and no thermal boundary conditions,
+//              body force rho beta along +y (the reference's Poiseuille
+//              test of the TRT + Guo collision, src/uniform/tests.rs:246-376,
+//              turned by 90 degrees).
+template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE, bool CHANNEL = false>
 __global__ void __launch_bounds__(256) k_fused(const St* __restrict__ src, St* __restrict__ dst,
                                                typename Fmt<St>::A* __restrict__ fy,
                                                typename Fmt<St>::A* __restrict__ nut, double* __restrict__ acc_hot,
@@ -384,7 +435,7 @@ __global__ void __launch_bounds__(256) k_fused(const St* __restrict__ src, St* _
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iy = blockIdx.y * blockDim.y + threadIdx.y;
     if (ix >= G.nx || iy >= G.ny) return;
-    fused_node<St, WRITE_NUT, ACC_NU, NO_COLLIDE>(src, dst, fy, nut, acc_hot, acc_cold, G, ix, iy, c);
+    fused_node<St, WRITE_NUT, ACC_NU, NO_COLLIDE, CHANNEL>(src, dst, fy, nut, acc_hot, acc_cold, G, ix, iy, c);
 }
 
 // collide(step) on a REF state (populations + fields), writing PC to dst.
@@ -429,7 +480,7 @@ __global__ void __launch_bounds__(256) k_collide_ref(const St* __restrict__ src,
 
 // PC(src) -> REF(dst): stream + thermal BC + macroscopic + no-slip, without
 // the next collision.  Produces the reference's observable state.
-template <class St>
+template <class St, bool CHANNEL = false>
 __global__ void __launch_bounds__(256) k_materialize(const St* __restrict__ src, St* __restrict__ dst,
                                                      const typename Fmt<St>::A* __restrict__ fy,
                                                      typename Fmt<St>::A* __restrict__ rho,
@@ -444,8 +495,13 @@ __global__ void __launch_bounds__(256) k_materialize(const St* __restrict__ src,
     if (ix >= G.nx || iy >= G.ny) return;
     const long long k = (long long)iy * G.pitch + ix;
     A f[Q], g[Q];
-    pull_node<St>(src, G, ix, iy, c, f, g);
-    Macro<A, SH> m = macro_node<A, SH>(f, g, fy[k], is_wall(G, ix, iy));
+    if constexpr (CHANNEL) {
+        pull_f<St, false, true>(src, G, ix, iy, f);
+        pull_g_channel<St>(src, G, ix, iy, g);
+    } else {
+        pull_node<St>(src, G, ix, iy, c, f, g);
+    }
+    Macro<A, SH> m = macro_node<A, SH>(f, g, fy[k], !CHANNEL && is_wall(G, ix, iy));
     rho[k] = m.rho;
     ux[k] = m.ux;
     uy[k] = m.uy;

@@ -71,6 +71,7 @@ template <>
 struct Fmt<double> {
     using A = double;
     static constexpr bool SHIFT = false, SR = false, HW_SR_F = false, HW_SR_G = false;
+    static constexpr bool KIND_BF16 = false, FIXED_G = false;
     static constexpr int EF = 0, EG = 0;
     __host__ __device__ static A load(double v, int) { return v; }
     __host__ __device__ static double store(A v, int, uint32_t) { return v; }
@@ -81,6 +82,7 @@ template <>
 struct Fmt<float> {
     using A = float;
     static constexpr bool SHIFT = true, SR = false, HW_SR_F = false, HW_SR_G = false;
+    static constexpr bool KIND_BF16 = false, FIXED_G = false;
     static constexpr int EF = 0, EG = 0;
     __host__ __device__ static A load(float v, int) { return v; }
     __host__ __device__ static float store(A v, int, uint32_t) { return v; }
@@ -195,16 +197,22 @@ struct P16 {
     unsigned short bits;
 };
 constexpr int K_HALF = 0, K_BF16 = 1, K_MIX = 2;  // MIX: binary16 f - w, fixed-point g
+template <class St>
+struct is_p16 : std::false_type {};
+template <int KIND, bool SRND>
+struct is_p16<P16<KIND, SRND>> : std::true_type {};
 
 template <int KIND, bool SRND>
 struct Fmt<P16<KIND, SRND>> {
     using A = float;
     using St = P16<KIND, SRND>;
     static constexpr bool SHIFT = true, SR = SRND;
-    // stochastic rounding of the binary16 (bfloat16) planes by the hardware,
-    // two planes per cvt.rs (enc2_sr): the f planes of every 16-bit format,
-    // the g planes unless they are fixed point
+    // stochastic rounding of the binary16 (bfloat16) planes by the hardware
+    // cvt.rs: the f planes of every 16-bit format, the g planes unless they
+    // are fixed point.  enc2_sr rounds two planes of one node (the octree's
+    // stores); the uniform solver rounds one plane of two nodes (kernels.cuh)
     static constexpr bool HW_SR_F = SRND, HW_SR_G = SRND && KIND != K_MIX;
+    static constexpr bool KIND_BF16 = KIND == K_BF16, FIXED_G = KIND == K_MIX;
 #ifdef __CUDACC__
     __device__ static uint32_t enc2_sr(float a, float b, uint32_t r) {
         if constexpr (KIND == K_BF16)
@@ -283,6 +291,16 @@ struct NodeRng {
     __host__ __device__ uint32_t next() {
         s = s * 1664525u + 1013904223u;
         return s;
+    }
+    // Advances by K draws in one multiply-add: s <- a^K s + c (a^(K-1) + ... + 1).
+    template <int K>
+    __host__ __device__ void skip() {
+        uint32_t a = 1u, c = 0u;
+        for (int j = 0; j < K; ++j) {
+            c = c * 1664525u + 1013904223u;
+            a = a * 1664525u;
+        }
+        s = s * a + c;
     }
 };
 
@@ -524,28 +542,55 @@ struct CollF {
 // and pi_neq only needs the symmetric parts.  Same arithmetic as the
 // reference up to rounding, a third of the operations.  f, drho and the
 // non-equilibrium parts in lane units (scaled by 2^EF).
+// The pieces of the pairwise split, each one expression so that every caller
+// (whatever it keeps in registers and what it recomputes) gets the same bits.
+template <class L>
+__device__ __forceinline__ L m15u2_lane(L u, L v) {
+    return lmul(lbc<L>(-1.5f), lfma(u, u, lmul(v, v)));
+}
+// q_p = 4.5 (c_p.u)^2 - 1.5 u^2
+template <class L>
+__device__ __forceinline__ L q_lane(int p, L u, L v, L m15u2) {
+    const L eu = eu_pair<L>(p, u, v);
+    return lfma(lbc<L>(4.5f), lmul(eu, eu), m15u2);
+}
+// (h_p + h_opp) - 2 w (drho + rho q)
+template <class L>
+__device__ __forceinline__ L dS_lane(int p, const L (&f)[Q], L r, L drho, L q) {
+    return lfma(lbc<L>(-2.0f * float(WD(p))), lfma(r, q, drho), ladd(f[p], f[p + 4]));
+}
+// (h_p - h_opp) - 2 w rho 3 e.u
+template <class L>
+__device__ __forceinline__ L dD_lane(int p, const L (&f)[Q], L r, L u, L v) {
+    return lfma(lbc<L>(-6.0f * float(WD(p))), lmul(r, eu_pair<L>(p, u, v)), lsub(f[p], f[p + 4]));
+}
+// rest: h_0 - (feq_0 - w_0) = h_0 - w_0 (drho - 1.5 rho u^2)
+template <class L>
+__device__ __forceinline__ L d0_lane(const L (&f)[Q], L r, L drho, L m15u2) {
+    return lfma(lbc<L>(-float(WD(0))), lfma(r, m15u2, drho), f[0]);
+}
+template <class L, int EF>
+__device__ __forceinline__ L rho_scaled(const Macro<L, true>& m) {
+    return EF == 0 ? m.rho : lmul(m.rho, lbc<L>(p2(EF)));  // rho 2^EF
+}
+
+// The relaxation coefficients alone (nu_t from pi_neq, 1/tau+-, k+-): what
+// collide_f_pre_lane computes besides the non-equilibrium parts.
+template <class L>
+struct CollCoef {
+    L nut, w1, w2, k1, k2;
+};
 template <class L, int EF = 0>
-__device__ __forceinline__ CollF<L> collide_f_pre_lane(const L (&f)[Q], const Macro<L, true>& m,
-                                                       const StepScalars<float>& c, const L* nut_ovr) {
-    CollF<L> o;
-    const L u = m.ux, v = m.uy;
-    const L r = EF == 0 ? m.rho : lmul(m.rho, lbc<L>(p2(EF)));  // rho 2^EF
-    const L u2 = lfma(u, u, lmul(v, v));
-    const L m15u2 = lmul(lbc<L>(-1.5f), u2);
-    // rest: h_0 - (feq_0 - w_0) = h_0 - w_0 (drho - 1.5 rho u^2)
-    o.d0 = lfma(lbc<L>(-float(WD(0))), lfma(r, m15u2, m.drho), f[0]);
+__device__ __forceinline__ CollCoef<L> collide_f_coef_lane(const L (&f)[Q], const Macro<L, true>& m,
+                                                           const StepScalars<float>& c, const L* nut_ovr) {
+    CollCoef<L> o;
+    const L u = m.ux, v = m.uy, r = rho_scaled<L, EF>(m), m15u2 = m15u2_lane<L>(u, v);
+    L dS[5];
 #pragma unroll
-    for (int p = 1; p <= 4; ++p) {
-        const float w = float(WD(p));
-        const L eu = eu_pair<L>(p, u, v);
-        o.q[p] = lfma(lbc<L>(4.5f), lmul(eu, eu), m15u2);
-        // (h_p + h_opp) - 2 w (drho + rho q),  (h_p - h_opp) - 2 w rho 3 e.u
-        o.dS[p] = lfma(lbc<L>(-2.0f * w), lfma(r, o.q[p], m.drho), ladd(f[p], f[p + 4]));
-        o.dD[p] = lfma(lbc<L>(-6.0f * w), lmul(r, eu), lsub(f[p], f[p + 4]));
-    }
+    for (int p = 1; p <= 4; ++p) dS[p] = dS_lane<L>(p, f, r, m.drho, q_lane<L>(p, u, v, m15u2));
     // pi_neq (solver.rs:1096-1106) from the symmetric parts.
-    const L s34 = ladd(o.dS[3], o.dS[4]);
-    const L pxx = ladd(o.dS[1], s34), pyy = ladd(o.dS[2], s34), pxy = lsub(o.dS[3], o.dS[4]);
+    const L s34 = ladd(dS[3], dS[4]);
+    const L pxx = ladd(dS[1], s34), pyy = ladd(dS[2], s34), pxy = lsub(dS[3], dS[4]);
     const L pi2 = lfma(pxx, pxx, lfma(lmul(lbc<L>(2.0f), pxy), pxy, lmul(pyy, pyy)));
     // nu_t = Cs^2 |S|, |S| = sqrt(pi:pi) / (2 cs^2 tau rho) = sqrt(pi:pi) (1.5 / tau) / rho
     const float kS = c.cs * c.cs * (1.5f * c.inv_tau_s) * p2(-EF);
@@ -556,6 +601,33 @@ __device__ __forceinline__ CollF<L> collide_f_pre_lane(const L (&f)[Q], const Ma
     o.k1 = lfma(lbc<L>(-0.5f), o.w1, lbc<L>(1.0f));
     o.k2 = lfma(lbc<L>(-0.5f), o.w2, lbc<L>(1.0f));
     return o;
+}
+
+// The non-equilibrium parts (d0, dS, dD) and q, around given coefficients.
+template <class L, int EF = 0>
+__device__ __forceinline__ CollF<L> collide_f_parts_lane(const L (&f)[Q], const Macro<L, true>& m,
+                                                         const CollCoef<L>& k) {
+    CollF<L> o;
+    const L u = m.ux, v = m.uy, r = rho_scaled<L, EF>(m), m15u2 = m15u2_lane<L>(u, v);
+    o.d0 = d0_lane<L>(f, r, m.drho, m15u2);
+#pragma unroll
+    for (int p = 1; p <= 4; ++p) {
+        o.q[p] = q_lane<L>(p, u, v, m15u2);
+        o.dS[p] = dS_lane<L>(p, f, r, m.drho, o.q[p]);
+        o.dD[p] = dD_lane<L>(p, f, r, u, v);
+    }
+    o.nut = k.nut;
+    o.w1 = k.w1;
+    o.w2 = k.w2;
+    o.k1 = k.k1;
+    o.k2 = k.k2;
+    return o;
+}
+
+template <class L, int EF = 0>
+__device__ __forceinline__ CollF<L> collide_f_pre_lane(const L (&f)[Q], const Macro<L, true>& m,
+                                                       const StepScalars<float>& c, const L* nut_ovr) {
+    return collide_f_parts_lane<L, EF>(f, m, collide_f_coef_lane<L, EF>(f, m, c, nut_ovr));
 }
 
 // The f update with the Guo force fy = rho beta T: S+_p = w_p (-3 u_y +

@@ -37,6 +37,7 @@
 #include "diag.cuh"
 #include "kernels.cuh"
 #include "sgs.cuh"
+#include "xpair.cuh"
 
 namespace cav {
 
@@ -118,6 +119,11 @@ struct Solver {
     // set_dynamic_sgs (src/uniform/solver.rs:215-220) and the model's
     // coefficient statistics (cs_dyn_mean, cs_dyn_max, kappa_dyn_mean,
     // kappa_dyn_max) of the last step.
+    // Kernel of the fused step: 0 one node per thread (k_fused), 1 two
+    // x-adjacent nodes per thread (k_fused_x, 16-bit formats).  Both give
+    // the same bits.
+    virtual void set_step_kernel(int k) = 0;
+    virtual int step_kernel() const = 0;
     virtual void set_dynamic_sgs(bool on, double smag_alpha, double nu_sm_min, double eta_test) = 0;
     virtual void dynamic_stats(double* out4) = 0;
     bool dyn = false;
@@ -163,6 +169,10 @@ struct Impl final : Solver {
     // 2.51 with 32 x 4.
     static constexpr int BYF = std::is_same<St, float>::value ? 4 : BY;
     dim3 blk{BX, BYF}, grd{};
+    // the node-pair kernel: 32 x BYX threads cover 64 columns x BYX rows
+    static constexpr int BYX = 2;
+    dim3 blkx{BX, BYX}, grdx{};
+    int kern = is_p16<St>::value ? 1 : 0;
     // dynamic subgrid model
     double dyn_alpha = 0.5, dyn_min = -0.1, dyn_eta = 2.0;
     double* sgs_w = nullptr;       // S_NPLANES FP64 work planes
@@ -191,6 +201,7 @@ struct Impl final : Solver {
         if ((long long)NPLANES * G.plane >= (1ll << 31))
             throw ArgError{CAV_ERR_ARG, "grid too large: 18 * ny * pitch must stay below 2^31 elements"};
         grd = dim3((p.nx + BX - 1) / BX, (p.ny + BYF - 1) / BYF);
+        grdx = dim3(((p.nx + 1) / 2 + BX - 1) / BX, (p.ny + BYX - 1) / BYX);
         if (!stream) {
             CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
             own_stream = true;
@@ -386,9 +397,33 @@ struct Impl final : Solver {
         attr[0].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
+        if constexpr (is_p16<St>::value) {
+            if (kern == 1) {
+                cfg.gridDim = grdx;
+                cfg.blockDim = blkx;
+                CK(cudaLaunchKernelEx(&cfg, k_fused_x<St, WN, ACC, false>, (const St*)pop[cur], pop[cur ^ 1], fy,
+                                      nut, acc_hot, acc_cold, G, c));
+                return;
+            }
+        }
         CK(cudaLaunchKernelEx(&cfg, k_fused<St, WN, ACC, false>, (const St*)pop[cur], pop[cur ^ 1], fy, nut,
                               acc_hot, acc_cold, G, c));
     }
+
+    void set_step_kernel(int k) override {
+        if (k != 0 && k != 1) throw ArgError{CAV_ERR_ARG, "step kernel must be 0 or 1"};
+        if (k == 1 && !is_p16<St>::value)
+            throw ArgError{CAV_ERR_ARG, "the node-pair step kernel is for the 16-bit storage formats"};
+        CK(cudaStreamSynchronize(stream));
+        kern = k;
+        for (auto& row : graph)
+            for (auto& gx : row)
+                if (gx) {
+                    CK(cudaGraphExecDestroy(gx));
+                    gx = nullptr;
+                }
+    }
+    int step_kernel() const override { return kern; }
 
     void launch_fused(int64_t s, bool write_nut, bool acc, const long long* sdev = nullptr, int64_t off = 0) {
         StepScalars<A> c = scalars(s);
@@ -645,13 +680,53 @@ struct Impl final : Solver {
                 pc_form = true;
                 ref_cached = false;
                 for (int64_t j = 0; j < step_arg; ++j) {
-                    k_fused<St, false, false, true><<<grd, blk, 0, stream>>>(pop[cur], pop[cur ^ 1], fy, nut,
-                                                                            acc_hot, acc_cold, G,
-                                                                            scalars(time_step));
+                    bool done = false;
+                    if constexpr (is_p16<St>::value) {
+                        if (kern == 1) {
+                            k_fused_x<St, false, false, true><<<grdx, blkx, 0, stream>>>(
+                                pop[cur], pop[cur ^ 1], fy, nut, acc_hot, acc_cold, G, scalars(time_step));
+                            done = true;
+                        }
+                    }
+                    if (!done)
+                        k_fused<St, false, false, true><<<grd, blk, 0, stream>>>(pop[cur], pop[cur ^ 1], fy, nut,
+                                                                                acc_hot, acc_cold, G,
+                                                                                scalars(time_step));
                     check_launch();
                     cur ^= 1;
                 }
                 to_ref_form();
+                break;
+            }
+            case CAV_PHASE_CHANNEL: {
+                // step_arg steps of the fused kernel's plane-channel variant
+                // (k_fused CHANNEL), the first from the REF state by
+                // collide(step), then back to a REF state by the channel pull
+                if (step_arg < 1) throw ArgError{CAV_ERR_ARG, "the channel needs at least one step"};
+                int64_t n = step_arg;
+                if (!pc_form) {
+                    k_collide_ref<St><<<grd, blk, 0, stream>>>(pop[cur], pop[cur ^ 1], rho, ux, uy, tt, fy, nut, G,
+                                                               scalars(time_step));
+                    check_launch();
+                    cur ^= 1;
+                    pc_form = true;
+                    time_step += 1;
+                    n -= 1;
+                }
+                ref_cached = false;
+                for (int64_t j = 0; j < n; ++j) {
+                    k_fused<St, false, false, false, true><<<grd, blk, 0, stream>>>(
+                        pop[cur], pop[cur ^ 1], fy, nut, acc_hot, acc_cold, G, scalars(time_step));
+                    check_launch();
+                    cur ^= 1;
+                    time_step += 1;
+                }
+                k_materialize<St, true><<<grd, blk, 0, stream>>>(pop[cur], pop[cur ^ 1], fy, rho, ux, uy, tt, G,
+                                                                 scalars(time_step));
+                check_launch();
+                cur ^= 1;
+                pc_form = false;
+                ref_cached = false;
                 break;
             }
             default:

@@ -1,0 +1,238 @@
+// xpair.cuh -- the fused step on two x-adjacent nodes per thread (16-bit
+// population storage).
+//
+// A thread owns the nodes (ix, iy) and (ix + 1, iy), ix even.  In the SoA
+// planes (pitch a multiple of 32 elements) those two 16-bit values are one
+// aligned 32-bit word, node ix in the low half, so every plane is pulled and
+// stored as words:
+//  - directions with c_x = 0: one word load (the source pair is aligned);
+//  - c_x = +1 / -1: the two source values straddle two words; both words are
+//    loaded and one byte permute (prmt) assembles the pair, with the
+//    bounce-back / wall cases chosen by the permute selector;
+//  - the collision's results for a plane of the two nodes are rounded
+//    together by one cvt.{rn,rs}.{f16x2,bf16x2}.f32 and written by one
+//    32-bit store.
+// The macroscopic update and the collision run on Blackwell's packed FP32x2
+// add / mul / fma (the lane arithmetic of lattice.cuh): every operation is
+// explicitly rounded, so each node gets exactly the bits the one-node
+// kernels give it.  Stochastic rounding draws its bits per node pair (see
+// sr_pair_rng in kernels.cuh), the convention every uniform-solver kernel
+// follows, so a cavity stepped by either kernel is bit for bit the same.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace cav {
+
+// Register budget of the node-pair kernels.
+#ifndef XPAIR_MAXNREG
+#define XPAIR_MAXNREG 64
+#endif
+
+template <class St>
+struct PairEnc;
+
+template <int KIND, bool SRND>
+struct PairEnc<P16<KIND, SRND>> {
+    using F = Fmt<P16<KIND, SRND>>;
+    static constexpr bool SR = SRND;
+    // lane units (the formats' own power-of-two scales), as Fmt::lload
+    __device__ static float2 dec(uint32_t w, int q) {
+        if constexpr (KIND == K_BF16) {
+            return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
+        } else {
+            if (KIND == K_MIX && q >= Q)
+                return make_float2(fx_load((unsigned short)(w & 0xffffu), q), fx_load((unsigned short)(w >> 16), q));
+            return make_float2(h16_raw((unsigned short)(w & 0xffffu)), h16_raw((unsigned short)(w >> 16)));
+        }
+    }
+    // v.x -> low half (node ix), v.y -> high half (node ix + 1); r: the
+    // pair's draw for this plane (stochastic formats).
+    __device__ static uint32_t enc(float2 v, int q, uint32_t r) {
+        uint32_t d;
+        if constexpr (KIND == K_BF16) {
+            if constexpr (SRND)
+                asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(v.y), "f"(v.x), "r"(sr_bits_bf16(r)));
+            else
+                asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(v.y), "f"(v.x));
+        } else {
+            if (KIND == K_MIX && q >= Q) {
+                const uint32_t lo = fx_store(v.x, q, SRND, sr_bits_fx(r, 0));
+                const uint32_t hi = fx_store(v.y, q, SRND, sr_bits_fx(r, 1));
+                return (lo & 0xffffu) | (hi << 16);
+            }
+            if constexpr (SRND)
+                asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(v.y), "f"(v.x), "r"(sr_bits_f16(r)));
+            else
+                asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(v.y), "f"(v.x));
+        }
+        return d;
+    }
+};
+
+// Pull of the f planes of the pair (stream, src/uniform/solver.rs:838-913):
+// f_i(x) = f*_i(x - c_i) in the domain, else f*_opp(i)(x) (bounce-back).
+// Words of raw storage bits, node ix in the low half.
+template <class St>
+__device__ __forceinline__ void pull_f_x(const St* __restrict__ src, const Geom& G, int ix, int iy,
+                                         uint32_t (&w)[Q]) {
+    const uint32_t* __restrict__ s = reinterpret_cast<const uint32_t*>(src);
+    const int P2 = int(G.plane >> 1), W2 = G.pitch >> 1;
+    const int k2 = iy * W2 + (ix >> 1);
+    const bool ym = iy > 0, yp = iy < G.ny - 1;
+    const bool x0 = ix == 0;            // node ix: its c_x = +1 sources are outside
+    const bool xl = ix + 2 >= G.nx;     // node ix + 1: its c_x = -1 sources are outside
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const int cx = CX(i), cy = CY(i);
+        const bool y_ok = cy > 0 ? ym : (cy < 0 ? yp : true);
+        const int own = OPP(i) * P2 + k2;       // the pair's word of the opposite plane
+        const int srow = i * P2 + k2 - cy * W2; // word (ix, iy - c_y) of plane i
+        if (cx == 0) {
+            w[i] = s[y_ok ? srow : own];
+        } else if (cx > 0) {
+            // low half: (ix - 1) = high half of the word to the left; high
+            // half: (ix) = low half of the word above/below
+            const uint32_t w1 = s[y_ok ? srow : own];
+            const uint32_t w0 = s[(y_ok && !x0) ? srow - 1 : own];
+            w[i] = __byte_perm(w0, w1, !y_ok ? 0x7654u : (x0 ? 0x5410u : 0x5432u));
+        } else {
+            // low half: (ix + 1) = high half of the pair's word; high half:
+            // (ix + 2) = low half of the word to the right
+            const uint32_t w0 = s[y_ok ? srow : own];
+            const uint32_t w1 = s[(y_ok && !xl) ? srow + 1 : own];
+            w[i] = __byte_perm(w0, w1, !y_ok ? 0x3210u : (xl ? 0x7632u : 0x5432u));
+        }
+    }
+}
+
+// Pull of the g planes with the thermal boundary conditions
+// (src/uniform/solver.rs:951-988): rows 0 / ny-1 take the post-stream g of
+// rows 1 / ny-2; wall columns are overwritten by the caller (equilibrium of
+// the wall temperature), so their words may hold anything.
+template <class St>
+__device__ __forceinline__ void pull_g_x(const St* __restrict__ src, const Geom& G, int ix, int iy,
+                                         uint32_t (&w)[Q]) {
+    const uint32_t* __restrict__ s = reinterpret_cast<const uint32_t*>(src);
+    const int P2 = int(G.plane >> 1), W2 = G.pitch >> 1;
+    const int gy = iy == 0 ? 1 : (iy == G.ny - 1 ? G.ny - 2 : iy);
+    const int k2 = gy * W2 + (ix >> 1);
+    const bool x0 = ix == 0, xl = ix + 2 >= G.nx;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const int cx = CX(i), cy = CY(i);
+        const int srow = (Q + i) * P2 + k2 - cy * W2;
+        if (cx == 0) {
+            w[i] = s[srow];
+        } else if (cx > 0) {
+            w[i] = __byte_perm(s[x0 ? srow : srow - 1], s[srow], 0x5432u);
+        } else {
+            w[i] = __byte_perm(s[srow], s[xl ? srow : srow + 1], 0x5432u);
+        }
+    }
+}
+
+// One reference step of the nodes (ix, iy), (ix + 1, iy): the pull, the
+// macroscopic update with the Guo half force, no-slip, the collision of the
+// next step and the stores (what fused_node does for one node).  Node ix + 1
+// may lie in the row padding (odd nx): its values are computed and stored
+// into the padding, which no kernel reads as a node.
+// NO_COLLIDE: identity collision (the pulled values are stored back; checks
+// the pull / bounce-back / boundary index maps bit for bit).
+template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE = false>
+__device__ __forceinline__ void fused_xpair(const St* __restrict__ src, St* __restrict__ dst,
+                                            const float* fy_in, float* fy_out, float* __restrict__ nut,
+                                            double* __restrict__ acc_hot, double* __restrict__ acc_cold,
+                                            const Geom& G, int ix, int iy, const StepScalars<float>& c) {
+    using E = PairEnc<St>;
+    constexpr int EF = Fmt<St>::EF, EG = Fmt<St>::EG;
+    const int k0 = iy * G.pitch + ix;
+    // f first: rho, u and the f collision's coefficients need no g
+    float2 f[Q];
+    {
+        uint32_t w[Q];
+        pull_f_x<St>(src, G, ix, iy, w);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) f[i] = E::dec(w[i], i);
+    }
+    const bool wy = iy == 0 || iy == G.ny - 1;
+    const Mask2 wall{wy || ix == 0 || ix == G.nx - 1, wy || ix + 1 == G.nx - 1};
+    Macro<float2, true> m = macro_f_lane<float2, EF>(f, *reinterpret_cast<const float2*>(fy_in + k0), wall);
+    // the relaxation coefficients now; the non-equilibrium parts are formed
+    // again at the f update (same expressions, same bits), so they are not
+    // held in registers across the g half of the step
+    const CollCoef<float2> kc = collide_f_coef_lane<float2, EF>(f, m, c, nullptr);
+    float2 g[Q];
+    {
+        uint32_t w[Q];
+        pull_g_x<St>(src, G, ix, iy, w);
+        const int gy = iy == 0 ? 1 : (iy == G.ny - 1 ? G.ny - 2 : iy);
+        const bool h0 = ix == 0, c0 = ix == G.nx - 1, c1 = ix + 1 == G.nx - 1;
+        const float tw0 = (h0 ? c.t_hot[gy] : c.t_cold) * p2(EG), tw1 = c.t_cold * p2(EG);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const float2 v = E::dec(w[i], Q + i);
+            // wall columns: geq(T_wall, 0, 0) = w_i T_wall (geq_rest)
+            g[i].x = (h0 || c0) ? float(WD(i)) * tw0 : v.x;
+            g[i].y = c1 ? float(WD(i)) * tw1 : v.y;
+        }
+    }
+    m.t = sum_g<float2>(g);
+    if (!NO_COLLIDE && ACC_NU) {
+        const float t0 = m.t.x * p2(-EG), t1 = m.t.y * p2(-EG);
+        if (ix + 1 == 1) acc_hot[iy] += fabs(double(t1) - double(gather_t<St>(src, G, 2, iy, c)));
+        if (ix == G.nx - 2) acc_cold[iy] += fabs(double(t0) - double(gather_t<St>(src, G, G.nx - 3, iy, c)));
+        if (ix + 1 == G.nx - 2) acc_cold[iy] += fabs(double(t1) - double(gather_t<St>(src, G, G.nx - 3, iy, c)));
+    }
+    // g collided and stored first (its registers free), then the f update;
+    // stores: one word per plane, the draws in plane order 0..17
+    uint32_t* __restrict__ d = reinterpret_cast<uint32_t*>(dst);
+    const int P2 = int(G.plane >> 1), k2 = k0 >> 1;
+    if (!NO_COLLIDE) {
+        float2 qv[5];
+        const float2 m15u2 = m15u2_lane<float2>(m.ux, m.uy);
+#pragma unroll
+        for (int p = 1; p <= 4; ++p) qv[p] = q_lane<float2>(p, m.ux, m.uy, m15u2);
+        collide_g_lane<float2>(g, m.t, m.ux, m.uy, kc.nut, qv, c, nullptr);
+    }
+    if constexpr (E::SR) {
+        NodeRng rng = sr_pair_rng(c, G, ix, iy);
+        rng.skip<Q>();  // the f planes' draws come first
+#pragma unroll
+        for (int q = 0; q < Q; ++q) d[(Q + q) * P2 + k2] = E::enc(g[q], Q + q, rng.next());
+    } else {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) d[(Q + q) * P2 + k2] = E::enc(g[q], Q + q, 0u);
+    }
+    if (!NO_COLLIDE) {
+        const CollF<float2> o = collide_f_parts_lane<float2, EF>(f, m, kc);
+        const float2 fyv = collide_f_post_lane<float2, EF, EG>(f, o, m, c, m.t);
+        *reinterpret_cast<float2*>(fy_out + k0) = fyv;
+        if (WRITE_NUT) *reinterpret_cast<float2*>(nut + k0) = kc.nut;
+    }
+    if constexpr (E::SR) {
+        NodeRng rng = sr_pair_rng(c, G, ix, iy);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) d[q * P2 + k2] = E::enc(f[q], q, rng.next());
+    } else {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) d[q * P2 + k2] = E::enc(f[q], q, 0u);
+    }
+}
+
+// The single-cavity step on node pairs: 32 x BY threads cover 64 columns x
+// BY rows.
+template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE>
+__global__ void __launch_bounds__(256) k_fused_x(const St* __restrict__ src, St* __restrict__ dst,
+                                                 float* __restrict__ fy, float* __restrict__ nut,
+                                                 double* __restrict__ acc_hot, double* __restrict__ acc_cold, Geom G,
+                                                 StepScalars<float> c) {
+    pdl_wait();
+    pdl_trigger();
+    const int ix = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= G.nx || iy >= G.ny) return;
+    fused_xpair<St, WRITE_NUT, ACC_NU, NO_COLLIDE>(src, dst, fy, fy, nut, acc_hot, acc_cold, G, ix, iy, c);
+}
+
+}  // namespace cav

@@ -163,6 +163,16 @@ class CavitySolver:
         self._ck(L.load().cav_get_stream(self._h, ctypes.byref(s)))
         return s.value or 0
 
+    def set_step_kernel(self, kernel):
+        """Kernel of the fused step: 0 one node per thread, 1 two x-adjacent
+        nodes per thread (16-bit formats, their default); same bits."""
+        self._ck(L.load().cav_set_step_kernel(self._h, int(kernel)))
+
+    def step_kernel(self):
+        k = ctypes.c_int32()
+        self._ck(L.load().cav_get_step_kernel(self._h, ctypes.byref(k)))
+        return k.value
+
     def launch_count(self):
         n = ctypes.c_int64()
         self._ck(L.load().cav_launch_count(self._h, ctypes.byref(n)))

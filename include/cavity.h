@@ -6,7 +6,7 @@
  * FFI of its own.  Each entry point below replaces one method of that type,
  * or one direct field access its callers make, and names the reference
  * interface it stands for.  A Rust caller binds them with `extern "C"`
- * (see INTEGRATION.md).
+ * declarations of the same names and #[repr(C)] mirrors of the structs.
  *
  * Conventions
  *  - Every function returns an int status (CAV_OK = 0) and never aborts or
@@ -74,6 +74,15 @@ extern "C" {
  * the streaming / bounce-back / thermal-BC index maps of the production
  * kernel against stream() + apply_thermal_boundary_conditions() bit for bit. */
 #define CAV_PHASE_FUSED_IDENTITY 6
+/* step_arg steps of the fused step kernel's plane-channel variant: periodic
+ * in y, bounce-back walls at x = 0 and nx-1 without the wall-velocity
+ * override or thermal boundary conditions, body force rho * beta_eff along
+ * +y in the TRT + Guo collision (Cs from the parameters), then the REF state
+ * of the channel.  The reference's Poiseuille test of the forcing
+ * (src/uniform/tests.rs:246-376) turned by 90 degrees; start it from
+ * init_from_fields with rho = 1, u = 0, T = 1 (the first collision's force
+ * is rho * beta_eff * T). */
+#define CAV_PHASE_CHANNEL 7
 
 /* ---- parameters ------------------------------------------------------------ */
 /* Arguments of CavitySolver::new (src/uniform/solver.rs:108) plus the
@@ -183,6 +192,14 @@ int cav_get_stream(cav_handle* h, void** stream);
 /* Number of kernels the handle has launched so far (graph replays count
  * every kernel they contain; no counterpart in the reference). */
 int cav_launch_count(cav_handle* h, int64_t* n);
+/* Kernel of the fused step (no counterpart in the reference):
+ * CAV_STEP_NODE one node per thread; CAV_STEP_PAIR two x-adjacent nodes per
+ * thread, each plane one 32-bit word (16-bit formats only, their default).
+ * Both give the same bits; CAV_ERR_ARG for a pair kernel on FP64 / FP32. */
+#define CAV_STEP_NODE 0
+#define CAV_STEP_PAIR 1
+int cav_set_step_kernel(cav_handle* h, int32_t kernel);
+int cav_get_step_kernel(cav_handle* h, int32_t* kernel);
 
 /* ---- snapshots and restart ------------------------------------------------ */
 /* CAVSNAP1 files of the reference (src/uniform/snapshot.rs:10-131): rho, ux,
@@ -249,16 +266,23 @@ int cav_adjoint_run(cav_handle* h, const cav_adjoint_spec* spec, double* grad_th
  * share one precision and one device.  Each cavity of a batch evolves
  * bit-identically to the same cavity created with cav_create. */
 typedef struct cav_batch cav_batch;
+/* kernel and the fields it uses (the others are ignored):
+ *   0  persistent grid of ctas_per_sm x #SMs CTAs over 32-column x
+ *      rows_per_item tiles, one thread per node;
+ *   1, 2  TMA-staged shared-memory tiles in shape 1 or 2 (taller),
+ *      ctas_per_sm persistent CTAs per SM (at most its resident CTAs);
+ *   3  one CTA per 32-column x rows_per_item item (1, 2, 4 or 8 rows), one
+ *      thread per node;
+ *   4  the same items, two rows per thread on packed FP32x2 arithmetic
+ *      (2, 4 or 8 rows; FP64 runs it as 3);
+ *   5  one CTA per 64-column x rows_per_item item (1, 2, 4 or 8 rows), two
+ *      x-adjacent nodes per thread, each plane one 32-bit word (16-bit
+ *      formats; FP64 and FP32 run it as 3).
+ * Default: kernel 3, 4 rows. */
 typedef struct cav_batch_tuning {
-    int32_t rows_per_item; /* tile height of k_batch (tiles are 32 columns wide) */
-    int32_t ctas_per_sm;   /* persistent grid = ctas_per_sm x #SMs CTAs (the tile
-                              kernel: at most its resident CTAs per SM)          */
-    int32_t kernel;        /* 0: persistent, one thread per node from global
-                              memory; 1, 2: TMA-staged shared-memory tiles in
-                              shape 1 or 2 (taller); 3: one CTA per 32 x 4 item,
-                              one thread per node; 4: the same items, two nodes
-                              per thread on packed FP32x2 arithmetic (default;
-                              FP64 batches run it as 3)                          */
+    int32_t rows_per_item; /* item / tile height in rows                     */
+    int32_t ctas_per_sm;   /* resident CTAs per SM of the persistent kernels */
+    int32_t kernel;        /* 0..5, above                                    */
 } cav_batch_tuning;
 int cav_batch_create(const cav_params* params, int32_t n, cav_batch** out);
 int cav_batch_destroy(cav_batch* b);
@@ -421,9 +445,12 @@ int cav_octree_get_nu_t(cav_octree* h, int32_t level, double* nu_t, double* alph
  *  - Output: out, a device pointer to 11 doubles in the field order of
  *    cav_diag_out, the last being 1.0 when every field is finite (else 0.0).
  *  - Runs asynchronously on `stream` (a cudaStream_t; NULL = default stream).
- *  - The first call on a device (with that device current) looks up the
- *    scratch's device address; make that first call before any stream
- *    capture on that device.
+ *  - Every call looks up the scratch's device address on the current device
+ *    (nothing is cached, so a device reset between calls is harmless); the
+ *    first call on a device may load the library's device code there, so
+ *    make that first call before any stream capture on that device.
+ *  - A CUDA error already pending when the call starts is returned as
+ *    CAV_ERR_CUDA without launching, and left pending for the caller.
  *  - All calls on a device share the scratch: calls whose kernels can overlap
  *    on the GPU race on it, so order them (same stream, or an event).
  * Rejections return CAV_ERR_ARG / CAV_ERR_CUDA and print one line on stderr. */

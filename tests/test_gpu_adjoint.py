@@ -65,7 +65,64 @@ def test_adjoint_state_checks():
     assert e.value.code == L.CAV_ERR_ARG
 
 
+MID = dict(nx=64, ny=256, ra=1e7, cs=0.1, n=5000, ws=2501, ck=500)
+
+
+@pytest.mark.parametrize("precision,tol", [("f64", 1e-8), ("f32", 1e-3)])
+def test_adjoint_mid_size_matches_tangent_linear_oracle(precision, tol):
+    """A mid-size case against the FP64 tangent-linear oracle: 64x256,
+    Ra = 1e7, theta = 0 + 1e-4 noise (the benchmark initial field), 5000
+    steps, J over steps 2501-5000, checkpoints every 500 (ten segments); a
+    random direction in (theta profile, Cs).  FP64 adjoint within 1e-8
+    relative, FP32 within 1e-3."""
+    import os
+
+    c = MID
+    th = profile(c["ny"], seed=11)
+    kw = dict(init_mode=L.CAV_INIT_ZERO, noise_amp=1e-4, t_hot_profile=th)
+    s = CavitySolver(c["nx"], c["ny"], c["ra"], 0.71, c["cs"], 0.9, 0.02, 42, precision=precision, **kw)
+    J, gth, gcs, info = s.adjoint_nusselt(c["n"], c["ws"], c["ck"])
+    assert info["checkpoints"] == -(-(c["n"] - 1) // c["ck"])
+    rng = np.random.default_rng(5)
+    v = rng.standard_normal(c["ny"])
+    dcs = float(rng.standard_normal())
+    Jo, dJo = oracle.tangent_nusselt(c["nx"], c["ny"], c["ra"], 0.71, c["cs"], 0.9, 0.02, 42, c["n"], c["ws"],
+                                     dtheta=v, dcs=dcs, jobs=max(1, os.cpu_count() or 1), **kw)
+    adj = float(np.dot(gth, v) + gcs * dcs)
+    assert abs(J - Jo) <= (1e-12 if precision == "f64" else 1e-5) * abs(Jo)
+    assert abs(adj - dJo) <= tol * abs(dJo), (adj, dJo)
+
+
 C4 = dict(nx=96, ny=384, ra=1e7, cs=0.1, n=60_000, ws=40_001, ck=500)
+
+
+def test_adjoint_c4_fp32_gradient_matches_fp64_adjoint_in_every_component():
+    """The C4 gradient (96x384, Ra = 1e7, 60 000 steps, J over 40 001-60 000,
+    checkpoints every 500) of the FP32 adjoint against the FP64 adjoint (the
+    one that matches the tangent-linear oracle to 1e-8) in all 385
+    components: the 384 hot-wall theta values and Cs.  Tolerances: 1e-3
+    relative on the gradient's norm and on dJ/dCs; per theta component
+    1e-3 of its own size plus 1e-4 of the gradient's RMS (components that
+    are almost zero, the wall rows, are judged on the RMS scale)."""
+    c = C4
+    th = profile(c["ny"])
+    out = {}
+    for prec in ("f64", "f32"):
+        s = CavitySolver(c["nx"], c["ny"], c["ra"], 0.71, c["cs"], 0.9, 0.02, 42, precision=prec,
+                         t_hot_profile=th, init_mode=L.CAV_INIT_ZERO, noise_amp=1e-4)
+        out[prec] = s.adjoint_nusselt(c["n"], c["ws"], c["ck"])
+        s.close()
+    J64, g64, cs64, _ = out["f64"]
+    J32, g32, cs32, _ = out["f32"]
+    rms = float(np.sqrt(np.mean(g64 ** 2)))
+    err = np.abs(g32 - g64)
+    print(f"C4 FP32 vs FP64 adjoint: |dg|/|g| {np.linalg.norm(g32 - g64) / np.linalg.norm(g64):.3e}, "
+          f"max component error / (|g_i| + 0.1 rms) {np.max(err / (np.abs(g64) + 0.1 * rms)):.3e}, "
+          f"dJ/dCs {cs32:.6e} vs {cs64:.6e}")
+    assert abs(J32 - J64) <= 1e-4 * abs(J64)
+    assert np.linalg.norm(g32 - g64) <= 1e-3 * np.linalg.norm(g64)
+    assert np.all(err <= 1e-3 * np.abs(g64) + 1e-4 * rms), int(np.argmax(err - 1e-3 * np.abs(g64)))
+    assert abs(cs32 - cs64) <= 1e-3 * abs(cs64)
 
 
 def _j_fp64(th, cs):

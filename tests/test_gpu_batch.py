@@ -23,9 +23,13 @@ def single(c, precision):
                         precision=precision, init_mode=L.CAV_INIT_ZERO, noise_amp=1e-4)
 
 
-@pytest.mark.parametrize("precision", ["f64", "f32", "f16sr", "f16gsr"])
-def test_batch_is_bitwise_equal_to_single_cavities(precision):
+@pytest.mark.parametrize("precision,kernel", [("f64", 3), ("f32", 3), ("f32", 4), ("f16sr", 3), ("f16sr", 5),
+                                              ("f16gsr", 5), ("bf16sr", 5), ("f16", 5)])
+def test_batch_is_bitwise_equal_to_single_cavities(precision, kernel):
+    """Every cavity of the batch against the same cavity created alone (its
+    default single-cavity kernel: node pairs for the 16-bit formats)."""
     b = CavityBatch(MIXED, precision=precision)
+    b.set_tuning(4, 8, kernel=kernel)
     singles = [single(c, precision) for c in MIXED]
     for n in (1, 150, 137):  # spin-up steps (table rows), graph replays, remainders
         b.step(n)
@@ -51,12 +55,16 @@ def test_batch_tuning_does_not_change_results(precision):
     b.set_tuning(32, 16, kernel=1)
     a.step(90)
     b.step(40)
-    b.set_tuning(5, 7, kernel=3)
+    b.set_tuning(2, 7, kernel=3)
     b.step(20)
     b.set_tuning(5, 1, kernel=2)
     b.step(15)
-    b.set_tuning(5, 1, kernel=4)
-    b.step(15)
+    b.set_tuning(8, 1, kernel=4)
+    b.step(5)
+    b.set_tuning(1, 1, kernel=5)
+    b.step(5)
+    b.set_tuning(8, 1, kernel=5)
+    b.step(5)
     for i in range(len(MIXED)):
         fa, fb = a.fields(i), b.fields(i)
         for k in fa:
@@ -71,16 +79,26 @@ def test_autotune_picks_a_candidate_and_leaves_the_state_alone():
     b.step(10)
     ref.step(10)
     t = b.autotune(trial_steps=16)
-    assert t["kernel"] in (0, 1, 2, 3, 4)
+    assert t["kernel"] in (0, 1, 2, 3, 4, 5)
     if t["kernel"] == 0:
-        assert t["rows_per_item"] in (2, 4, 8, 16, 32) and t["ctas_per_sm"] in (4, 8, 12, 16)
+        assert t["rows_per_item"] in (4, 8, 16) and t["ctas_per_sm"] in (4, 8, 16)
     elif t["kernel"] in (1, 2):
-        assert t["ctas_per_sm"] in (1, 2, 3, 4)
+        assert set(t) == {"kernel", "ctas_per_sm"} and t["ctas_per_sm"] in (1, 2, 3, 4)
+    else:
+        assert set(t) == {"kernel", "rows_per_item"} and t["rows_per_item"] in (1, 2, 4, 8)
     assert b.tuning() == t
     assert b.info()["time_step"] == 10
     b.step(70)
     ref.step(70)
     assert np.array_equal(b.fields(1)["temperature"], ref.fields(1)["temperature"])
+
+
+def test_item_heights_outside_a_kernels_range_are_rejected():
+    b = CavityBatch(MIXED[:2], precision="f16sr")
+    for rows, kernel in ((3, 3), (16, 5), (1, 4)):
+        with pytest.raises(L.CavError) as e:
+            b.set_tuning(rows, 8, kernel=kernel)
+        assert e.value.code == L.CAV_ERR_ARG
 
 
 def test_sweep_batch_runs_and_conserves_mass():

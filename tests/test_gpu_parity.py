@@ -25,10 +25,11 @@ GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
 
 def pair(nx, ny, ra, *, precision="f64", cs=0.1, init_mode=0, noise=1e-3, nu=None, seed=42,
-         t_hot=None, utarget=0.02, t_cold=-0.5):
+         t_hot=None, utarget=0.02, t_cold=-0.5, alpha_mult=1.0, nu_start_mult=1.0):
     kw = dict(init_mode=init_mode, noise_amp=noise, t_hot_profile=t_hot, t_cold=t_cold)
-    o = oracle.OracleSolver(nx, ny, ra, 0.71, cs, 0.9, utarget, seed, 4, 1.0, 1.0, nu, **kw)
-    g = CavitySolver(nx, ny, ra, 0.71, cs, 0.9, utarget, seed, 1, 1.0, 1.0, nu, precision=precision, **kw)
+    o = oracle.OracleSolver(nx, ny, ra, 0.71, cs, 0.9, utarget, seed, 4, alpha_mult, nu_start_mult, nu, **kw)
+    g = CavitySolver(nx, ny, ra, 0.71, cs, 0.9, utarget, seed, 1, alpha_mult, nu_start_mult, nu,
+                     precision=precision, **kw)
     return o, g
 
 
@@ -52,21 +53,28 @@ def assert_same_state(o, g, tol=0.0):
 ALL_FORMATS = ["f64", "f32", "f16", "bf16", "f16g", "f16sr", "bf16sr", "f16gsr"]
 
 
-@pytest.mark.parametrize("precision", ALL_FORMATS)
+P16_FORMATS = ["f16", "bf16", "f16g", "f16sr", "bf16sr", "f16gsr"]
+MAP_CASES = [(p, 0) for p in ALL_FORMATS] + [(p, 1) for p in P16_FORMATS]
+
+
+@pytest.mark.parametrize("precision,step_kernel", MAP_CASES)
 @pytest.mark.parametrize("shape", [(16, 40), (37, 23), (5, 4)])
-def test_stream_bounce_back_bc_index_maps_bitexact(precision, shape):
+def test_stream_bounce_back_bc_index_maps_bitexact(precision, step_kernel, shape):
     """The fused kernel's pull/bounce-back/thermal-BC maps against the
     reference's stream() + apply_thermal_boundary_conditions(), bit for bit.
     Random populations are first rounded through the storage format (read
     back from the device), so every later value is a moved copy.  The wall
     g values are computed (geq of the wall temperature) in the storage's
     arithmetic and then stream inwards; for the reduced formats the walls
-    are set to theta = 0 so that those values are exact too."""
+    are set to theta = 0 so that those values are exact too.  step_kernel 1:
+    the node-pair kernel (word loads assembled by byte permutes; odd nx puts
+    the last pair's second node in the row padding)."""
     nx, ny = shape
     if precision == "f64":
         o, g = pair(nx, ny, 1e5, precision=precision)
     else:
         o, g = pair(nx, ny, 1e5, precision=precision, t_hot=np.zeros(ny), t_cold=0.0)
+    g.set_step_kernel(step_kernel)
     rng = np.random.default_rng(nx * 1000 + ny)
     n = nx * ny
     f = 0.11 + 0.01 * rng.standard_normal((n, 9))
@@ -119,6 +127,69 @@ def test_fp64_fields_after_1000_steps(cfg):
     fo, fg = o.fields(), g.fields()
     assert np.array_equal(fo["temperature"], fg["temperature"])
     assert np.array_equal(fo["nu_t"], fg["nu_t"])
+
+
+@pytest.mark.parametrize("precision", P16_FORMATS)
+@pytest.mark.parametrize("shape", [(64, 256), (37, 61), (6, 9)])
+def test_node_pair_and_one_node_kernels_give_the_same_bits(precision, shape):
+    """The node-pair step kernel (two x-adjacent nodes per thread, packed
+    FP32x2 arithmetic, one rounding instruction and one 32-bit store per
+    plane pair) against the one-node kernel: every field and population
+    identical after the spin-up ramp and graph replays, stochastic rounding
+    included (both draw per node pair)."""
+    nx, ny = shape
+    a = CavitySolver(nx, ny, 1e7, 0.71, 0.1, 0.9, 0.02, 11, precision=precision)
+    b = CavitySolver(nx, ny, 1e7, 0.71, 0.1, 0.9, 0.02, 11, precision=precision)
+    assert a.step_kernel() == L.CAV_STEP_PAIR
+    b.set_step_kernel(L.CAV_STEP_NODE)
+    a.nu_accumulate(True)
+    b.nu_accumulate(True)
+    for n in (1, 250, 77):
+        a.step(n)
+        b.step(n)
+    fa, fb = a.fields(), b.fields()
+    for k in fa:
+        assert np.array_equal(fa[k], fb[k]), k
+    pa, pb = a.populations(), b.populations()
+    assert np.array_equal(pa[0], pb[0]) and np.array_equal(pa[1], pb[1])
+    assert a.nu_accumulated() == b.nu_accumulated()
+
+
+def test_node_pair_kernel_is_refused_for_fp64_and_fp32():
+    for prec in ("f64", "f32"):
+        s = CavitySolver(16, 40, 1e5, 0.71, 0.1, 0.9, 0.02, 1, precision=prec)
+        assert s.step_kernel() == L.CAV_STEP_NODE
+        with pytest.raises(L.CavError) as e:
+            s.set_step_kernel(L.CAV_STEP_PAIR)
+        assert e.value.code == L.CAV_ERR_ARG
+
+
+@pytest.mark.parametrize("nu_start_mult", [2.5, 10.0])
+def test_fp64_viscosity_ramp_and_alpha_mult_bitexact(nu_start_mult):
+    """ramp_nu_alpha (src/uniform/solver.rs:390-410) with nu_start_mult > 1,
+    and alpha = alpha_phys * alpha_mult with alpha_mult = 1.2 (:137-138), the
+    multiplier of the reference's Ra = 1e8 anchor run: FP64 fields and
+    populations bit-identical to the oracle at the ramp's start, middle and
+    end (spin-up S = 200 steps at ny = 64) and 100 steps past it; the ramped
+    scalars the host hands the kernels are the oracle's, and the ramp is
+    taken as CUDA-graph replays as well as single launches."""
+    o, g = pair(24, 64, 1e7, alpha_mult=1.2, nu_start_mult=nu_start_mult)
+    io, ig = o.info(), g.info()
+    assert ig["spin_up_steps"] == io["spin_up_steps"] == 200
+    for k in ("nu", "alpha", "alpha_phys", "beta_eff", "tau", "tau_t"):
+        assert ig[k] == io[k], k
+    assert ig["alpha"] == ig["alpha_phys"] * 1.2
+    for n in (1, 99, 100, 100):  # after steps 1, 100 (mid-ramp), 200 (end), 300
+        o.step(n)
+        g.step(n)
+        assert_same_state(o, g, 0.0)
+    # FP32 arithmetic follows the same ramp (within the FP32 tolerances)
+    o32, g32 = pair(24, 64, 1e7, precision="f32", alpha_mult=1.2, nu_start_mult=nu_start_mult)
+    o32.step(300)
+    g32.step(300)
+    fo, fg = o32.fields(), g32.fields()
+    assert np.max(np.abs(fg["temperature"] - fo["temperature"])) <= 2e-5
+    assert np.max(np.abs(fg["rho"] - fo["rho"])) <= 1e-6
 
 
 @pytest.mark.parametrize("precision", ["f64", "f16sr", "f16gsr"])

@@ -45,13 +45,13 @@ def _device_state(s, torch):
     return dev
 
 
-def _call(fn, dev, s, out, torch):
+def _call(fn, dev, s, out, torch, stream=None):
     info = s.info()
-    stream = torch.cuda.current_stream().cuda_stream
+    st = stream if stream is not None else torch.cuda.current_stream()
     rc = fn(dev["rho"].data_ptr(), dev["ux"].data_ptr(), dev["uy"].data_ptr(),
             dev["temperature"].data_ptr(), dev["nu_t"].data_ptr(), dev["f"].data_ptr(),
-            s.nx(), s.ny(), info["nu"], info["lz"], out.data_ptr(), stream)
-    torch.cuda.synchronize()
+            s.nx(), s.ny(), info["nu"], info["lz"], out.data_ptr(), st.cuda_stream)
+    st.synchronize()
     return rc, out.cpu().numpy().copy()
 
 
@@ -97,3 +97,20 @@ def test_noalloc_rejects_more_rows_than_its_scratch():
     assert rc == L.CAV_ERR_ARG
     rc = fn(p, p, p, p, p, p, 4, 3, 0.01, 2.0, p, None)
     assert rc == L.CAV_ERR_ARG
+
+
+def test_noalloc_at_the_row_limit_on_a_side_stream():
+    """ny equal to the scratch's row count (its last row in use), on a
+    caller-created stream rather than the default one."""
+    torch = pytest.importorskip("torch")
+    fn = _fn()
+    s = CavitySolver(4, MAX_ROWS, 1e6, 0.71, 0.1, 0.9, 0.02, 7, precision="f64")
+    s.step(40)
+    dev = _device_state(s, torch)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        out = torch.full((11,), float("nan"), dtype=torch.float64, device="cuda")
+        rc, vals = _call(fn, dev, s, out, torch, stream=side)
+    assert rc == L.CAV_OK
+    _check(vals, s.diag())
