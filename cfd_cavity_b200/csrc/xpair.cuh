@@ -81,6 +81,7 @@ __device__ __forceinline__ void pull_f_x(const St* __restrict__ src, const Geom&
     const int k2 = iy * W2 + (ix >> 1);
     const bool ym = iy > 0, yp = iy < G.ny - 1;
     const bool x0 = ix == 0;            // node ix: its c_x = +1 sources are outside
+    const bool xe = ix + 1 >= G.nx;     // node ix (the last column, odd nx): its c_x = -1 sources are outside
     const bool xl = ix + 2 >= G.nx;     // node ix + 1: its c_x = -1 sources are outside
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
@@ -98,10 +99,12 @@ __device__ __forceinline__ void pull_f_x(const St* __restrict__ src, const Geom&
             w[i] = __byte_perm(w0, w1, !y_ok ? 0x7654u : (x0 ? 0x5410u : 0x5432u));
         } else {
             // low half: (ix + 1) = high half of the pair's word; high half:
-            // (ix + 2) = low half of the word to the right
-            const uint32_t w0 = s[y_ok ? srow : own];
+            // (ix + 2) = low half of the word to the right; where a source
+            // is outside, the opposite plane's value at the node itself
+            // (the pair's own word: low half for ix, high half for ix + 1)
+            const uint32_t w0 = s[(y_ok && !xe) ? srow : own];
             const uint32_t w1 = s[(y_ok && !xl) ? srow + 1 : own];
-            w[i] = __byte_perm(w0, w1, !y_ok ? 0x3210u : (xl ? 0x7632u : 0x5432u));
+            w[i] = __byte_perm(w0, w1, (!y_ok || xe) ? 0x3210u : (xl ? 0x7632u : 0x5432u));
         }
     }
 }
