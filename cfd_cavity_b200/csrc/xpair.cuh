@@ -26,8 +26,22 @@ namespace cav {
 
 // Register budget of the node-pair kernels.
 #ifndef XPAIR_MAXNREG
-#define XPAIR_MAXNREG 64
+#define XPAIR_MAXNREG 96
 #endif
+#ifndef XPAIR_EARLY_G
+#define XPAIR_EARLY_G 0
+#endif
+#ifndef XPAIR_REDECODE_F
+#define XPAIR_REDECODE_F 0
+#endif
+
+// The value itself, opaque to the compiler: a decode of it is not merged
+// with an earlier decode of the same word (so the decoded values need not
+// stay live in between).
+__device__ __forceinline__ uint32_t opaque_u32(uint32_t x) {
+    asm volatile("mov.b32 %0, %1;" : "=r"(x) : "r"(x));
+    return x;
+}
 
 template <class St>
 struct PairEnc;
@@ -152,12 +166,13 @@ __device__ __forceinline__ void fused_xpair(const St* __restrict__ src, St* __re
     const int k0 = iy * G.pitch + ix;
     // f first: rho, u and the f collision's coefficients need no g
     float2 f[Q];
-    {
-        uint32_t w[Q];
-        pull_f_x<St>(src, G, ix, iy, w);
+    uint32_t wg[Q], wf[Q];
+    pull_f_x<St>(src, G, ix, iy, wf);
+#if XPAIR_EARLY_G
+    pull_g_x<St>(src, G, ix, iy, wg);
+#endif
 #pragma unroll
-        for (int i = 0; i < Q; ++i) f[i] = E::dec(w[i], i);
-    }
+    for (int i = 0; i < Q; ++i) f[i] = E::dec(wf[i], i);
     const bool wy = iy == 0 || iy == G.ny - 1;
     const Mask2 wall{wy || ix == 0 || ix == G.nx - 1, wy || ix + 1 == G.nx - 1};
     Macro<float2, true> m = macro_f_lane<float2, EF>(f, *reinterpret_cast<const float2*>(fy_in + k0), wall);
@@ -167,8 +182,10 @@ __device__ __forceinline__ void fused_xpair(const St* __restrict__ src, St* __re
     const CollCoef<float2> kc = collide_f_coef_lane<float2, EF>(f, m, c, nullptr);
     float2 g[Q];
     {
-        uint32_t w[Q];
-        pull_g_x<St>(src, G, ix, iy, w);
+#if !XPAIR_EARLY_G
+        pull_g_x<St>(src, G, ix, iy, wg);
+#endif
+        const uint32_t(&w)[Q] = wg;
         const int gy = iy == 0 ? 1 : (iy == G.ny - 1 ? G.ny - 2 : iy);
         const bool h0 = ix == 0, c0 = ix == G.nx - 1, c1 = ix + 1 == G.nx - 1;
         const float tw0 = (h0 ? c.t_hot[gy] : c.t_cold) * p2(EG), tw1 = c.t_cold * p2(EG);
@@ -208,6 +225,12 @@ __device__ __forceinline__ void fused_xpair(const St* __restrict__ src, St* __re
         for (int q = 0; q < Q; ++q) d[(Q + q) * P2 + k2] = E::enc(g[q], Q + q, 0u);
     }
     if (!NO_COLLIDE) {
+#if XPAIR_REDECODE_F
+        // f again from its words (the decoded values were not kept alive
+        // across the g half)
+#pragma unroll
+        for (int i = 0; i < Q; ++i) f[i] = E::dec(opaque_u32(wf[i]), i);
+#endif
         const CollF<float2> o = collide_f_parts_lane<float2, EF>(f, m, kc);
         const float2 fyv = collide_f_post_lane<float2, EF, EG>(f, o, m, c, m.t);
         *reinterpret_cast<float2*>(fy_out + k0) = fyv;

@@ -74,7 +74,7 @@ def test_adjoint_mid_size_matches_tangent_linear_oracle(precision, tol):
     Ra = 1e7, theta = 0 + 1e-4 noise (the benchmark initial field), 5000
     steps, J over steps 2501-5000, checkpoints every 500 (ten segments); a
     random direction in (theta profile, Cs).  FP64 adjoint within 1e-8
-    relative, FP32 within 1e-3."""
+    relative, FP32 within 1e-3 (J itself: 1e-12 / 1e-4)."""
     import os
 
     c = MID
@@ -89,7 +89,8 @@ def test_adjoint_mid_size_matches_tangent_linear_oracle(precision, tol):
     Jo, dJo = oracle.tangent_nusselt(c["nx"], c["ny"], c["ra"], 0.71, c["cs"], 0.9, 0.02, 42, c["n"], c["ws"],
                                      dtheta=v, dcs=dcs, jobs=max(1, os.cpu_count() or 1), **kw)
     adj = float(np.dot(gth, v) + gcs * dcs)
-    assert abs(J - Jo) <= (1e-12 if precision == "f64" else 1e-5) * abs(Jo)
+    # J: FP64 to 1e-12; FP32 arithmetic over 5000 steps at Ra = 1e7 to 1e-4
+    assert abs(J - Jo) <= (1e-12 if precision == "f64" else 1e-4) * abs(Jo), (J, Jo)
     assert abs(adj - dJo) <= tol * abs(dJo), (adj, dJo)
 
 
