@@ -435,9 +435,9 @@ def main():
     ap.add_argument("--batch-only", default="", metavar="PRECISION",
                     help="only time the 64-cavity batched sweep in PRECISION for --steps lattice steps "
                          "(profiling runs); --batch-kernel selects the kernel")
-    ap.add_argument("--batch-kernel", type=int, default=5, choices=[0, 1, 2, 3, 4, 5])
+    ap.add_argument("--batch-kernel", type=int, default=6, choices=[0, 1, 2, 3, 4, 5, 6])
     ap.add_argument("--batch-rows", type=int, default=4,
-                    help="tile / item height of --batch-only (kernels 3 and 5: 1, 2, 4 or 8)")
+                    help="tile / item height of --batch-only (kernels 3 and 5: 1, 2, 4 or 8; 6: 4 or 8)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.octree_only:

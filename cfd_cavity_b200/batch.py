@@ -133,6 +133,8 @@ class CavityBatch:
             return {"kernel": 0, "rows_per_item": t.rows_per_item, "ctas_per_sm": t.ctas_per_sm}
         if k in (1, 2):
             return {"kernel": k, "ctas_per_sm": t.ctas_per_sm}
+        if k == 6:
+            return {"kernel": 6, "rows_per_item": t.rows_per_item, "ctas_per_sm": t.ctas_per_sm}
         return {"kernel": k, "rows_per_item": t.rows_per_item}
 
     def tuning(self):
@@ -148,7 +150,9 @@ class CavityBatch:
         node per thread (1, 2, 4 or 8 rows); 4: the same items, two rows per
         thread on packed FP32x2 arithmetic (2, 4 or 8 rows); 5: one CTA per
         64-column x rows_per_item item, two x-adjacent nodes per thread
-        (16-bit formats; 1, 2, 4 or 8 rows)."""
+        (16-bit formats; 1, 2, 4 or 8 rows); 6: the node-pair body on
+        TMA-staged tiles of 64 columns x rows_per_item rows (4 or 8),
+        ctas_per_sm persistent CTAs per SM (16-bit formats)."""
         t = L.CavBatchTuning(rows_per_item, ctas_per_sm, int(kernel))
         self._ck(L.load().cav_batch_set_tuning(self._b, ctypes.byref(t)))
 

@@ -17,6 +17,7 @@
 
 #include "solver.cuh"
 #include "tile.cuh"
+#include "tilex.cuh"
 #include "xpair.cuh"
 
 namespace cav {
@@ -157,9 +158,12 @@ __global__ void __maxnreg__(XPAIR_MAXNREG)
 //                   lanes (rows_per_item in {2, 4, 8}; FP32-arithmetic formats);
 //   5  k_batch_x    one CTA per 64-column x rows_per_item item (rows_per_item
 //                   in {1, 2, 4, 8}), two x-adjacent nodes per thread, every
-//                   plane one 32-bit word (16-bit formats).
-// A kernel a format has no version of runs as kernel 3 (FP64: 4 and 5; FP32:
-// 5).  Parameters a kernel does not use are ignored.
+//                   plane one 32-bit word (16-bit formats);
+//   6  k_tile_x     the node-pair body on TMA-staged shared-memory tiles of
+//                   64 columns x rows_per_item rows (4 or 8), ctas_per_sm
+//                   persistent CTAs per SM (16-bit formats).
+// A kernel a format has no version of runs as kernel 3 (FP64: 4, 5 and 6;
+// FP32: 5 and 6).  Parameters a kernel does not use are ignored.
 struct BatchTuning {
     int rows_per_item = 4;
     int ctas_per_sm = 8;
@@ -198,6 +202,10 @@ struct Batch final : BatchBase {
     // the tile kernel (tile.cuh)
     TileCav<St>* d_tcavs = nullptr;
     CUtensorMap* d_maps[3] = {nullptr, nullptr, nullptr};   // per tile shape
+    // the node-pair tile kernel: tensor maps and tile lists per tile height (4, 8)
+    CUtensorMap* d_xmaps[2] = {nullptr, nullptr};
+    TileItem* d_xitems[2] = {nullptr, nullptr};
+    int n_xitems[2] = {0, 0}, xgrid = 0;
     TileItem* d_titems[3] = {nullptr, nullptr, nullptr};
     unsigned* d_err = nullptr;
     unsigned* h_err = nullptr;  // pinned copy of *d_err
@@ -208,7 +216,8 @@ struct Batch final : BatchBase {
         if (graph) cudaGraphExecDestroy(graph);
         if (h_err) cudaFreeHost(h_err);
         void* bufs[] = {d_cavs,      d_items,     d_table, step_dev, d_tcavs,   d_maps[1],
-                        d_maps[2],   d_titems[1], d_titems[2], d_err};
+                        d_maps[2],   d_titems[1], d_titems[2], d_err,  d_xmaps[0],
+                        d_xmaps[1],  d_xitems[0], d_xitems[1]};
         for (void* b : bufs)
             if (b) cudaFree(b);
         for (Solver* s : cavs) delete s;
@@ -243,6 +252,10 @@ struct Batch final : BatchBase {
         *h_err = 0;
         setup_tiles<1>();
         setup_tiles<2>();
+        if constexpr (is_p16<St>::value) {
+            setup_xtiles<4>(0);
+            setup_xtiles<8>(1);
+        }
         set_tuning(tun);
         CK(cudaStreamSynchronize(stream));
     }
@@ -272,6 +285,41 @@ struct Batch final : BatchBase {
         CK(cudaStreamSynchronize(stream));
     }
 
+    // Tensor maps (64 + 16 columns x TY + 4 rows x 18 planes) and the tile
+    // list of the node-pair tile kernel for tile height TY.
+    template <int TY>
+    void setup_xtiles(int slot) {
+        using TS = TileXShape<TY>;
+        const int n = int(cv.size());
+        std::vector<CUtensorMap> maps(2 * size_t(n));
+        for (int i = 0; i < n; ++i)
+            for (int b = 0; b < 2; ++b) maps[2 * size_t(i) + b] = make_box_map<St>(cv[i]->pop[b], cv[i]->G, TX_BX, TS::BY);
+        CK(cudaMalloc(&d_xmaps[slot], sizeof(CUtensorMap) * maps.size()));
+        CK(cudaMemcpyAsync(d_xmaps[slot], maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice,
+                           stream));
+        std::vector<std::pair<int, int>> sizes;
+        for (auto* c : cv) sizes.push_back({c->p.nx, c->p.ny});
+        std::vector<TileItem> ti;
+        tilex_items(sizes, TY, ti);
+        n_xitems[slot] = int(ti.size());
+        CK(cudaMalloc(&d_xitems[slot], sizeof(TileItem) * ti.size()));
+        CK(cudaMemcpyAsync(d_xitems[slot], ti.data(), sizeof(TileItem) * ti.size(), cudaMemcpyHostToDevice, stream));
+        if constexpr (is_p16<St>::value) {
+            CK(cudaFuncSetAttribute(k_tile_x<St, TY, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TS::SMEM));
+            CK(cudaFuncSetAttribute(k_tile_x<St, TY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TS::SMEM));
+        }
+        CK(cudaStreamSynchronize(stream));
+    }
+
+    template <int TY>
+    int xtile_grid(int slot, int ctas_per_sm) {
+        int occ = 0;
+        if constexpr (is_p16<St>::value)
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tile_x<St, TY, false>, TileXShape<TY>::THREADS,
+                                                             TileXShape<TY>::SMEM));
+        return std::max(1, std::min(n_xitems[slot], std::max(1, std::min(ctas_per_sm, occ)) * n_sm));
+    }
+
     template <int V>
     int tile_grid(int ctas_per_sm) {
         int occ = 0;
@@ -282,14 +330,14 @@ struct Batch final : BatchBase {
 
     // The kernel this format runs for a requested one (see BatchTuning).
     static int effective_kernel(int k) {
-        if (k == 5 && !is_p16<St>::value) k = 3;
+        if ((k == 5 || k == 6) && !is_p16<St>::value) k = 3;
         if (k == 4 && !Fmt<St>::SHIFT) k = 3;
         return k;
     }
 
     void set_tuning(const BatchTuning& t) override {
         if (t.rows_per_item < 1 || t.rows_per_item > 1024 || t.ctas_per_sm < 1 || t.ctas_per_sm > 32 ||
-            t.kernel < 0 || t.kernel > 5)
+            t.kernel < 0 || t.kernel > 6)
             throw ArgError{CAV_ERR_ARG, "tuning out of range"};
         const int k = effective_kernel(t.kernel);
         const int r = t.rows_per_item;
@@ -297,6 +345,7 @@ struct Batch final : BatchBase {
             throw ArgError{CAV_ERR_ARG, "rows_per_item of kernels 3 and 5 must be 1, 2, 4 or 8"};
         if (k == 4 && !(r == 2 || r == 4 || r == 8))
             throw ArgError{CAV_ERR_ARG, "rows_per_item of kernel 4 must be 2, 4 or 8"};
+        if (k == 6 && !(r == 4 || r == 8)) throw ArgError{CAV_ERR_ARG, "rows_per_item of kernel 6 must be 4 or 8"};
         tun = t;
         // work items: 64 columns for the node-pair kernel, 32 otherwise
         const int width = k == 5 ? 64 : 32;
@@ -314,6 +363,7 @@ struct Batch final : BatchBase {
         grid = std::max(1, std::min(n_items, t.ctas_per_sm * n_sm));
         if (t.kernel == 1) tgrid = tile_grid<1>(t.ctas_per_sm);
         if (t.kernel == 2) tgrid = tile_grid<2>(t.ctas_per_sm);
+        if (k == 6) xgrid = r == 4 ? xtile_grid<4>(0, t.ctas_per_sm) : xtile_grid<8>(1, t.ctas_per_sm);
         if (graph) {
             cudaGraphExecDestroy(graph);
             graph = nullptr;
@@ -422,8 +472,36 @@ struct Batch final : BatchBase {
                               (const StepScalars<A>*)d_table, int(cv.size()), step, sdev));
     }
 
+    template <int TY, bool WN>
+    void launch_xtiles(int slot, const long long* sdev, long long step) {
+        if constexpr (is_p16<St>::value) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(xgrid);
+            cfg.blockDim = dim3(TileXShape<TY>::THREADS);
+            cfg.dynamicSmemBytes = TileXShape<TY>::SMEM;
+            cfg.stream = stream;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            attr[0].val.programmaticStreamSerializationAllowed = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            CK(cudaLaunchKernelEx(&cfg, k_tile_x<St, TY, WN>, (const TileCav<St>*)d_tcavs,
+                                  (const CUtensorMap*)d_xmaps[slot], (const TileItem*)d_xitems[slot], n_xitems[slot],
+                                  (const StepScalars<float>*)d_table, int(cv.size()), step, sdev, d_err));
+        }
+    }
+
     void launch(bool write_nut, const long long* sdev, long long step) {
         const int k = effective_kernel(tun.kernel);
+        if (k == 6) {
+            if (tun.rows_per_item == 4)
+                write_nut ? launch_xtiles<4, true>(0, sdev, step) : launch_xtiles<4, false>(0, sdev, step);
+            else
+                write_nut ? launch_xtiles<8, true>(1, sdev, step) : launch_xtiles<8, false>(1, sdev, step);
+            ++launches;
+            CK(cudaGetLastError());
+            return;
+        }
         if (k >= 3) {
             write_nut ? launch_np<true>(k, sdev, step) : launch_np<false>(k, sdev, step);
             ++launches;

@@ -647,8 +647,11 @@ int cav_batch_autotune(cav_batch* b, int32_t trial_steps, cav_batch_tuning* chos
         for (int r : {1, 2, 4, 8}) add(3, r, 8);
         if (prec != CAV_PREC_F64)
             for (int r : {2, 4, 8}) add(4, r, 8);
-        if (p16)
+        if (p16) {
             for (int r : {1, 2, 4, 8}) add(5, r, 8);
+            for (int r : {4, 8})
+                for (int c : {2, 3, 4}) add(6, r, c);
+        }
         // each candidate timed three times (after its warm-up steps), the
         // median kept: one-off noise cannot pick the winner
         BatchTuning best = x.tun;

@@ -262,9 +262,10 @@ inline PFN_cuTensorMapEncodeTiled_v12000 tile_map_encoder() {
     return fn;
 }
 
-// pop (18 planes of ny x pitch St) as a 3-D tensor with the tile box.
-template <class St, int V>
-CUtensorMap make_tile_map(const St* pop, const Geom& G) {
+// pop (18 planes of ny x pitch St) as a 3-D tensor with a box of box_x x
+// box_y x 18 elements.
+template <class St>
+CUtensorMap make_box_map(const St* pop, const Geom& G, int box_x, int box_y) {
     static_assert(sizeof(St) == 2 || sizeof(St) == 4 || sizeof(St) == 8, "element size");
     if ((G.pitch * sizeof(St)) % 16 != 0 || (reinterpret_cast<uintptr_t>(pop) & 15) != 0)
         throw ArgError{CAV_ERR_ARG, "tile map: rows must start on 16-byte boundaries"};
@@ -274,13 +275,21 @@ CUtensorMap make_tile_map(const St* pop, const Geom& G) {
                                                      : CU_TENSOR_MAP_DATA_TYPE_UINT64;
     const cuuint64_t dims[3] = {cuuint64_t(G.pitch), cuuint64_t(G.ny), cuuint64_t(NPLANES)};
     const cuuint64_t strides[2] = {cuuint64_t(G.pitch) * sizeof(St), cuuint64_t(G.plane) * sizeof(St)};
-    const cuuint32_t box[3] = {cuuint32_t(TILE_BX), cuuint32_t(TileShape<St, V>::BY), cuuint32_t(NPLANES)};
+    if ((box_x * sizeof(St)) % 16 != 0 || box_x > 256 || box_y > 256)
+        throw ArgError{CAV_ERR_ARG, "tile map: box rows must be multiples of 16 bytes, at most 256 elements"};
+    const cuuint32_t box[3] = {cuuint32_t(box_x), cuuint32_t(box_y), cuuint32_t(NPLANES)};
     const cuuint32_t estr[3] = {1, 1, 1};
     const CUresult r = tile_map_encoder()(&m, dt, 3, const_cast<St*>(pop), dims, strides, box, estr,
                                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) throw ArgError{CAV_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")"};
     return m;
+}
+
+// ... with the box of tile shape V.
+template <class St, int V>
+CUtensorMap make_tile_map(const St* pop, const Geom& G) {
+    return make_box_map<St>(pop, G, TILE_BX, TileShape<St, V>::BY);
 }
 
 // Tiles of every cavity, cavity-major then row-block then column block.

@@ -149,33 +149,37 @@ __device__ __forceinline__ void pull_g_x(const St* __restrict__ src, const Geom&
     }
 }
 
-// One reference step of the nodes (ix, iy), (ix + 1, iy): the pull, the
-// macroscopic update with the Guo half force, no-slip, the collision of the
-// next step and the stores (what fused_node does for one node).  Node ix + 1
-// may lie in the row padding (odd nx): its values are computed and stored
-// into the padding, which no kernel reads as a node.
+// Everything of one node-pair step after the pull: the macroscopic update
+// with the Guo half force, no-slip, the collision of the next step and the
+// stores (what fused_core does for one node).  pull_f(wf) / pull_g(wg) fill
+// the pulled f / g words (from global memory or a staged tile); t_at(x) is T
+// of the streamed state at column x of the row (Nusselt accumulation only);
+// fy_prev the previous collision's Guo force of the pair.  Node ix + 1 may
+// lie in the row padding (odd nx): its values are computed and stored into
+// the padding, which no kernel reads as a node.
 // NO_COLLIDE: identity collision (the pulled values are stored back; checks
 // the pull / bounce-back / boundary index maps bit for bit).
-template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE = false>
-__device__ __forceinline__ void fused_xpair(const St* __restrict__ src, St* __restrict__ dst,
-                                            const float* fy_in, float* fy_out, float* __restrict__ nut,
-                                            double* __restrict__ acc_hot, double* __restrict__ acc_cold,
-                                            const Geom& G, int ix, int iy, const StepScalars<float>& c) {
+// t_hot_row: the hot-wall theta of the row's g source row (c.t_hot[gy]).
+template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE, class PF, class PG, class TAt>
+__device__ __forceinline__ void xpair_core(PF&& pull_f, PG&& pull_g, TAt&& t_at, St* __restrict__ dst,
+                                           float2 fy_prev, float t_hot_row, float* fy_out, float* __restrict__ nut,
+                                           double* __restrict__ acc_hot, double* __restrict__ acc_cold,
+                                           const Geom& G, int ix, int iy, const StepScalars<float>& c) {
     using E = PairEnc<St>;
     constexpr int EF = Fmt<St>::EF, EG = Fmt<St>::EG;
     const int k0 = iy * G.pitch + ix;
     // f first: rho, u and the f collision's coefficients need no g
     float2 f[Q];
     uint32_t wg[Q], wf[Q];
-    pull_f_x<St>(src, G, ix, iy, wf);
+    pull_f(wf);
 #if XPAIR_EARLY_G
-    pull_g_x<St>(src, G, ix, iy, wg);
+    pull_g(wg);
 #endif
 #pragma unroll
     for (int i = 0; i < Q; ++i) f[i] = E::dec(wf[i], i);
     const bool wy = iy == 0 || iy == G.ny - 1;
     const Mask2 wall{wy || ix == 0 || ix == G.nx - 1, wy || ix + 1 == G.nx - 1};
-    Macro<float2, true> m = macro_f_lane<float2, EF>(f, *reinterpret_cast<const float2*>(fy_in + k0), wall);
+    Macro<float2, true> m = macro_f_lane<float2, EF>(f, fy_prev, wall);
     // the relaxation coefficients now; the non-equilibrium parts are formed
     // again at the f update (same expressions, same bits), so they are not
     // held in registers across the g half of the step
@@ -183,15 +187,13 @@ __device__ __forceinline__ void fused_xpair(const St* __restrict__ src, St* __re
     float2 g[Q];
     {
 #if !XPAIR_EARLY_G
-        pull_g_x<St>(src, G, ix, iy, wg);
+        pull_g(wg);
 #endif
-        const uint32_t(&w)[Q] = wg;
-        const int gy = iy == 0 ? 1 : (iy == G.ny - 1 ? G.ny - 2 : iy);
         const bool h0 = ix == 0, c0 = ix == G.nx - 1, c1 = ix + 1 == G.nx - 1;
-        const float tw0 = (h0 ? c.t_hot[gy] : c.t_cold) * p2(EG), tw1 = c.t_cold * p2(EG);
+        const float tw0 = (h0 ? t_hot_row : c.t_cold) * p2(EG), tw1 = c.t_cold * p2(EG);
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
-            const float2 v = E::dec(w[i], Q + i);
+            const float2 v = E::dec(wg[i], Q + i);
             // wall columns: geq(T_wall, 0, 0) = w_i T_wall (geq_rest)
             g[i].x = (h0 || c0) ? float(WD(i)) * tw0 : v.x;
             g[i].y = c1 ? float(WD(i)) * tw1 : v.y;
@@ -200,9 +202,9 @@ __device__ __forceinline__ void fused_xpair(const St* __restrict__ src, St* __re
     m.t = sum_g<float2>(g);
     if (!NO_COLLIDE && ACC_NU) {
         const float t0 = m.t.x * p2(-EG), t1 = m.t.y * p2(-EG);
-        if (ix + 1 == 1) acc_hot[iy] += fabs(double(t1) - double(gather_t<St>(src, G, 2, iy, c)));
-        if (ix == G.nx - 2) acc_cold[iy] += fabs(double(t0) - double(gather_t<St>(src, G, G.nx - 3, iy, c)));
-        if (ix + 1 == G.nx - 2) acc_cold[iy] += fabs(double(t1) - double(gather_t<St>(src, G, G.nx - 3, iy, c)));
+        if (ix + 1 == 1) acc_hot[iy] += fabs(double(t1) - double(t_at(2)));
+        if (ix == G.nx - 2) acc_cold[iy] += fabs(double(t0) - double(t_at(G.nx - 3)));
+        if (ix + 1 == G.nx - 2) acc_cold[iy] += fabs(double(t1) - double(t_at(G.nx - 3)));
     }
     // g collided and stored first (its registers free), then the f update;
     // stores: one word per plane, the draws in plane order 0..17
@@ -244,6 +246,22 @@ __device__ __forceinline__ void fused_xpair(const St* __restrict__ src, St* __re
 #pragma unroll
         for (int q = 0; q < Q; ++q) d[q * P2 + k2] = E::enc(f[q], q, 0u);
     }
+}
+
+// One reference step of the nodes (ix, iy), (ix + 1, iy) pulled from global
+// memory (xpair_core after pull_f_x / pull_g_x).
+template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE = false>
+__device__ __forceinline__ void fused_xpair(const St* __restrict__ src, St* __restrict__ dst,
+                                            const float* fy_in, float* fy_out, float* __restrict__ nut,
+                                            double* __restrict__ acc_hot, double* __restrict__ acc_cold,
+                                            const Geom& G, int ix, int iy, const StepScalars<float>& c) {
+    const int k0 = iy * G.pitch + ix;
+    const int gy = iy == 0 ? 1 : (iy == G.ny - 1 ? G.ny - 2 : iy);
+    xpair_core<St, WRITE_NUT, ACC_NU, NO_COLLIDE>(
+        [&](uint32_t(&w)[Q]) { pull_f_x<St>(src, G, ix, iy, w); },
+        [&](uint32_t(&w)[Q]) { pull_g_x<St>(src, G, ix, iy, w); },
+        [&](int x) { return gather_t<St>(src, G, x, iy, c); }, dst, *reinterpret_cast<const float2*>(fy_in + k0),
+        c.t_hot[gy], fy_out, nut, acc_hot, acc_cold, G, ix, iy, c);
 }
 
 // The single-cavity step on node pairs: 32 x BY threads cover 64 columns x

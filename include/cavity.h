@@ -277,12 +277,15 @@ typedef struct cav_batch cav_batch;
  *      (2, 4 or 8 rows; FP64 runs it as 3);
  *   5  one CTA per 64-column x rows_per_item item (1, 2, 4 or 8 rows), two
  *      x-adjacent nodes per thread, each plane one 32-bit word (16-bit
- *      formats; FP64 and FP32 run it as 3).
+ *      formats; FP64 and FP32 run it as 3);
+ *   6  the same node-pair body on TMA-staged shared-memory tiles of 64
+ *      columns x rows_per_item rows (4 or 8), ctas_per_sm persistent CTAs per
+ *      SM (16-bit formats; FP64 and FP32 run it as 3).
  * Default: kernel 3, 4 rows. */
 typedef struct cav_batch_tuning {
     int32_t rows_per_item; /* item / tile height in rows                     */
     int32_t ctas_per_sm;   /* resident CTAs per SM of the persistent kernels */
-    int32_t kernel;        /* 0..5, above                                    */
+    int32_t kernel;        /* 0..6, above                                    */
 } cav_batch_tuning;
 int cav_batch_create(const cav_params* params, int32_t n, cav_batch** out);
 int cav_batch_destroy(cav_batch* b);

@@ -24,12 +24,13 @@ def single(c, precision):
 
 
 @pytest.mark.parametrize("precision,kernel", [("f64", 3), ("f32", 3), ("f32", 4), ("f16sr", 3), ("f16sr", 5),
-                                              ("f16gsr", 5), ("bf16sr", 5), ("f16", 5)])
+                                              ("f16gsr", 5), ("bf16sr", 5), ("f16", 5), ("f16sr", 6), ("f16gsr", 6),
+                                              ("bf16sr", 6), ("bf16", 6)])
 def test_batch_is_bitwise_equal_to_single_cavities(precision, kernel):
     """Every cavity of the batch against the same cavity created alone (its
     default single-cavity kernel: node pairs for the 16-bit formats)."""
     b = CavityBatch(MIXED, precision=precision)
-    b.set_tuning(4, 8, kernel=kernel)
+    b.set_tuning(4, 3, kernel=kernel)
     singles = [single(c, precision) for c in MIXED]
     for n in (1, 150, 137):  # spin-up steps (table rows), graph replays, remainders
         b.step(n)
@@ -53,7 +54,7 @@ def test_batch_tuning_does_not_change_results(precision):
     b = CavityBatch(MIXED, precision=precision)
     a.set_tuning(3, 2, kernel=0)
     b.set_tuning(32, 16, kernel=1)
-    a.step(90)
+    a.step(100)
     b.step(40)
     b.set_tuning(2, 7, kernel=3)
     b.step(20)
@@ -64,6 +65,10 @@ def test_batch_tuning_does_not_change_results(precision):
     b.set_tuning(1, 1, kernel=5)
     b.step(5)
     b.set_tuning(8, 1, kernel=5)
+    b.step(5)
+    b.set_tuning(8, 3, kernel=6)
+    b.step(5)
+    b.set_tuning(4, 2, kernel=6)
     b.step(5)
     for i in range(len(MIXED)):
         fa, fb = a.fields(i), b.fields(i)
@@ -79,11 +84,13 @@ def test_autotune_picks_a_candidate_and_leaves_the_state_alone():
     b.step(10)
     ref.step(10)
     t = b.autotune(trial_steps=16)
-    assert t["kernel"] in (0, 1, 2, 3, 4, 5)
+    assert t["kernel"] in (0, 1, 2, 3, 4, 5, 6)
     if t["kernel"] == 0:
         assert t["rows_per_item"] in (4, 8, 16) and t["ctas_per_sm"] in (4, 8, 16)
     elif t["kernel"] in (1, 2):
         assert set(t) == {"kernel", "ctas_per_sm"} and t["ctas_per_sm"] in (1, 2, 3, 4)
+    elif t["kernel"] == 6:
+        assert t["rows_per_item"] in (4, 8) and t["ctas_per_sm"] in (2, 3, 4)
     else:
         assert set(t) == {"kernel", "rows_per_item"} and t["rows_per_item"] in (1, 2, 4, 8)
     assert b.tuning() == t
@@ -95,7 +102,7 @@ def test_autotune_picks_a_candidate_and_leaves_the_state_alone():
 
 def test_item_heights_outside_a_kernels_range_are_rejected():
     b = CavityBatch(MIXED[:2], precision="f16sr")
-    for rows, kernel in ((3, 3), (16, 5), (1, 4)):
+    for rows, kernel in ((3, 3), (16, 5), (1, 4), (2, 6)):
         with pytest.raises(L.CavError) as e:
             b.set_tuning(rows, 8, kernel=kernel)
         assert e.value.code == L.CAV_ERR_ARG
