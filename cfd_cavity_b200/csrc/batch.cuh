@@ -204,6 +204,7 @@ struct Batch final : BatchBase {
     CUtensorMap* d_maps[3] = {nullptr, nullptr, nullptr};   // per tile shape
     // the node-pair tile kernel: tensor maps and tile lists per tile height (4, 8)
     CUtensorMap* d_xmaps[2] = {nullptr, nullptr};
+    CUtensorMap* d_fmaps[2] = {nullptr, nullptr};  // the Guo force field of every cavity
     TileItem* d_xitems[2] = {nullptr, nullptr};
     int n_xitems[2] = {0, 0}, xgrid = 0;
     TileItem* d_titems[3] = {nullptr, nullptr, nullptr};
@@ -217,7 +218,7 @@ struct Batch final : BatchBase {
         if (h_err) cudaFreeHost(h_err);
         void* bufs[] = {d_cavs,      d_items,     d_table, step_dev, d_tcavs,   d_maps[1],
                         d_maps[2],   d_titems[1], d_titems[2], d_err,  d_xmaps[0],
-                        d_xmaps[1],  d_xitems[0], d_xitems[1]};
+                        d_xmaps[1],  d_xitems[0], d_xitems[1], d_fmaps[0], d_fmaps[1]};
         for (void* b : bufs)
             if (b) cudaFree(b);
         for (Solver* s : cavs) delete s;
@@ -296,6 +297,12 @@ struct Batch final : BatchBase {
             for (int b = 0; b < 2; ++b) maps[2 * size_t(i) + b] = make_box_map<St>(cv[i]->pop[b], cv[i]->G, TX_BX, TS::BY);
         CK(cudaMalloc(&d_xmaps[slot], sizeof(CUtensorMap) * maps.size()));
         CK(cudaMemcpyAsync(d_xmaps[slot], maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice,
+                           stream));
+        std::vector<CUtensorMap> fmaps(n);
+        if constexpr (is_p16<St>::value)
+            for (int i = 0; i < n; ++i) fmaps[i] = make_field_map(cv[i]->fy, cv[i]->G, TX_W, TY);
+        CK(cudaMalloc(&d_fmaps[slot], sizeof(CUtensorMap) * fmaps.size()));
+        CK(cudaMemcpyAsync(d_fmaps[slot], fmaps.data(), sizeof(CUtensorMap) * fmaps.size(), cudaMemcpyHostToDevice,
                            stream));
         std::vector<std::pair<int, int>> sizes;
         for (auto* c : cv) sizes.push_back({c->p.nx, c->p.ny});
@@ -486,8 +493,9 @@ struct Batch final : BatchBase {
             cfg.attrs = attr;
             cfg.numAttrs = 1;
             CK(cudaLaunchKernelEx(&cfg, k_tile_x<St, TY, WN>, (const TileCav<St>*)d_tcavs,
-                                  (const CUtensorMap*)d_xmaps[slot], (const TileItem*)d_xitems[slot], n_xitems[slot],
-                                  (const StepScalars<float>*)d_table, int(cv.size()), step, sdev, d_err));
+                                  (const CUtensorMap*)d_xmaps[slot], (const CUtensorMap*)d_fmaps[slot],
+                                  (const TileItem*)d_xitems[slot], n_xitems[slot], (const StepScalars<float>*)d_table,
+                                  int(cv.size()), step, sdev, d_err));
         }
     }
 

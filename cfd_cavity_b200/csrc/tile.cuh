@@ -286,6 +286,25 @@ CUtensorMap make_box_map(const St* pop, const Geom& G, int box_x, int box_y) {
     return m;
 }
 
+// A pitched FP32 field (ny rows of pitch floats) as a 2-D tensor with a box
+// of box_x x box_y elements.
+inline CUtensorMap make_field_map(const float* field, const Geom& G, int box_x, int box_y) {
+    if ((G.pitch * sizeof(float)) % 16 != 0 || (reinterpret_cast<uintptr_t>(field) & 15) != 0 ||
+        (box_x * sizeof(float)) % 16 != 0 || box_x > 256 || box_y > 256)
+        throw ArgError{CAV_ERR_ARG, "field map: rows and box rows must be multiples of 16 bytes"};
+    CUtensorMap m;
+    const cuuint64_t dims[2] = {cuuint64_t(G.pitch), cuuint64_t(G.ny)};
+    const cuuint64_t strides[1] = {cuuint64_t(G.pitch) * sizeof(float)};
+    const cuuint32_t box[2] = {cuuint32_t(box_x), cuuint32_t(box_y)};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = tile_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(field), dims,
+                                          strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw ArgError{CAV_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")"};
+    return m;
+}
+
 // ... with the box of tile shape V.
 template <class St, int V>
 CUtensorMap make_tile_map(const St* pop, const Geom& G) {

@@ -28,16 +28,43 @@ constexpr int TX_W = 64;                   // tile columns (32 node pairs)
 constexpr int TX_BX = TX_W + 2 * TILE_HX;  // box width, halo included (80)
 constexpr int TX_WORDS = TX_BX / 2;        // 32-bit words per staged row (40)
 
+// Warps per CTA of the 8-row tiles (each warp TY / WARPS rows).
+#ifndef TILEX_R8_WARPS
+#define TILEX_R8_WARPS 4
+#endif
+
 template <int TY_>
 struct TileXShape {
     static constexpr int TY = TY_;
-    static constexpr int WARPS = 4;
+    static constexpr int WARPS = TY_ == 8 ? TILEX_R8_WARPS : 4;
+    // resident CTAs per SM the register budget is sized for
+    static constexpr int MIN_CTAS = WARPS == 8 ? 3 : 4;
     static constexpr int THREADS = 32 * WARPS;
     static constexpr int BY = TY + 2 * TILE_HY;
-    static constexpr int STAGE_BYTES = NPLANES * BY * TX_BX * 2;
+    static constexpr int POP_BYTES = NPLANES * BY * TX_BX * 2;  // the populations of the tile and its halo
+    static constexpr int FY_BYTES = TY * TX_W * 4;              // the previous Guo force of the tile
+    static constexpr int STAGE_BYTES = POP_BYTES + FY_BYTES;
     static constexpr int SMEM = 2 * STAGE_BYTES + 128;  // + alignment slack of the stage base
-    static_assert(TY % WARPS == 0 && STAGE_BYTES % 128 == 0, "tile shape");
+    static_assert(TY % WARPS == 0 && POP_BYTES % 128 == 0 && FY_BYTES % 128 == 0, "tile shape");
 };
+
+// The cavity of the tiles in flight, kept in shared memory (refreshed when
+// a CTA's tile range crosses into another cavity).
+template <class St>
+struct TileXMeta {
+    TileCav<St> cv;
+    StepScalars<float> c;
+};
+
+// One box of a 2-D tensor map into shared memory, completing on *bar
+// (x * element size a multiple of 16 bytes).
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
 
 // pull_f_x from a staged tile: trow = the row's position in the stage (halo
 // included), wc = the pair's word column (4 + lane).
@@ -87,20 +114,28 @@ __device__ __forceinline__ void pull_g_tx(const uint32_t* __restrict__ S, const 
     }
 }
 
-// One lattice step of every tile in `items` (x0 multiples of 64, y0 of TY);
-// step scalars of cavity c at step s are table[min(s, spin_up) * n_cav + c].
+// One lattice step of every tile in `items` (x0 multiples of 64, y0 of TY;
+// cavity-major); step scalars of cavity c at step s are
+// table[min(s, spin_up) * n_cav + c].  CTA b takes the contiguous range of
+// tiles [b per, (b + 1) per), so consecutive tiles share the cavity (its
+// metadata is loaded once per range crossing) and their halo rows (L2).  Per
+// tile, the populations with their halo (maps[2 cav + buffer]) and the
+// previous Guo force of the tile (fmaps[cav]) arrive by TMA; the next tile's
+// copies are issued before the current one is computed.
 template <class St, int TY, bool WRITE_NUT>
-__global__ void __launch_bounds__(TileXShape<TY>::THREADS, 4)
+__global__ void __launch_bounds__(TileXShape<TY>::THREADS, TileXShape<TY>::MIN_CTAS)
     k_tile_x(const TileCav<St>* __restrict__ cavs, const CUtensorMap* __restrict__ maps,
-             const TileItem* __restrict__ items, int n_items, const StepScalars<float>* __restrict__ table, int n_cav,
-             long long step, const long long* __restrict__ step_dev, unsigned* __restrict__ err) {
+             const CUtensorMap* __restrict__ fmaps, const TileItem* __restrict__ items, int n_items,
+             const StepScalars<float>* __restrict__ table, int n_cav, long long step,
+             const long long* __restrict__ step_dev, unsigned* __restrict__ err) {
     using TS = TileXShape<TY>;
     extern __shared__ __align__(128) unsigned char tilex_smem[];
     __shared__ __align__(8) uint64_t bar[2];
+    __shared__ TileXMeta<St> meta;
     // TMA destinations on a 128-byte boundary
     unsigned char* base = tilex_smem + ((128u - (smem_u32(tilex_smem) & 127u)) & 127u);
-    const uint32_t* stage0 = reinterpret_cast<const uint32_t*>(base);
-    const uint32_t* stage1 = reinterpret_cast<const uint32_t*>(base + TS::STAGE_BYTES);
+    unsigned char* const stage0 = base;
+    unsigned char* const stage1 = base + TS::STAGE_BYTES;
     const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
     if (threadIdx.x == 0) {
         mbar_init(&bar[0], 1);
@@ -111,59 +146,70 @@ __global__ void __launch_bounds__(TileXShape<TY>::THREADS, 4)
     pdl_wait();
     pdl_trigger();
     const long long s = step_dev ? *step_dev + step : step;
-    auto issue = [&](int item, int st) {
-        const TileItem I = items[item];
-        const int b = (cavs[I.cav].parity + int(s & 1)) & 1;
-        uint64_t* br = &bar[st];
-        mbar_expect_tx(br, TS::STAGE_BYTES);
-        tma_load_3d(const_cast<uint32_t*>(st ? stage1 : stage0), maps + 2 * I.cav + b, br, I.x0 - TILE_HX,
-                    I.y0 - TILE_HY, 0);
+    const int per = (n_items + int(gridDim.x) - 1) / int(gridDim.x);
+    const int it0 = min(n_items, int(blockIdx.x) * per), it1 = min(n_items, it0 + per);
+    // the issuing thread's cavity and its buffer parity
+    int icav = -1, ipar = 0;
+    auto issue = [&](const TileItem& I, int st) {
+        if (I.cav != icav) {
+            icav = I.cav;
+            ipar = cavs[I.cav].parity;
+        }
+        const int b = (ipar + int(s & 1)) & 1;
+        mbar_expect_tx(&bar[st], TS::STAGE_BYTES);
+        unsigned char* const d = st ? stage1 : stage0;
+        tma_load_3d(d, maps + 2 * I.cav + b, &bar[st], I.x0 - TILE_HX, I.y0 - TILE_HY, 0);
+        tma_load_2d(d + TS::POP_BYTES, fmaps + I.cav, &bar[st], I.x0, I.y0);
     };
-    if (threadIdx.x == 0 && int(blockIdx.x) < n_items) issue(blockIdx.x, 0);
+    TileItem Icur{0, 0, 0}, Inext{0, 0, 0};
+    if (it0 < it1) {
+        Icur = items[it0];
+        if (threadIdx.x == 0) issue(Icur, 0);
+    }
+    if (it0 + 1 < it1) Inext = items[it0 + 1];
+    int mcav = -1;  // the cavity whose metadata is in `meta`
     int k = 0;
     bool next_issued = false, failed = false;
-    for (int it = blockIdx.x; it < n_items; it += gridDim.x, ++k) {
+    for (int it = it0; it < it1; ++it, ++k) {
         const int st = k & 1;
-        next_issued = it + int(gridDim.x) < n_items;
-        if (threadIdx.x == 0 && next_issued) issue(it + gridDim.x, st ^ 1);
-        // what does not depend on the staged tile, before the wait: the
-        // tile's cavity and step scalars, and this warp's rows of the
-        // previous Guo force (the only per-node global loads of the step)
-        const TileItem I = items[it];
-        const TileCav<St> cv = cavs[I.cav];
-        const Geom G = cv.G;
-        const int ix = I.x0 + 2 * lane;
-        const int srow = s < cv.spin_up ? int(s) : cv.spin_up;
-        StepScalars<float> c = table[(long long)srow * n_cav + I.cav];
-        c.step = s;
-        c.step_dev = nullptr;
-        // (a select, not cv.pop[index]: an indexed copy would live in local memory)
-        St* const dst = ((cv.parity + int(s & 1)) & 1) ? cv.pop[0] : cv.pop[1];
-        constexpr int RPW = TY / TS::WARPS;  // rows per warp
-        float2 fyp[RPW];
-        float thp[RPW];
-#pragma unroll
-        for (int j = 0; j < RPW; ++j) {
-            const int iy = I.y0 + wy + j * TS::WARPS;
-            const bool in = ix < G.nx && iy < G.ny;
-            fyp[j] = in ? *reinterpret_cast<const float2*>(cv.fy + iy * G.pitch + ix) : make_float2(0.0f, 0.0f);
-            const int gy = iy == 0 ? 1 : (iy == G.ny - 1 ? G.ny - 2 : iy);
-            thp[j] = in ? c.t_hot[gy] : 0.0f;
+        next_issued = it + 1 < it1;
+        if (threadIdx.x == 0 && next_issued) issue(Inext, st ^ 1);
+        const TileItem I = Icur;
+        Icur = Inext;
+        if (it + 2 < it1) Inext = items[it + 2];
+        if (I.cav != mcav) {  // the same for every thread of the CTA
+            if (threadIdx.x == 0) {
+                meta.cv = cavs[I.cav];
+                const int row = s < meta.cv.spin_up ? int(s) : meta.cv.spin_up;
+                meta.c = table[(long long)row * n_cav + I.cav];
+                meta.c.step = s;
+                meta.c.step_dev = nullptr;
+            }
+            __syncthreads();
+            mcav = I.cav;
         }
+        const Geom G = meta.cv.G;
+        const int ix = I.x0 + 2 * lane;
         const bool ok = mbar_wait_bounded(&bar[st], uint32_t((k >> 1) & 1));
         if (ok && ix < G.nx) {
-            const uint32_t* S = st ? stage1 : stage0;
+            const unsigned char* const sb = st ? stage1 : stage0;
+            const uint32_t* S = reinterpret_cast<const uint32_t*>(sb);
+            const float* FY = reinterpret_cast<const float*>(sb + TS::POP_BYTES);
+            // (a select, not pop[index]: an indexed copy would live in local memory)
+            St* const dst = ((meta.cv.parity + int(s & 1)) & 1) ? meta.cv.pop[0] : meta.cv.pop[1];
 #pragma unroll
-            for (int j = 0; j < RPW; ++j) {
+            for (int j = 0; j < TY / TS::WARPS; ++j) {
                 const int r = wy + j * TS::WARPS;
                 const int iy = I.y0 + r;
                 if (iy < G.ny) {
                     const int trow = r + TILE_HY, wc = TILE_HX / 2 + lane;
+                    const int gy = iy == 0 ? 1 : (iy == G.ny - 1 ? G.ny - 2 : iy);
+                    const float th = ix == 0 ? meta.c.t_hot[gy] : 0.0f;
                     xpair_core<St, WRITE_NUT, false, false>(
                         [=](uint32_t(&w)[Q]) { pull_f_tx<TS::BY>(S, G, ix, iy, trow, wc, w); },
                         [=](uint32_t(&w)[Q]) { pull_g_tx<TS::BY>(S, G, ix, iy, trow, wc, w); },
-                        [](int) { return 0.0f; }, dst, fyp[j], thp[j], cv.fy, cv.nut, nullptr, nullptr, G, ix, iy,
-                        c);
+                        [](int) { return 0.0f; }, dst, *reinterpret_cast<const float2*>(FY + r * TX_W + 2 * lane),
+                        th, meta.cv.fy, meta.cv.nut, nullptr, nullptr, G, ix, iy, meta.c);
                 }
             }
         }
