@@ -310,12 +310,11 @@ def octree_c5(dev, chain=(30_000, 30_000, 60_000), window=40_000, sample_every=1
     return out
 
 
-def batch_only(precision, steps, kernel, rows):
+def batch_only(precision, steps, kernel, rows, ctas):
     """C3 batch timing alone (profiling runs): the 64-cavity sweep in one
     storage format with a fixed tuning (kernel `kernel`, `rows` rows per
-    tile or item; 4 CTAs per SM for the persistent global-memory kernel, 3
-    for the tile kernel), 250 spin-up steps, then `steps` timed lattice
-    steps."""
+    tile or item, `ctas` resident CTAs per SM for the persistent kernels),
+    250 spin-up steps, then `steps` timed lattice steps."""
     import torch
 
     from cfd_cavity_b200 import CavityBatch, sweep_configs
@@ -323,7 +322,7 @@ def batch_only(precision, steps, kernel, rows):
     cfg = sweep_configs(64)
     nodes = sum(c["nx"] * c["ny"] for c in cfg)
     bt = CavityBatch(cfg, precision=precision, device=0)
-    bt.set_tuning(rows, 4 if kernel == 0 else 3, kernel=kernel)
+    bt.set_tuning(rows, ctas, kernel=kernel)
     bt.step(250)
     st = torch.cuda.ExternalStream(bt.stream_handle(), device=0)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -336,6 +335,7 @@ def batch_only(precision, steps, kernel, rows):
     bt.sync()
     ms = e0.elapsed_time(e1)
     print(json.dumps({"workload": f"batched sweep 64 cavities {precision}", "kernel": kernel, "rows": rows,
+                      "ctas_per_sm": ctas,
                       "steps": steps,
                       "us_per_step": ms * 1e3 / steps, "mlups": nodes * steps / (ms * 1e-3) / 1e6}), flush=True)
     bt.close()
@@ -436,6 +436,7 @@ def main():
                     help="only time the 64-cavity batched sweep in PRECISION for --steps lattice steps "
                          "(profiling runs); --batch-kernel selects the kernel")
     ap.add_argument("--batch-kernel", type=int, default=6, choices=[0, 1, 2, 3, 4, 5, 6])
+    ap.add_argument("--batch-ctas", type=int, default=4, help="resident CTAs per SM of --batch-only (kernels 0, 1, 2, 6)")
     ap.add_argument("--batch-rows", type=int, default=4,
                     help="tile / item height of --batch-only (kernels 3 and 5: 1, 2, 4 or 8; 6: 4 or 8)")
     args = ap.parse_args()
@@ -443,7 +444,7 @@ def main():
     if args.octree_only:
         return octree_only(args.octree_only)
     if args.batch_only:
-        return batch_only(args.batch_only, args.steps, args.batch_kernel, args.batch_rows)
+        return batch_only(args.batch_only, args.steps, args.batch_kernel, args.batch_rows, args.batch_ctas)
     world, rank, local, dist = dist_setup(args)
     if args.impl == "reference":
         rc = run_reference(args, world, rank, dist)
@@ -585,7 +586,8 @@ def main():
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "peak_spec": SPEC_HBM_GBS, "frac_spec": achieved / SPEC_HBM_GBS,
                          "traffic": profile_traffic(prec),
-                         "kernel": "k_fused", "algorithmic_bytes_per_node": bpn,
+                         "kernel": ["k_fused", "k_fused_x", "k_fused_xs"][s.step_kernel()],
+                         "algorithmic_bytes_per_node": bpn,
                          "avg_launch_us": kernel_us},
             "cpu_baseline": base,
             "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": 4 * 8 * n,

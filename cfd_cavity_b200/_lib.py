@@ -27,7 +27,7 @@ PRECISIONS = {"f64": CAV_PREC_F64, "f32": CAV_PREC_F32, "f16": CAV_PREC_F16, "bf
               "f16g": CAV_PREC_F16G, "f16sr": CAV_PREC_F16SR, "bf16sr": CAV_PREC_BF16SR,
               "f16gsr": CAV_PREC_F16GSR}
 CAV_INIT_LINEAR, CAV_INIT_ZERO = 0, 1
-CAV_STEP_NODE, CAV_STEP_PAIR = 0, 1
+CAV_STEP_NODE, CAV_STEP_PAIR, CAV_STEP_PAIR_SPLIT = 0, 1, 2
 (CAV_PHASE_COLLIDE, CAV_PHASE_STREAM, CAV_PHASE_BOUNCE_BACK, CAV_PHASE_THERMAL_BC,
  CAV_PHASE_MACRO, CAV_PHASE_NOSLIP, CAV_PHASE_FUSED_IDENTITY, CAV_PHASE_CHANNEL) = range(8)
 

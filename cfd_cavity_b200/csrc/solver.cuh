@@ -172,6 +172,11 @@ struct Impl final : Solver {
     // the node-pair kernel: 32 x BYX threads cover 64 columns x BYX rows
     static constexpr int BYX = 2;
     dim3 blkx{BX, BYX}, grdx{};
+    // the 16-bit formats' default step kernel: pairs split over two warps
+    // for cavities that cannot fill the GPU (a step is then one thread's
+    // latency chain; on a B200 128 x 512 f16sr 2.32 us against 2.42, 64 x 256
+    // 1.67 against 2.00), plain pairs above (512 x 2048: 16.3 against 23.8)
+    static constexpr long long SPLIT_MAX_NODES = 70000;
     int kern = is_p16<St>::value ? 1 : 0;
     // dynamic subgrid model
     double dyn_alpha = 0.5, dyn_min = -0.1, dyn_eta = 2.0;
@@ -202,6 +207,7 @@ struct Impl final : Solver {
             throw ArgError{CAV_ERR_ARG, "grid too large: 18 * ny * pitch must stay below 2^31 elements"};
         grd = dim3((p.nx + BX - 1) / BX, (p.ny + BYF - 1) / BYF);
         grdx = dim3(((p.nx + 1) / 2 + BX - 1) / BX, (p.ny + BYX - 1) / BYX);
+        if (is_p16<St>::value && (long long)p.nx * p.ny <= SPLIT_MAX_NODES) kern = 2;
         if (!stream) {
             CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
             own_stream = true;
@@ -405,14 +411,21 @@ struct Impl final : Solver {
                                       nut, acc_hot, acc_cold, G, c));
                 return;
             }
+            if (kern == 2) {
+                cfg.gridDim = dim3(((p.nx + 1) / 2 + 31) / 32, (p.ny + 1) / 2);
+                cfg.blockDim = dim3(128);
+                CK(cudaLaunchKernelEx(&cfg, k_fused_xs<St, WN, ACC>, (const St*)pop[cur], pop[cur ^ 1], fy, nut,
+                                      acc_hot, acc_cold, G, c));
+                return;
+            }
         }
         CK(cudaLaunchKernelEx(&cfg, k_fused<St, WN, ACC, false>, (const St*)pop[cur], pop[cur ^ 1], fy, nut,
                               acc_hot, acc_cold, G, c));
     }
 
     void set_step_kernel(int k) override {
-        if (k != 0 && k != 1) throw ArgError{CAV_ERR_ARG, "step kernel must be 0 or 1"};
-        if (k == 1 && !is_p16<St>::value)
+        if (k < 0 || k > 2) throw ArgError{CAV_ERR_ARG, "step kernel must be 0, 1 or 2"};
+        if (k >= 1 && !is_p16<St>::value)
             throw ArgError{CAV_ERR_ARG, "the node-pair step kernel is for the 16-bit storage formats"};
         CK(cudaStreamSynchronize(stream));
         kern = k;
@@ -682,7 +695,7 @@ struct Impl final : Solver {
                 for (int64_t j = 0; j < step_arg; ++j) {
                     bool done = false;
                     if constexpr (is_p16<St>::value) {
-                        if (kern == 1) {
+                        if (kern >= 1) {
                             k_fused_x<St, false, false, true><<<grdx, blkx, 0, stream>>>(
                                 pop[cur], pop[cur ^ 1], fy, nut, acc_hot, acc_cold, G, scalars(time_step));
                             done = true;

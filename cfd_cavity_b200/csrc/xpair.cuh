@@ -264,6 +264,116 @@ __device__ __forceinline__ void fused_xpair(const St* __restrict__ src, St* __re
         c.t_hot[gy], fy_out, nut, acc_hot, acc_cold, G, ix, iy, c);
 }
 
+// The node-pair step with the work of each pair split over two warps: an f
+// warp (pull of f, macroscopic update, the collision's coefficients, the f
+// update and stores) and a g warp (pull of g with the boundary conditions,
+// T, the g collision and stores) exchange T and (u, v, nu_t) through shared
+// memory at one named barrier per row.  Twice the warps of k_fused_x, each
+// with about half its dependent chain: for grids too small to fill the GPU,
+// where a step is one thread's latency.  The same expressions in the same
+// order per node: bit-identical to k_fused_x.  CTA: 32 pairs x 2 rows x 2
+// roles (warps 0-1: f of rows 0-1; warps 2-3: g).
+__device__ __forceinline__ void named_bar_sync(int id, int threads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
+template <class St, bool WRITE_NUT, bool ACC_NU>
+__global__ void __launch_bounds__(128) k_fused_xs(const St* __restrict__ src, St* __restrict__ dst,
+                                                  float* __restrict__ fy, float* __restrict__ nut,
+                                                  double* __restrict__ acc_hot, double* __restrict__ acc_cold, Geom G,
+                                                  StepScalars<float> c) {
+    using E = PairEnc<St>;
+    constexpr int EF = Fmt<St>::EF, EG = Fmt<St>::EG;
+    __shared__ float2 sh_t[2][32], sh_u[2][32], sh_v[2][32], sh_nut[2][32];
+    pdl_wait();
+    pdl_trigger();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int r = w & 1, role = w >> 1;
+    const int ix = 2 * (blockIdx.x * 32 + lane);
+    const int iy = blockIdx.y * 2 + r;
+    const bool act = ix < G.nx && iy < G.ny;
+    const int k0 = iy * G.pitch + ix, k2 = k0 >> 1;
+    const int P2 = int(G.plane >> 1);
+    uint32_t* __restrict__ d = reinterpret_cast<uint32_t*>(dst);
+    if (role == 0) {
+        float2 f[Q];
+        Macro<float2, true> m{};
+        CollCoef<float2> kc{};
+        if (act) {
+            uint32_t wf[Q];
+            pull_f_x<St>(src, G, ix, iy, wf);
+#pragma unroll
+            for (int i = 0; i < Q; ++i) f[i] = E::dec(wf[i], i);
+            const bool wy = iy == 0 || iy == G.ny - 1;
+            const Mask2 wall{wy || ix == 0 || ix == G.nx - 1, wy || ix + 1 == G.nx - 1};
+            m = macro_f_lane<float2, EF>(f, *reinterpret_cast<const float2*>(fy + k0), wall);
+            kc = collide_f_coef_lane<float2, EF>(f, m, c, nullptr);
+            sh_u[r][lane] = m.ux;
+            sh_v[r][lane] = m.uy;
+            sh_nut[r][lane] = kc.nut;
+        }
+        named_bar_sync(1 + r, 64);
+        if (act) {
+            m.t = sh_t[r][lane];
+            const CollF<float2> o = collide_f_parts_lane<float2, EF>(f, m, kc);
+            const float2 fyv = collide_f_post_lane<float2, EF, EG>(f, o, m, c, m.t);
+            *reinterpret_cast<float2*>(fy + k0) = fyv;
+            if (WRITE_NUT) *reinterpret_cast<float2*>(nut + k0) = kc.nut;
+            if constexpr (E::SR) {
+                NodeRng rng = sr_pair_rng(c, G, ix, iy);
+#pragma unroll
+                for (int q = 0; q < Q; ++q) d[q * P2 + k2] = E::enc(f[q], q, rng.next());
+            } else {
+#pragma unroll
+                for (int q = 0; q < Q; ++q) d[q * P2 + k2] = E::enc(f[q], q, 0u);
+            }
+        }
+    } else {
+        float2 g[Q], t{};
+        if (act) {
+            uint32_t wg[Q];
+            pull_g_x<St>(src, G, ix, iy, wg);
+            const int gy = iy == 0 ? 1 : (iy == G.ny - 1 ? G.ny - 2 : iy);
+            const bool h0 = ix == 0, c0 = ix == G.nx - 1, c1 = ix + 1 == G.nx - 1;
+            const float tw0 = (h0 ? c.t_hot[gy] : c.t_cold) * p2(EG), tw1 = c.t_cold * p2(EG);
+#pragma unroll
+            for (int i = 0; i < Q; ++i) {
+                const float2 v = E::dec(wg[i], Q + i);
+                g[i].x = (h0 || c0) ? float(WD(i)) * tw0 : v.x;
+                g[i].y = c1 ? float(WD(i)) * tw1 : v.y;
+            }
+            t = sum_g<float2>(g);
+            sh_t[r][lane] = t;
+            if (ACC_NU) {
+                const float t0 = t.x * p2(-EG), t1 = t.y * p2(-EG);
+                if (ix + 1 == 1) acc_hot[iy] += fabs(double(t1) - double(gather_t<St>(src, G, 2, iy, c)));
+                if (ix == G.nx - 2)
+                    acc_cold[iy] += fabs(double(t0) - double(gather_t<St>(src, G, G.nx - 3, iy, c)));
+                if (ix + 1 == G.nx - 2)
+                    acc_cold[iy] += fabs(double(t1) - double(gather_t<St>(src, G, G.nx - 3, iy, c)));
+            }
+        }
+        named_bar_sync(1 + r, 64);
+        if (act) {
+            const float2 u = sh_u[r][lane], v = sh_v[r][lane], nt = sh_nut[r][lane];
+            float2 qv[5];
+            const float2 m15u2 = m15u2_lane<float2>(u, v);
+#pragma unroll
+            for (int p = 1; p <= 4; ++p) qv[p] = q_lane<float2>(p, u, v, m15u2);
+            collide_g_lane<float2>(g, t, u, v, nt, qv, c, nullptr);
+            if constexpr (E::SR) {
+                NodeRng rng = sr_pair_rng(c, G, ix, iy);
+                rng.skip<Q>();
+#pragma unroll
+                for (int q = 0; q < Q; ++q) d[(Q + q) * P2 + k2] = E::enc(g[q], Q + q, rng.next());
+            } else {
+#pragma unroll
+                for (int q = 0; q < Q; ++q) d[(Q + q) * P2 + k2] = E::enc(g[q], Q + q, 0u);
+            }
+        }
+    }
+}
+
 // The single-cavity step on node pairs: 32 x BY threads cover 64 columns x
 // BY rows.
 template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE>

@@ -165,7 +165,9 @@ class CavitySolver:
 
     def set_step_kernel(self, kernel):
         """Kernel of the fused step: 0 one node per thread, 1 two x-adjacent
-        nodes per thread (16-bit formats, their default); same bits."""
+        nodes per thread, 2 the same pairs with their f and g halves on two
+        warps (16-bit formats: 2 is the default up to 70 000 nodes, 1
+        above); same bits."""
         self._ck(L.load().cav_set_step_kernel(self._h, int(kernel)))
 
     def step_kernel(self):

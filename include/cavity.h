@@ -194,10 +194,16 @@ int cav_get_stream(cav_handle* h, void** stream);
 int cav_launch_count(cav_handle* h, int64_t* n);
 /* Kernel of the fused step (no counterpart in the reference):
  * CAV_STEP_NODE one node per thread; CAV_STEP_PAIR two x-adjacent nodes per
- * thread, each plane one 32-bit word (16-bit formats only, their default).
- * Both give the same bits; CAV_ERR_ARG for a pair kernel on FP64 / FP32. */
+ * thread, each plane one 32-bit word (16-bit formats only);
+ * CAV_STEP_PAIR_SPLIT the same node pairs with the f and g halves of each
+ * pair's work on two warps (twice the warps, each a shorter chain: for
+ * cavities too small to fill the GPU).  Default for the 16-bit formats:
+ * CAV_STEP_PAIR_SPLIT up to 70 000 nodes, CAV_STEP_PAIR above; FP64 / FP32:
+ * CAV_STEP_NODE.  All give the same bits; CAV_ERR_ARG for a pair kernel on
+ * FP64 / FP32. */
 #define CAV_STEP_NODE 0
 #define CAV_STEP_PAIR 1
+#define CAV_STEP_PAIR_SPLIT 2
 int cav_set_step_kernel(cav_handle* h, int32_t kernel);
 int cav_get_step_kernel(cav_handle* h, int32_t* kernel);
 

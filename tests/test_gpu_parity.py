@@ -134,25 +134,32 @@ def test_fp64_fields_after_1000_steps(cfg):
 def test_node_pair_and_one_node_kernels_give_the_same_bits(precision, shape):
     """The node-pair step kernel (two x-adjacent nodes per thread, packed
     FP32x2 arithmetic, one rounding instruction and one 32-bit store per
-    plane pair) against the one-node kernel: every field and population
+    plane pair), and its variant with each pair's f and g halves on two
+    warps, against the one-node kernel: every field and population
     identical after the spin-up ramp and graph replays, stochastic rounding
-    included (both draw per node pair)."""
+    included (all draw per node pair)."""
     nx, ny = shape
     a = CavitySolver(nx, ny, 1e7, 0.71, 0.1, 0.9, 0.02, 11, precision=precision)
     b = CavitySolver(nx, ny, 1e7, 0.71, 0.1, 0.9, 0.02, 11, precision=precision)
-    assert a.step_kernel() == L.CAV_STEP_PAIR
+    c = CavitySolver(nx, ny, 1e7, 0.71, 0.1, 0.9, 0.02, 11, precision=precision)
+    assert a.step_kernel() == (L.CAV_STEP_PAIR_SPLIT if nx * ny <= 70000 else L.CAV_STEP_PAIR)
+    a.set_step_kernel(L.CAV_STEP_PAIR)
     b.set_step_kernel(L.CAV_STEP_NODE)
-    a.nu_accumulate(True)
-    b.nu_accumulate(True)
+    c.set_step_kernel(L.CAV_STEP_PAIR_SPLIT)
+    for s in (a, b, c):
+        s.nu_accumulate(True)
     for n in (1, 250, 77):
-        a.step(n)
-        b.step(n)
-    fa, fb = a.fields(), b.fields()
-    for k in fa:
-        assert np.array_equal(fa[k], fb[k]), k
-    pa, pb = a.populations(), b.populations()
-    assert np.array_equal(pa[0], pb[0]) and np.array_equal(pa[1], pb[1])
-    assert a.nu_accumulated() == b.nu_accumulated()
+        for s in (a, b, c):
+            s.step(n)
+    fa = a.fields()
+    pa = a.populations()
+    for other in (b, c):
+        fb = other.fields()
+        for k in fa:
+            assert np.array_equal(fa[k], fb[k]), k
+        pb = other.populations()
+        assert np.array_equal(pa[0], pb[0]) and np.array_equal(pa[1], pb[1])
+        assert a.nu_accumulated() == other.nu_accumulated()
 
 
 def test_node_pair_kernel_is_refused_for_fp64_and_fp32():
