@@ -650,7 +650,7 @@ int cav_batch_autotune(cav_batch* b, int32_t trial_steps, cav_batch_tuning* chos
         if (p16) {
             for (int r : {1, 2, 4, 8}) add(5, r, 8);
             for (int r : {4, 8})
-                for (int c : {2, 3, 4}) add(6, r, c);
+                for (int c : {3, 4, 5}) add(6, r, c);
         }
         // each candidate timed three times (after its warm-up steps), the
         // median kept: one-off noise cannot pick the winner

@@ -62,7 +62,7 @@ struct TileCav {
     int spin_up;  // scalar-table row of the steady state
 };
 struct TileItem {
-    int cav, x0, y0;
+    int cav, x0, y0, y1;  // rows y0 .. y1 - 1
 };
 
 // ---- mbarrier / TMA (inline PTX) ---------------------------------------------
@@ -316,7 +316,8 @@ inline void tile_items(const std::vector<std::pair<int, int>>& sizes, int ty, st
     out.clear();
     for (int i = 0; i < int(sizes.size()); ++i)
         for (int y0 = 0; y0 < sizes[i].second; y0 += ty)
-            for (int x0 = 0; x0 < sizes[i].first; x0 += TILE_X) out.push_back({i, x0, y0});
+            for (int x0 = 0; x0 < sizes[i].first; x0 += TILE_X)
+                out.push_back({i, x0, y0, std::min(y0 + ty, sizes[i].second)});
 }
 
 }  // namespace cav

@@ -1,12 +1,15 @@
 // tilex.cuh -- the node-pair step on shared-memory tiles staged by TMA
 // (16-bit storage).
 //
-// A CTA owns tiles of 64 columns x TY rows of one cavity: four warps, each
-// a row at a time, each thread the node pair (2 lane, 2 lane + 1) of the
-// tile's row.  The 18 population planes of a tile plus a halo (8 columns on
-// each side, so that the box starts on a 16-byte boundary, and 2 rows, the
-// reach of the g boundary rows) arrive in shared memory with one
-// cp.async.bulk.tensor load completing on an mbarrier.  CTAs are persistent:
+// A CTA owns tiles of 64 columns x (at most) TY rows of one cavity: four
+// warps, each a row at a time, each thread the node pair (2 lane,
+// 2 lane + 1) of the tile's row.  The 18 population planes of a tile plus a
+// halo (8 columns on each side, so that the box starts on a 16-byte
+// boundary, and 1 row) arrive in shared memory with one cp.async.bulk.tensor
+// load completing on an mbarrier.  The g boundary rows 0 / ny-1 read rows up
+// to 2 away (the post-stream g of rows 1 / ny-2); one halo row suffices
+// because every tile is at least two rows tall (tilex_items), so those rows
+// lie inside the tile or its halo.  CTAs are persistent:
 // they stride over the work list and prefetch the next tile into the second
 // stage while the current one is computed, so the population loads of the
 // pull come from shared memory (no DRAM latency in the node's chain) and the
@@ -27,6 +30,18 @@ namespace cav {
 constexpr int TX_W = 64;                   // tile columns (32 node pairs)
 constexpr int TX_BX = TX_W + 2 * TILE_HX;  // box width, halo included (80)
 constexpr int TX_WORDS = TX_BX / 2;        // 32-bit words per staged row (40)
+constexpr int TX_HY = 1;                   // staged y halo
+
+// Interior rows pulled without the y bounce-back selects (a warp-uniform
+// branch on the row).
+#ifndef TILEX_INTERIOR_PULL
+#define TILEX_INTERIOR_PULL 1
+#endif
+
+// Resident CTAs per SM the 4-row tiles' register budget is sized for.
+#ifndef TILEX_R4_CTAS
+#define TILEX_R4_CTAS 5
+#endif
 
 // Warps per CTA of the 8-row tiles (each warp TY / WARPS rows).
 #ifndef TILEX_R8_WARPS
@@ -38,9 +53,9 @@ struct TileXShape {
     static constexpr int TY = TY_;
     static constexpr int WARPS = TY_ == 8 ? TILEX_R8_WARPS : 4;
     // resident CTAs per SM the register budget is sized for
-    static constexpr int MIN_CTAS = WARPS == 8 ? 3 : 4;
+    static constexpr int MIN_CTAS = WARPS == 8 ? 3 : (TY_ == 4 ? TILEX_R4_CTAS : 4);
     static constexpr int THREADS = 32 * WARPS;
-    static constexpr int BY = TY + 2 * TILE_HY;
+    static constexpr int BY = TY + 2 * TX_HY;
     static constexpr int POP_BYTES = NPLANES * BY * TX_BX * 2;  // the populations of the tile and its halo
     static constexpr int FY_BYTES = TY * TX_W * 4;              // the previous Guo force of the tile
     static constexpr int STAGE_BYTES = POP_BYTES + FY_BYTES;
@@ -67,11 +82,13 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
 }
 
 // pull_f_x from a staged tile: trow = the row's position in the stage (halo
-// included), wc = the pair's word column (4 + lane).
-template <int BY>
+// included), wc = the pair's word column (4 + lane).  INTERIOR: the row is
+// neither 0 nor ny - 1 (no bounce-back in y; the caller branches on the
+// row, the same for the whole warp).
+template <int BY, bool INTERIOR = false>
 __device__ __forceinline__ void pull_f_tx(const uint32_t* __restrict__ S, const Geom& G, int ix, int iy, int trow,
                                           int wc, uint32_t (&w)[Q]) {
-    const bool ym = iy > 0, yp = iy < G.ny - 1;
+    const bool ym = INTERIOR || iy > 0, yp = INTERIOR || iy < G.ny - 1;
     const bool x0 = ix == 0, xe = ix + 1 >= G.nx, xl = ix + 2 >= G.nx;
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
@@ -158,10 +175,10 @@ __global__ void __launch_bounds__(TileXShape<TY>::THREADS, TileXShape<TY>::MIN_C
         const int b = (ipar + int(s & 1)) & 1;
         mbar_expect_tx(&bar[st], TS::STAGE_BYTES);
         unsigned char* const d = st ? stage1 : stage0;
-        tma_load_3d(d, maps + 2 * I.cav + b, &bar[st], I.x0 - TILE_HX, I.y0 - TILE_HY, 0);
+        tma_load_3d(d, maps + 2 * I.cav + b, &bar[st], I.x0 - TILE_HX, I.y0 - TX_HY, 0);
         tma_load_2d(d + TS::POP_BYTES, fmaps + I.cav, &bar[st], I.x0, I.y0);
     };
-    TileItem Icur{0, 0, 0}, Inext{0, 0, 0};
+    TileItem Icur{0, 0, 0, 0}, Inext{0, 0, 0, 0};
     if (it0 < it1) {
         Icur = items[it0];
         if (threadIdx.x == 0) issue(Icur, 0);
@@ -201,12 +218,17 @@ __global__ void __launch_bounds__(TileXShape<TY>::THREADS, TileXShape<TY>::MIN_C
             for (int j = 0; j < TY / TS::WARPS; ++j) {
                 const int r = wy + j * TS::WARPS;
                 const int iy = I.y0 + r;
-                if (iy < G.ny) {
-                    const int trow = r + TILE_HY, wc = TILE_HX / 2 + lane;
+                if (iy < I.y1) {
+                    const int trow = r + TX_HY, wc = TILE_HX / 2 + lane;
                     const int gy = iy == 0 ? 1 : (iy == G.ny - 1 ? G.ny - 2 : iy);
                     const float th = ix == 0 ? meta.c.t_hot[gy] : 0.0f;
                     xpair_core<St, WRITE_NUT, false, false>(
-                        [=](uint32_t(&w)[Q]) { pull_f_tx<TS::BY>(S, G, ix, iy, trow, wc, w); },
+                        [=](uint32_t(&w)[Q]) {
+                            if (TILEX_INTERIOR_PULL && iy > 0 && iy < G.ny - 1)
+                                pull_f_tx<TS::BY, true>(S, G, ix, iy, trow, wc, w);
+                            else
+                                pull_f_tx<TS::BY, false>(S, G, ix, iy, trow, wc, w);
+                        },
                         [=](uint32_t(&w)[Q]) { pull_g_tx<TS::BY>(S, G, ix, iy, trow, wc, w); },
                         [](int) { return 0.0f; }, dst, *reinterpret_cast<const float2*>(FY + r * TX_W + 2 * lane),
                         th, meta.cv.fy, meta.cv.nut, nullptr, nullptr, G, ix, iy, meta.c);
@@ -227,12 +249,21 @@ __global__ void __launch_bounds__(TileXShape<TY>::THREADS, TileXShape<TY>::MIN_C
 }
 
 // Tiles of 64 columns x ty rows of every cavity, cavity-major then row block
-// then column block.
+// then column block; where the last row block would be a single row, the
+// block before it gives it one row (every tile at least two rows tall).
 inline void tilex_items(const std::vector<std::pair<int, int>>& sizes, int ty, std::vector<TileItem>& out) {
     out.clear();
-    for (int i = 0; i < int(sizes.size()); ++i)
-        for (int y0 = 0; y0 < sizes[i].second; y0 += ty)
-            for (int x0 = 0; x0 < sizes[i].first; x0 += TX_W) out.push_back({i, x0, y0});
+    for (int i = 0; i < int(sizes.size()); ++i) {
+        const int ny = sizes[i].second;
+        std::vector<std::pair<int, int>> rows;
+        for (int y0 = 0; y0 < ny; y0 += ty) rows.push_back({y0, std::min(y0 + ty, ny)});
+        if (rows.size() > 1 && rows.back().second - rows.back().first == 1) {
+            rows[rows.size() - 2].second -= 1;
+            rows.back().first -= 1;
+        }
+        for (const auto& r : rows)
+            for (int x0 = 0; x0 < sizes[i].first; x0 += TX_W) out.push_back({i, x0, r.first, r.second});
+    }
 }
 
 }  // namespace cav

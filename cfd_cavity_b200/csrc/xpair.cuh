@@ -191,12 +191,15 @@ __device__ __forceinline__ void xpair_core(PF&& pull_f, PG&& pull_g, TAt&& t_at,
 #endif
         const bool h0 = ix == 0, c0 = ix == G.nx - 1, c1 = ix + 1 == G.nx - 1;
         const float tw0 = (h0 ? t_hot_row : c.t_cold) * p2(EG), tw1 = c.t_cold * p2(EG);
+        const float2 tw = make_float2(tw0, tw1);
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
             const float2 v = E::dec(wg[i], Q + i);
-            // wall columns: geq(T_wall, 0, 0) = w_i T_wall (geq_rest)
-            g[i].x = (h0 || c0) ? float(WD(i)) * tw0 : v.x;
-            g[i].y = c1 ? float(WD(i)) * tw1 : v.y;
+            // wall columns: geq(T_wall, 0, 0) = w_i T_wall (geq_rest), both
+            // halves in one packed multiply
+            const float2 wv = lmul(lbc<float2>(float(WD(i))), tw);
+            g[i].x = (h0 || c0) ? wv.x : v.x;
+            g[i].y = c1 ? wv.y : v.y;
         }
     }
     m.t = sum_g<float2>(g);
@@ -217,9 +220,13 @@ __device__ __forceinline__ void xpair_core(PF&& pull_f, PG&& pull_g, TAt&& t_at,
         for (int p = 1; p <= 4; ++p) qv[p] = q_lane<float2>(p, m.ux, m.uy, m15u2);
         collide_g_lane<float2>(g, m.t, m.ux, m.uy, kc.nut, qv, c, nullptr);
     }
+    // the pair's generator: planes 0..8 (f) draw from rng_f, 9..17 (g) from
+    // the same stream nine draws on
+    NodeRng rng_f(0u, 0, 0);
     if constexpr (E::SR) {
-        NodeRng rng = sr_pair_rng(c, G, ix, iy);
-        rng.skip<Q>();  // the f planes' draws come first
+        rng_f = sr_pair_rng(c, G, ix, iy);
+        NodeRng rng = rng_f;
+        rng.skip<Q>();
 #pragma unroll
         for (int q = 0; q < Q; ++q) d[(Q + q) * P2 + k2] = E::enc(g[q], Q + q, rng.next());
     } else {
@@ -239,9 +246,8 @@ __device__ __forceinline__ void xpair_core(PF&& pull_f, PG&& pull_g, TAt&& t_at,
         if (WRITE_NUT) *reinterpret_cast<float2*>(nut + k0) = kc.nut;
     }
     if constexpr (E::SR) {
-        NodeRng rng = sr_pair_rng(c, G, ix, iy);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) d[q * P2 + k2] = E::enc(f[q], q, rng.next());
+        for (int q = 0; q < Q; ++q) d[q * P2 + k2] = E::enc(f[q], q, rng_f.next());
     } else {
 #pragma unroll
         for (int q = 0; q < Q; ++q) d[q * P2 + k2] = E::enc(f[q], q, 0u);
