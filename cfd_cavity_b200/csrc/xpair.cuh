@@ -283,13 +283,117 @@ __device__ __forceinline__ void named_bar_sync(int id, int threads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
 }
 
+// The f half of a split node-pair step: pull of f, macroscopic update,
+// relaxation coefficients, publish (u, v, nu_t), named barrier `bar_id`
+// (64 threads: this warp and its g warp), read T, the f update and its
+// stores (draws 0..8 of the pair).  act: the pair is in the grid (an
+// inactive warp lane still takes the barrier).
+template <class St, bool WRITE_NUT, class PF>
+__device__ __forceinline__ void xpair_f_half(PF&& pull_f, float2* xu, float2* xv, float2* xnut, const float2* xt,
+                                             int bar_id, bool act, St* __restrict__ dst, float2 fy_prev,
+                                             float* fy_out, float* __restrict__ nut, const Geom& G, int ix, int iy,
+                                             const StepScalars<float>& c) {
+    using E = PairEnc<St>;
+    constexpr int EF = Fmt<St>::EF, EG = Fmt<St>::EG;
+    const int k0 = iy * G.pitch + ix, k2 = k0 >> 1;
+    const int P2 = int(G.plane >> 1);
+    uint32_t* __restrict__ d = reinterpret_cast<uint32_t*>(dst);
+    float2 f[Q];
+    Macro<float2, true> m{};
+    CollCoef<float2> kc{};
+    if (act) {
+        uint32_t wf[Q];
+        pull_f(wf);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) f[i] = E::dec(wf[i], i);
+        const bool wy = iy == 0 || iy == G.ny - 1;
+        const Mask2 wall{wy || ix == 0 || ix == G.nx - 1, wy || ix + 1 == G.nx - 1};
+        m = macro_f_lane<float2, EF>(f, fy_prev, wall);
+        kc = collide_f_coef_lane<float2, EF>(f, m, c, nullptr);
+        *xu = m.ux;
+        *xv = m.uy;
+        *xnut = kc.nut;
+    }
+    named_bar_sync(bar_id, 64);
+    if (act) {
+        m.t = *xt;
+        const CollF<float2> o = collide_f_parts_lane<float2, EF>(f, m, kc);
+        const float2 fyv = collide_f_post_lane<float2, EF, EG>(f, o, m, c, m.t);
+        *reinterpret_cast<float2*>(fy_out + k0) = fyv;
+        if (WRITE_NUT) *reinterpret_cast<float2*>(nut + k0) = kc.nut;
+        if constexpr (E::SR) {
+            NodeRng rng = sr_pair_rng(c, G, ix, iy);
+#pragma unroll
+            for (int q = 0; q < Q; ++q) d[q * P2 + k2] = E::enc(f[q], q, rng.next());
+        } else {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) d[q * P2 + k2] = E::enc(f[q], q, 0u);
+        }
+    }
+}
+
+// The g half: pull of g with the boundary conditions (t_hot_row: the hot
+// wall's theta at the row's g source row), T, publish T, the Nusselt
+// accumulation (t_at as in xpair_core), the named barrier, read
+// (u, v, nu_t), the g collision and its stores (draws 9..17 of the pair).
+template <class St, bool ACC_NU, class PG, class TAt>
+__device__ __forceinline__ void xpair_g_half(PG&& pull_g, TAt&& t_at, float2* xt, const float2* xu,
+                                             const float2* xv, const float2* xnut, int bar_id, bool act,
+                                             St* __restrict__ dst, float t_hot_row, double* __restrict__ acc_hot,
+                                             double* __restrict__ acc_cold, const Geom& G, int ix, int iy,
+                                             const StepScalars<float>& c) {
+    using E = PairEnc<St>;
+    constexpr int EG = Fmt<St>::EG;
+    const int k2 = (iy * G.pitch + ix) >> 1;
+    const int P2 = int(G.plane >> 1);
+    uint32_t* __restrict__ d = reinterpret_cast<uint32_t*>(dst);
+    float2 g[Q], t{};
+    if (act) {
+        uint32_t wg[Q];
+        pull_g(wg);
+        const bool h0 = ix == 0, c0 = ix == G.nx - 1, c1 = ix + 1 == G.nx - 1;
+        const float2 tw = make_float2((h0 ? t_hot_row : c.t_cold) * p2(EG), c.t_cold * p2(EG));
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const float2 v = E::dec(wg[i], Q + i);
+            const float2 wv = lmul(lbc<float2>(float(WD(i))), tw);
+            g[i].x = (h0 || c0) ? wv.x : v.x;
+            g[i].y = c1 ? wv.y : v.y;
+        }
+        t = sum_g<float2>(g);
+        *xt = t;
+        if (ACC_NU) {
+            const float t0 = t.x * p2(-EG), t1 = t.y * p2(-EG);
+            if (ix + 1 == 1) acc_hot[iy] += fabs(double(t1) - double(t_at(2)));
+            if (ix == G.nx - 2) acc_cold[iy] += fabs(double(t0) - double(t_at(G.nx - 3)));
+            if (ix + 1 == G.nx - 2) acc_cold[iy] += fabs(double(t1) - double(t_at(G.nx - 3)));
+        }
+    }
+    named_bar_sync(bar_id, 64);
+    if (act) {
+        const float2 u = *xu, v = *xv, nt = *xnut;
+        float2 qv[5];
+        const float2 m15u2 = m15u2_lane<float2>(u, v);
+#pragma unroll
+        for (int p = 1; p <= 4; ++p) qv[p] = q_lane<float2>(p, u, v, m15u2);
+        collide_g_lane<float2>(g, t, u, v, nt, qv, c, nullptr);
+        if constexpr (E::SR) {
+            NodeRng rng = sr_pair_rng(c, G, ix, iy);
+            rng.skip<Q>();
+#pragma unroll
+            for (int q = 0; q < Q; ++q) d[(Q + q) * P2 + k2] = E::enc(g[q], Q + q, rng.next());
+        } else {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) d[(Q + q) * P2 + k2] = E::enc(g[q], Q + q, 0u);
+        }
+    }
+}
+
 template <class St, bool WRITE_NUT, bool ACC_NU>
 __global__ void __launch_bounds__(128) k_fused_xs(const St* __restrict__ src, St* __restrict__ dst,
                                                   float* __restrict__ fy, float* __restrict__ nut,
                                                   double* __restrict__ acc_hot, double* __restrict__ acc_cold, Geom G,
                                                   StepScalars<float> c) {
-    using E = PairEnc<St>;
-    constexpr int EF = Fmt<St>::EF, EG = Fmt<St>::EG;
     __shared__ float2 sh_t[2][32], sh_u[2][32], sh_v[2][32], sh_nut[2][32];
     pdl_wait();
     pdl_trigger();
@@ -298,88 +402,20 @@ __global__ void __launch_bounds__(128) k_fused_xs(const St* __restrict__ src, St
     const int ix = 2 * (blockIdx.x * 32 + lane);
     const int iy = blockIdx.y * 2 + r;
     const bool act = ix < G.nx && iy < G.ny;
-    const int k0 = iy * G.pitch + ix, k2 = k0 >> 1;
-    const int P2 = int(G.plane >> 1);
-    uint32_t* __restrict__ d = reinterpret_cast<uint32_t*>(dst);
     if (role == 0) {
-        float2 f[Q];
-        Macro<float2, true> m{};
-        CollCoef<float2> kc{};
-        if (act) {
-            uint32_t wf[Q];
-            pull_f_x<St>(src, G, ix, iy, wf);
-#pragma unroll
-            for (int i = 0; i < Q; ++i) f[i] = E::dec(wf[i], i);
-            const bool wy = iy == 0 || iy == G.ny - 1;
-            const Mask2 wall{wy || ix == 0 || ix == G.nx - 1, wy || ix + 1 == G.nx - 1};
-            m = macro_f_lane<float2, EF>(f, *reinterpret_cast<const float2*>(fy + k0), wall);
-            kc = collide_f_coef_lane<float2, EF>(f, m, c, nullptr);
-            sh_u[r][lane] = m.ux;
-            sh_v[r][lane] = m.uy;
-            sh_nut[r][lane] = kc.nut;
-        }
-        named_bar_sync(1 + r, 64);
-        if (act) {
-            m.t = sh_t[r][lane];
-            const CollF<float2> o = collide_f_parts_lane<float2, EF>(f, m, kc);
-            const float2 fyv = collide_f_post_lane<float2, EF, EG>(f, o, m, c, m.t);
-            *reinterpret_cast<float2*>(fy + k0) = fyv;
-            if (WRITE_NUT) *reinterpret_cast<float2*>(nut + k0) = kc.nut;
-            if constexpr (E::SR) {
-                NodeRng rng = sr_pair_rng(c, G, ix, iy);
-#pragma unroll
-                for (int q = 0; q < Q; ++q) d[q * P2 + k2] = E::enc(f[q], q, rng.next());
-            } else {
-#pragma unroll
-                for (int q = 0; q < Q; ++q) d[q * P2 + k2] = E::enc(f[q], q, 0u);
-            }
-        }
+        const float2 fy_prev = act ? *reinterpret_cast<const float2*>(fy + iy * G.pitch + ix) : make_float2(0.f, 0.f);
+        xpair_f_half<St, WRITE_NUT>([&](uint32_t(&wf)[Q]) { pull_f_x<St>(src, G, ix, iy, wf); }, &sh_u[r][lane],
+                                    &sh_v[r][lane], &sh_nut[r][lane], &sh_t[r][lane], 1 + r, act, dst, fy_prev, fy,
+                                    nut, G, ix, iy, c);
     } else {
-        float2 g[Q], t{};
-        if (act) {
-            uint32_t wg[Q];
-            pull_g_x<St>(src, G, ix, iy, wg);
-            const int gy = iy == 0 ? 1 : (iy == G.ny - 1 ? G.ny - 2 : iy);
-            const bool h0 = ix == 0, c0 = ix == G.nx - 1, c1 = ix + 1 == G.nx - 1;
-            const float tw0 = (h0 ? c.t_hot[gy] : c.t_cold) * p2(EG), tw1 = c.t_cold * p2(EG);
-#pragma unroll
-            for (int i = 0; i < Q; ++i) {
-                const float2 v = E::dec(wg[i], Q + i);
-                g[i].x = (h0 || c0) ? float(WD(i)) * tw0 : v.x;
-                g[i].y = c1 ? float(WD(i)) * tw1 : v.y;
-            }
-            t = sum_g<float2>(g);
-            sh_t[r][lane] = t;
-            if (ACC_NU) {
-                const float t0 = t.x * p2(-EG), t1 = t.y * p2(-EG);
-                if (ix + 1 == 1) acc_hot[iy] += fabs(double(t1) - double(gather_t<St>(src, G, 2, iy, c)));
-                if (ix == G.nx - 2)
-                    acc_cold[iy] += fabs(double(t0) - double(gather_t<St>(src, G, G.nx - 3, iy, c)));
-                if (ix + 1 == G.nx - 2)
-                    acc_cold[iy] += fabs(double(t1) - double(gather_t<St>(src, G, G.nx - 3, iy, c)));
-            }
-        }
-        named_bar_sync(1 + r, 64);
-        if (act) {
-            const float2 u = sh_u[r][lane], v = sh_v[r][lane], nt = sh_nut[r][lane];
-            float2 qv[5];
-            const float2 m15u2 = m15u2_lane<float2>(u, v);
-#pragma unroll
-            for (int p = 1; p <= 4; ++p) qv[p] = q_lane<float2>(p, u, v, m15u2);
-            collide_g_lane<float2>(g, t, u, v, nt, qv, c, nullptr);
-            if constexpr (E::SR) {
-                NodeRng rng = sr_pair_rng(c, G, ix, iy);
-                rng.skip<Q>();
-#pragma unroll
-                for (int q = 0; q < Q; ++q) d[(Q + q) * P2 + k2] = E::enc(g[q], Q + q, rng.next());
-            } else {
-#pragma unroll
-                for (int q = 0; q < Q; ++q) d[(Q + q) * P2 + k2] = E::enc(g[q], Q + q, 0u);
-            }
-        }
+        const int gy = iy == 0 ? 1 : (iy == G.ny - 1 ? G.ny - 2 : iy);
+        const float th = (act && ix == 0) ? c.t_hot[gy] : 0.0f;
+        xpair_g_half<St, ACC_NU>([&](uint32_t(&wg)[Q]) { pull_g_x<St>(src, G, ix, iy, wg); },
+                                 [&](int x) { return gather_t<St>(src, G, x, iy, c); }, &sh_t[r][lane], &sh_u[r][lane],
+                                 &sh_v[r][lane], &sh_nut[r][lane], 1 + r, act, dst, th, acc_hot, acc_cold, G, ix,
+                                 iy, c);
     }
 }
-
 // The single-cavity step on node pairs: 32 x BY threads cover 64 columns x
 // BY rows.
 template <class St, bool WRITE_NUT, bool ACC_NU, bool NO_COLLIDE>
