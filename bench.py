@@ -220,9 +220,11 @@ def octree_c5(dev, chain=(30_000, 30_000, 60_000), window=40_000, sample_every=1
     (Lx/16) on both vertical walls, levels 3 (L2 strips), Ra = 1e10, FP32
     arithmetic with 16-bit fine-level storage.
 
-    Timing: device time per coarse step (L0 once, L1 twice, L2 four times)
-    for FP64, FP32 and FP32/binary16 storage, from the reference's initial
-    state.  Physics: a cold start at Ra = 1e10 trips the reference's
+    Timing: device time per coarse step (L0 once, L1 twice, L2 twice: the
+    reference sub-cycles L2 in the first L1 sub-step only) for FP64, FP32
+    and FP32/binary16 storage, from the reference's initial state, on two
+    streams (the default) and, for FP32/binary16, also as one launch per
+    level step and coupling on one stream and as one cooperative launch.  Physics: a cold start at Ra = 1e10 trips the reference's
     max_u > 0.10 guard after ~4000 coarse steps in every precision (FP64
     included), so the run follows the reference's own restart chain
     (Ra = 1e8 -> 6.4e8 -> 1e10, set_from_snapshot on the same grid) with the
@@ -244,26 +246,32 @@ def octree_c5(dev, chain=(30_000, 30_000, 60_000), window=40_000, sample_every=1
     phys = (0.71, 0.02, 42)
     out = {"config": "256x1024 base, bl_width 16, levels 3, Ra=1e10, Pr=0.71, utarget 0.02"}
 
-    def timed(prec, n):
+    def timed(prec, n, mode=None):
         s = OctreeSolver(*geo, 1e10, *phys, levels=3, precision=prec, device=dev)
-        i = s.info()
-        upd = i["nx"][0] * i["ny"][0] + 2 * (2 * i["nx"][1] * i["ny"][1]) + 4 * (2 * i["nx"][3] * i["ny"][3])
+        if mode is not None:
+            s.set_step_mode(mode)
+        upd = octree_updates(s)
         s.step_cavity(64)
         st = torch.cuda.ExternalStream(s.stream_handle(), device=dev)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = s.launch_count()
         with torch.cuda.stream(st):
             e0.record(st)
         s.step_cavity(n)
         with torch.cuda.stream(st):
             e1.record(st)
         e1.synchronize()
+        s.sync()
         us = e0.elapsed_time(e1) * 1e3 / n
+        launches = (s.launch_count() - l0) / n
         s.close()
         return {"us_per_coarse_step": us, "node_updates_per_coarse_step": upd, "mlups": upd / us,
-                "launches_per_coarse_step": 10}
+                "launches_per_coarse_step": launches}
 
     for prec, n in (("f64", 512), ("f32", 1024), ("f32_f16", 2048)):
         out[prec] = timed(prec, n)
+    out["f32_f16_one_stream"] = timed("f32_f16", 2048, mode=0)
+    out["f32_f16_one_launch"] = timed("f32_f16", 2048, mode=1)
 
     t0 = time.perf_counter()
     run = {"cs": 0.1, "cs_at_1e10": 0.12, "nu_start_mult_at_1e10": 4.0, "phases": []}
@@ -342,15 +350,29 @@ def batch_only(precision, steps, kernel, rows, ctas):
     return 0
 
 
-def octree_only(coarse_steps):
+def octree_updates(s):
+    """Node updates of one coarse step: L0 once, both L1 blocks twice, both
+    L2 strips twice (ghost rings included, as the level steps run them)."""
+    i = s.info()
+    upd = i["nx"][0] * i["ny"][0] + 2 * (2 * i["nx"][1] * i["ny"][1])
+    if i["levels"] == 3:
+        upd += 2 * (2 * i["nx"][3] * i["ny"][3])
+    return upd
+
+
+def octree_only(coarse_steps, mode):
     """C5 octree timing alone: a few warm-up coarse steps, then
-    `coarse_steps` timed with CUDA events on the octree's stream."""
+    `coarse_steps` timed with CUDA events on the octree's stream (mode 2:
+    two streams, 1: one cooperative launch per coarse step, 0: one launch
+    per phase on one stream)."""
     import torch
 
     from cfd_cavity_b200.octree import OctreeSolver
 
     s = OctreeSolver(256, 1024, 16, 1e10, 0.71, 0.02, 42, levels=3, precision="f32_f16")
+    s.set_step_mode(mode)
     s.step_cavity(3)
+    s.step_cavity(32)  # both graph parities captured before the timed steps
     st = torch.cuda.ExternalStream(s.stream_handle(), device=0)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(st):
@@ -360,7 +382,7 @@ def octree_only(coarse_steps):
         e1.record(st)
     e1.synchronize()
     d = s.diag()
-    print(json.dumps({"workload": "octree 256x1024 bl16 levels 3 Ra=1e10 f32_f16",
+    print(json.dumps({"workload": "octree 256x1024 bl16 levels 3 Ra=1e10 f32_f16", "step_mode": mode,
                       "coarse_steps": coarse_steps,
                       "us_per_coarse_step": e0.elapsed_time(e1) * 1e3 / coarse_steps,
                       "finite": d["finite"]}), flush=True)
@@ -429,6 +451,10 @@ def main():
     ap.add_argument("--chunk", type=int, default=CHUNK)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched-sweep and FP32 extras")
+    ap.add_argument("--octree-mode", type=int, default=2, choices=[0, 1, 2],
+                    help="octree step form of --octree-only: 2 far parts of the level steps on a second "
+                         "stream, 1 one cooperative launch per coarse step, 0 one launch per level step "
+                         "and coupling on one stream")
     ap.add_argument("--octree-only", type=int, default=0, metavar="COARSE_STEPS",
                     help="only time COARSE_STEPS octree coarse steps of the 256x1024 levels-3 cavity "
                          "(FP32 / binary16) and print their device time (profiling runs)")
@@ -442,7 +468,7 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.octree_only:
-        return octree_only(args.octree_only)
+        return octree_only(args.octree_only, args.octree_mode)
     if args.batch_only:
         return batch_only(args.batch_only, args.steps, args.batch_kernel, args.batch_rows, args.batch_ctas)
     world, rank, local, dist = dist_setup(args)
