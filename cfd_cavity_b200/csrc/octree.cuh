@@ -1783,7 +1783,7 @@ struct OctImpl final : Octree {
             CK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
             for (auto& e : sev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         }
-        step_mode = split ? CAV_OCT_STEP_TWO_STREAMS : CAV_OCT_STEP_PER_PHASE;
+        step_mode = CAV_OCT_STEP_PER_PHASE;
         CK(cudaStreamSynchronize(stream));
         init_cavity();
     }

@@ -179,13 +179,12 @@ class OctreeSolver:
         return n.value
 
     def set_step_mode(self, mode):
-        """How a coarse step is launched: ``CAV_OCT_STEP_PER_PHASE`` (one
-        launch per level step and coupling, one stream),
+        """How a coarse step is launched: ``CAV_OCT_STEP_PER_PHASE`` (the
+        default: one launch per level step and coupling, one stream),
         ``CAV_OCT_STEP_ONE_LAUNCH`` (one cooperative launch with grid
-        barriers) or ``CAV_OCT_STEP_TWO_STREAMS`` (the default: the nodes of
-        the level steps that no coupling of the step touches on a second
-        stream beside the chain of couplings); the results are the same bit
-        for bit."""
+        barriers) or ``CAV_OCT_STEP_TWO_STREAMS`` (the nodes of the level
+        steps that no coupling of the step touches on a second stream beside
+        the chain of couplings); the results are the same bit for bit."""
         self._ck(L.load().cav_octree_set_step_mode(self._h, int(mode)))
 
     def step_mode(self):

@@ -422,9 +422,9 @@ int cav_octree_sync(cav_octree* h);
 int cav_octree_get_stream(cav_octree* h, void** stream);
 int cav_octree_launch_count(cav_octree* h, int64_t* n);
 /* How a coarse step is launched (same results bit for bit):
- *   CAV_OCT_STEP_PER_PHASE   one launch per level step and per coupling, in
- *                            the reference's order on one stream (10 with
- *                            levels = 3, 6 with levels = 2);
+ *   CAV_OCT_STEP_PER_PHASE   the default: one launch per level step and per
+ *                            coupling, in the reference's order on one
+ *                            stream (10 with levels = 3, 6 with levels = 2);
  *   CAV_OCT_STEP_ONE_LAUNCH  one cooperative launch per coarse step, the
  *                            phases separated by bounded grid barriers (where
  *                            the device supports cooperative launches; a
@@ -432,11 +432,10 @@ int cav_octree_launch_count(cav_octree* h, int64_t* n);
  *                            CAV_ERR_TIMEOUT by the next cav_octree_sync,
  *                            cav_octree_diag or cav_octree_get_level, the
  *                            steps since then being lost);
- *   CAV_OCT_STEP_TWO_STREAMS the default: the level steps split into the
- *                            nodes next to a coupling, on the chain of
- *                            couplings, and the rest, on a second stream
- *                            beside that chain (14 launches with levels = 3,
- *                            9 with levels = 2).
+ *   CAV_OCT_STEP_TWO_STREAMS the level steps split into the nodes next to
+ *                            a coupling, on the chain of couplings, and the
+ *                            rest, on a second stream beside that chain (14
+ *                            launches with levels = 3, 9 with levels = 2).
  * The dynamic SGS model always runs per phase. */
 #define CAV_OCT_STEP_PER_PHASE 0
 #define CAV_OCT_STEP_ONE_LAUNCH 1

@@ -255,9 +255,9 @@ def test_step_modes_bit_identical(prec, levels):
     a = OctreeSolver(*args, levels=levels, precision=prec, nu_start_mult=2.5)
     b = OctreeSolver(*args, levels=levels, precision=prec, nu_start_mult=2.5)
     c = OctreeSolver(*args, levels=levels, precision=prec, nu_start_mult=2.5)
-    assert a.step_mode() == L.CAV_OCT_STEP_TWO_STREAMS
-    b.set_step_mode(L.CAV_OCT_STEP_PER_PHASE)
     assert b.step_mode() == L.CAV_OCT_STEP_PER_PHASE
+    a.set_step_mode(L.CAV_OCT_STEP_TWO_STREAMS)
+    assert a.step_mode() == L.CAV_OCT_STEP_TWO_STREAMS
     c.set_step_mode(L.CAV_OCT_STEP_ONE_LAUNCH)
     for s in (a, b, c):
         s.step_cavity(1)
