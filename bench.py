@@ -222,10 +222,9 @@ def octree_c5(dev, chain=(30_000, 30_000, 60_000), window=40_000, sample_every=1
 
     Timing: device time per coarse step (L0 once, L1 twice, L2 twice: the
     reference sub-cycles L2 in the first L1 sub-step only) for FP64, FP32
-    and FP32/binary16 storage, from the reference's initial state, one
-    launch per level step and coupling (the default) and, for
-    FP32/binary16, also on two streams and as one cooperative launch.  Physics: a cold start at Ra = 1e10 trips the reference's
-    max_u > 0.10 guard after ~4000 coarse steps in every precision (FP64
+    and FP32/binary16 storage, from the reference's initial state.
+    Physics: a cold start at Ra = 1e10 trips the reference's max_u > 0.10
+    guard after ~4000 coarse steps in every precision (FP64
     included), so the run follows the reference's own restart chain
     (Ra = 1e8 -> 6.4e8 -> 1e10, set_from_snapshot on the same grid) with the
     fixed-Cs Smagorinsky extension on every level (the reference octree has
@@ -246,10 +245,8 @@ def octree_c5(dev, chain=(30_000, 30_000, 60_000), window=40_000, sample_every=1
     phys = (0.71, 0.02, 42)
     out = {"config": "256x1024 base, bl_width 16, levels 3, Ra=1e10, Pr=0.71, utarget 0.02"}
 
-    def timed(prec, n, mode=None):
+    def timed(prec, n):
         s = OctreeSolver(*geo, 1e10, *phys, levels=3, precision=prec, device=dev)
-        if mode is not None:
-            s.set_step_mode(mode)
         upd = octree_updates(s)
         s.step_cavity(64)
         st = torch.cuda.ExternalStream(s.stream_handle(), device=dev)
@@ -270,8 +267,6 @@ def octree_c5(dev, chain=(30_000, 30_000, 60_000), window=40_000, sample_every=1
 
     for prec, n in (("f64", 512), ("f32", 1024), ("f32_f16", 2048)):
         out[prec] = timed(prec, n)
-    out["f32_f16_two_streams"] = timed("f32_f16", 2048, mode=2)
-    out["f32_f16_one_launch"] = timed("f32_f16", 2048, mode=1)
 
     t0 = time.perf_counter()
     run = {"cs": 0.1, "cs_at_1e10": 0.12, "nu_start_mult_at_1e10": 4.0, "phases": []}
@@ -360,17 +355,14 @@ def octree_updates(s):
     return upd
 
 
-def octree_only(coarse_steps, mode):
+def octree_only(coarse_steps):
     """C5 octree timing alone: a few warm-up coarse steps, then
-    `coarse_steps` timed with CUDA events on the octree's stream (mode 2:
-    two streams, 1: one cooperative launch per coarse step, 0: one launch
-    per phase on one stream)."""
+    `coarse_steps` timed with CUDA events on the octree's stream."""
     import torch
 
     from cfd_cavity_b200.octree import OctreeSolver
 
     s = OctreeSolver(256, 1024, 16, 1e10, 0.71, 0.02, 42, levels=3, precision="f32_f16")
-    s.set_step_mode(mode)
     s.step_cavity(3)
     s.step_cavity(32)  # both graph parities captured before the timed steps
     st = torch.cuda.ExternalStream(s.stream_handle(), device=0)
@@ -382,7 +374,7 @@ def octree_only(coarse_steps, mode):
         e1.record(st)
     e1.synchronize()
     d = s.diag()
-    print(json.dumps({"workload": "octree 256x1024 bl16 levels 3 Ra=1e10 f32_f16", "step_mode": mode,
+    print(json.dumps({"workload": "octree 256x1024 bl16 levels 3 Ra=1e10 f32_f16",
                       "coarse_steps": coarse_steps,
                       "us_per_coarse_step": e0.elapsed_time(e1) * 1e3 / coarse_steps,
                       "finite": d["finite"]}), flush=True)
@@ -451,10 +443,6 @@ def main():
     ap.add_argument("--chunk", type=int, default=CHUNK)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched-sweep and FP32 extras")
-    ap.add_argument("--octree-mode", type=int, default=0, choices=[0, 1, 2],
-                    help="octree step form of --octree-only: 2 far parts of the level steps on a second "
-                         "stream, 1 one cooperative launch per coarse step, 0 one launch per level step "
-                         "and coupling on one stream")
     ap.add_argument("--octree-only", type=int, default=0, metavar="COARSE_STEPS",
                     help="only time COARSE_STEPS octree coarse steps of the 256x1024 levels-3 cavity "
                          "(FP32 / binary16) and print their device time (profiling runs)")
@@ -468,7 +456,7 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.octree_only:
-        return octree_only(args.octree_only, args.octree_mode)
+        return octree_only(args.octree_only)
     if args.batch_only:
         return batch_only(args.batch_only, args.steps, args.batch_kernel, args.batch_rows, args.batch_ctas)
     world, rank, local, dist = dist_setup(args)

@@ -35,11 +35,6 @@ namespace cav {
 namespace oct {
 
 constexpr int OT = 128;          // threads per CTA, node kernels
-// Lanes per target node of the couplings: 4 (a lane per stencil node and
-// round, the sums gathered by shuffles) or 1 (every stencil term on the lane).
-#ifndef OCT_CPL
-#define OCT_CPL 4
-#endif
 constexpr int OCT_GRAPH_STEPS = 16;  // even: a replay leaves every buffer parity unchanged
 constexpr int OSTAT = 6;         // per-CTA statistics: min rho, max rho, max |u|, nonfinite, sum (d)rho, unused
 constexpr int OSTAT_CTAS = 64;
@@ -301,10 +296,8 @@ __device__ __forceinline__ void store_pops(St* __restrict__ dst, int n, int k, t
     }
 }
 
-// (No __restrict__: the one-launch coarse step reads, in a later phase of the
-// same launch, buffers that it wrote, so these loads must stay coherent.)
 template <class St>
-__device__ __forceinline__ void load_pops(const St* src, int n, int k, typename Fmt<St>::A (&f)[Q],
+__device__ __forceinline__ void load_pops(const St* __restrict__ src, int n, int k, typename Fmt<St>::A (&f)[Q],
                                           typename Fmt<St>::A (&g)[Q]) {
 #pragma unroll
     for (int i = 0; i < Q; ++i) f[i] = Fmt<St>::load(src[i * n + k], i);
@@ -352,17 +345,16 @@ __device__ __forceinline__ Src src_of(const LvlIO<St>& L, int x, int y) {
     return r;
 }
 
-// Where population q_plane (plane i of f, or Q + i of g) streamed into the
-// node comes from (a plane of the same class: f stays f, g stays g).
+// Population q_plane (plane i of f, or Q + i of g) streamed into the node.
 template <class St>
-__device__ __forceinline__ const St* pull_addr(const LvlIO<St>& L, const Src& r, int q_plane, int i) {
+__device__ __forceinline__ typename Fmt<St>::A pull_one(const LvlIO<St>& L, const Src& r, int q_plane, int i) {
     const int cx = CX(i), cy = CY(i);
     const bool bb = (cx > 0 && r.bb_xm) || (cx < 0 && r.bb_xp) || (cy > 0 && r.bb_ym) || (cy < 0 && r.bb_yp);
     const bool ghost = !bb && ((cx > 0 && r.gh_xm) || (cx < 0 && r.gh_xp));
     const St* base = ghost ? L.ref_in : L.pc_in;
     const int qs = (bb && q_plane < Q) ? OPP(i) : q_plane;
     const int ks = bb ? r.k : r.k - cx - cy * r.nx;
-    return base + qs * L.n + ks;
+    return Fmt<St>::load(base[qs * L.n + ks], qs);
 }
 
 // Post-boundary-condition g of node (x, y).  L0
@@ -371,13 +363,15 @@ __device__ __forceinline__ const St* pull_addr(const LvlIO<St>& L, const Src& r,
 // (apply_thermal_boundary_conditions_block, :543-605): wall column 1 / nx-2
 // geq(T_w); rows 1 / ny-2 copy rows 2 / ny-3 (columns 1..nx-2); ghost
 // columns copy columns 1 / nx-2; ghost rows copy rows 1 / ny-2.  Resolving
-// the copy chain: g(x, y) is the post-stream g of (xs, ys) with xs the
-// column clamped to 1..nx-2 and ys the row clamped to 2..ny-3, or the wall
-// equilibrium geq(tw, 0, 0) when xs is a wall column (*wall).
+// the copy chain: g(x, y) is the post-stream g of (x', y'') with x' the
+// column clamped to 1..nx-2 and y'' the row clamped to 2..ny-3, or the wall
+// equilibrium when x' is a wall column.
 template <class St, bool COARSE>
-__device__ __forceinline__ void g_source(const LvlIO<St>& L, int x, int y, int& xs, int& ys, bool& wall,
-                                         typename Fmt<St>::A& tw) {
+__device__ __forceinline__ void bc_g(const LvlIO<St>& L, int x, int y, const Src& own, typename Fmt<St>::A (&g)[Q]) {
     using A = typename Fmt<St>::A;
+    int xs, ys;
+    bool wall;
+    A tw;
     if constexpr (COARSE) {
         wall = x == 0 || x == L.nx - 1;
         tw = x == 0 ? A(T_HOT_C) : A(T_COLD_C);
@@ -390,6 +384,14 @@ __device__ __forceinline__ void g_source(const LvlIO<St>& L, int x, int y, int& 
         wall = (L.hot && xs == 1) || (L.cold && xs == L.nx - 2);
         tw = (L.hot && xs == 1) ? A(T_HOT_C) : A(T_COLD_C);
     }
+    if (wall) {
+#pragma unroll
+        for (int i = 0; i < Q; ++i) g[i] = geq_full<A>(i, tw, A(0.0), A(0.0), 2);
+    } else {
+        const Src r = (xs == x && ys == y) ? own : src_of<COARSE>(L, xs, ys);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) g[i] = pull_one<St>(L, r, Q + i, i);
+    }
 }
 
 // Row and column of node k of a level with nx columns (exact for k < 2^22).
@@ -401,45 +403,40 @@ __device__ __forceinline__ void split_k(int k, int nx, float inv_nx, int& x, int
 // One (sub-)step of a level: pull + BC + macroscopic (update_macroscopic_guo,
 // src/octree/cavity.rs:252-325) + no-slip (enforce_wall_velocity[_block],
 // :609-656) -> REF; then the level's next collision -> PC.
-// Node (x, y) of L; s0 = the coarse step index (before its increment).
 template <class St, bool COARSE>
-__device__ __forceinline__ void oct_step_node(const LvlIO<St>& L, int x, int y,
-                                              const OctScal<typename Fmt<St>::A>* tab, int S, long long s0, int off,
-                                              int lvl, uint32_t seed, int phase, int collide) {
+__global__ void __launch_bounds__(OT) k_oct_step(LvlPair<St> P, const OctScal<typename Fmt<St>::A>* __restrict__ tab,
+                                                 int S, const long long* __restrict__ step_dev, int off, int lvl,
+                                                 uint32_t seed, int phase, float inv_nx, int collide) {
+    pdl_wait();
+    pdl_trigger();
     using A = typename Fmt<St>::A;
     constexpr bool SH = Fmt<St>::SHIFT;
-    // the collision constants first: the stores below may alias them as far
-    // as the compiler knows
-    const long long s = s0 + off;
-    const LvlScal<A> sc = tab[s < S ? s : S].l[lvl];
-    const int k = y * L.nx + x;
+    const LvlIO<St> L = P.b[blockIdx.y];
+    const int k = blockIdx.x * OT + threadIdx.x;
+    if (k >= L.n) return;
+    // the step index and the collision constants first: the stores below
+    // may alias them as far as the compiler knows
+    long long s;
+    const LvlScal<A> sc = row_of<A>(tab, S, step_dev, off, &s).l[lvl];
+    int x, y;
+    split_k(k, L.nx, inv_nx, x, y);
     const bool ghost = !COARSE && (x == 0 || x == L.nx - 1 || y == 0 || y == L.ny - 1);
     const Src own = src_of<COARSE>(L, x, y);
-    int xs, ys;
-    bool gwall;
-    A tw;
-    g_source<St, COARSE>(L, x, y, xs, ys, gwall, tw);
-    const Src gsrc = (xs == x && ys == y) ? own : src_of<COARSE>(L, xs, ys);
-    // every load of the node issued before any is used: a ghost node keeps
-    // its injected f (REF), the others pull f; g is pulled at the BC source
-    // node (and ignored on a wall column)
-    St rf[Q], rg[Q];
-#pragma unroll
-    for (int i = 0; i < Q; ++i) rf[i] = *(ghost ? L.ref_in + i * L.n + k : pull_addr<St>(L, own, i, i));
-#pragma unroll
-    for (int i = 0; i < Q; ++i) rg[i] = *pull_addr<St>(L, gsrc, Q + i, i);
-    const A fy_prev = L.fy[k];
     A f[Q], g[Q];
+    if (ghost) {
 #pragma unroll
-    for (int i = 0; i < Q; ++i) {
-        f[i] = Fmt<St>::load(rf[i], i);
-        g[i] = gwall ? geq_full<A>(i, tw, A(0.0), A(0.0), 2) : Fmt<St>::load(rg[i], Q + i);
+        for (int i = 0; i < Q; ++i) f[i] = Fmt<St>::load(L.ref_in[i * L.n + k], i);
+    } else {
+#pragma unroll
+        for (int i = 0; i < Q; ++i) f[i] = pull_one<St>(L, own, i, i);
     }
+    bc_g<St, COARSE>(L, x, y, own, g);
     bool wall;
     if constexpr (COARSE)
         wall = x == 0 || x == L.nx - 1 || y == 0 || y == L.ny - 1;
     else
         wall = (L.hot && x == 1) || (L.cold && x == L.nx - 2) || y == 1 || y == L.ny - 2;
+    const A fy_prev = L.fy[k];
     const Macro<A, SH> m = macro_node<A, SH>(f, g, fy_prev, wall);
     store_pops<St>(L.ref_out, L.n, k, f, g, false, 0, 0, 0);
     L.mac[k] = SH ? m.drho : m.rho;
@@ -451,64 +448,6 @@ __device__ __forceinline__ void oct_step_node(const LvlIO<St>& L, int x, int y,
     oct_collide<A, SH>(f, g, m, sc, fy_new);
     L.fy[k] = fy_new;
     store_pops<St>(L.pc_out, L.n, k, f, g, true, seed, s * 16 + phase, (long long)L.node_off + k);
-}
-// The nodes of one level-step launch: all, or the far part of a rectangle
-// (rows [y0, y1] x columns [x0[b], x1[b]] of block b) -- nodes whose step
-// depends on no coupling of the same coarse step and whose outputs no such
-// coupling reads or writes -- or the near part (the rest of the grid).
-// Thread t of block b maps to the t-th node of the part in row-major order.
-struct NodeSet {
-    int mode;  // 0 all, 1 far, 2 near
-    int y0, y1;
-    int x0[2], x1[2];
-};
-__device__ __forceinline__ bool node_of(const NodeSet& ns, int b, int t, int nx, int ny, float inv_nx, int& x,
-                                        int& y) {
-    if (ns.mode == 0) {
-        if (t >= nx * ny) return false;
-        split_k(t, nx, inv_nx, x, y);
-        return true;
-    }
-    const int w = ns.x1[b] - ns.x0[b] + 1, h = ns.y1 - ns.y0 + 1;
-    if (ns.mode == 1) {
-        if (t >= w * h) return false;
-        const int r = t / w;
-        y = ns.y0 + r;
-        x = ns.x0[b] + (t - r * w);
-        return true;
-    }
-    const int c1 = ns.y0 * nx, nl = nx - w, c2 = h * nl;
-    if (t < c1) {
-        y = t / nx;
-        x = t - y * nx;
-        return true;
-    }
-    t -= c1;
-    if (t < c2) {
-        const int r = t / nl, c = t - r * nl;
-        y = ns.y0 + r;
-        x = c < ns.x0[b] ? c : c + w;
-        return true;
-    }
-    t -= c2;
-    if (t >= (ny - 1 - ns.y1) * nx) return false;
-    const int r = t / nx;
-    y = ns.y1 + 1 + r;
-    x = t - r * nx;
-    return true;
-}
-
-template <class St, bool COARSE>
-__global__ void __launch_bounds__(OT) k_oct_step(LvlPair<St> P, NodeSet ns,
-                                                 const OctScal<typename Fmt<St>::A>* __restrict__ tab, int S,
-                                                 const long long* __restrict__ step_dev, int off, int lvl,
-                                                 uint32_t seed, int phase, float inv_nx, int collide) {
-    pdl_wait();
-    pdl_trigger();
-    const LvlIO<St>& L = P.b[blockIdx.y];
-    int x, y;
-    if (!node_of(ns, blockIdx.y, blockIdx.x * OT + threadIdx.x, L.nx, L.ny, inv_nx, x, y)) return;
-    oct_step_node<St, COARSE>(L, x, y, tab, S, *step_dev, off, lvl, seed, phase, collide);
 }
 
 // Collision of the REF state into PC: the first collision after the state
@@ -638,49 +577,37 @@ __device__ __forceinline__ void group_sum(A (&c)[NC]) {
 // interpolated, rescaled non-equilibrium parts; then its moments are
 // refreshed from the injected populations.  Four lanes per ghost, one per
 // stencil node.
-// Thread t of block blk's ghosts (4 per ghost); s0 = the coarse step index.
 template <class StC, class StF>
-__device__ __forceinline__ void oct_c2f_thread(const LvlIO<StC>& Lc, const LvlIO<StF>& Lf, int t, int blk,
-                                               const GhostE<typename Fmt<StF>::A>* __restrict__ tab, int n_ghost,
-                                               Xi<typename Fmt<StF>::A> xi_h,
-                                               const Xi<typename Fmt<StF>::A>* __restrict__ xi_dev, long long s0,
-                                               uint32_t seed, int phase) {
+__global__ void __launch_bounds__(OT) k_oct_c2f(LvlPair<StC> C, LvlPair<StF> F,
+                                                const GhostE<typename Fmt<StF>::A>* __restrict__ tab, int n_ghost,
+                                                Xi<typename Fmt<StF>::A> xi_h,
+                                                const Xi<typename Fmt<StF>::A>* __restrict__ xi_dev,
+                                                const long long* __restrict__ step_dev, uint32_t seed, int phase) {
+    pdl_wait();
+    pdl_trigger();
     using A = typename Fmt<StF>::A;
     constexpr bool SH = Fmt<StF>::SHIFT;
     static_assert(Fmt<StC>::SHIFT == SH, "levels share one convention");
-    constexpr int LN = OCT_CPL;
-    const int j = LN == 4 ? t >> 2 : t, s = LN == 4 ? t & 3 : 0;
-    if ((t & ~31) >= LN * n_ghost) return;  // whole warp past the end
+    const int t = blockIdx.x * OT + threadIdx.x;
+    const int j = t >> 2, s = t & 3;
+    if ((t & ~31) >= 4 * n_ghost) return;  // whole warp past the end
     const bool act = j < n_ghost;
-    const long long key = s0 * 16 + phase;
+    const LvlIO<StC> Lc = C.b[blockIdx.y];
+    const LvlIO<StF> Lf = F.b[blockIdx.y];
+    const long long key = *step_dev * 16 + phase;
     A c[NC];
     int kf = 0;
-    if constexpr (LN == 4) {
-        if (act) {
-            const GhostE<A>& e = tab[blk * n_ghost + j];
-            kf = e.kf;
-            stencil_term<StC>(Lc, e.kc[s], e.w[s], c);
-        } else {
-#pragma unroll
-            for (int m = 0; m < NC; ++m) c[m] = A(0.0);
-        }
-        group_sum<A, 4, 4>(c);
-    } else {
-        // one lane per ghost: the four stencil terms summed in stencil order
-        if (!act) return;
-        const GhostE<A>& e = tab[blk * n_ghost + j];
+    if (act) {
+        const GhostE<A>& e = tab[blockIdx.y * n_ghost + j];
         kf = e.kf;
-        stencil_term<StC>(Lc, e.kc[0], e.w[0], c);
+        stencil_term<StC>(Lc, e.kc[s], e.w[s], c);
+    } else {
 #pragma unroll
-        for (int q = 1; q < 4; ++q) {
-            A term[NC];
-            stencil_term<StC>(Lc, e.kc[q], e.w[q], term);
-#pragma unroll
-            for (int m = 0; m < NC; ++m) c[m] = c[m] + term[m];
-        }
+        for (int m = 0; m < NC; ++m) c[m] = A(0.0);
     }
+    group_sum<A, 4, 4>(c);
     if (!act || s != 0) return;
-    const Xi<A> xi = xi_dev ? xi_dev[blk] : xi_h;
+    const Xi<A> xi = xi_dev ? xi_dev[blockIdx.y] : xi_h;
     const A rho = c[0], ux = c[1], uy = c[2], tt = c[3];
     A fn[Q], fr[Q], f[Q], g[Q];
 #pragma unroll
@@ -698,19 +625,6 @@ __device__ __forceinline__ void oct_c2f_thread(const LvlIO<StC>& Lc, const LvlIO
     Lf.mac[2 * Lf.n + kf] = m.uy;
     Lf.mac[3 * Lf.n + kf] = m.t;
 }
-template <class StC, class StF>
-__global__ void __launch_bounds__(OT) k_oct_c2f(LvlPair<StC> C, LvlPair<StF> F,
-                                                const GhostE<typename Fmt<StF>::A>* __restrict__ tab, int n_ghost,
-                                                Xi<typename Fmt<StF>::A> xi_h,
-                                                const Xi<typename Fmt<StF>::A>* __restrict__ xi_dev,
-                                                const long long* __restrict__ step_dev, uint32_t seed, int phase) {
-    pdl_wait();
-    pdl_trigger();
-    const int t = blockIdx.x * OT + threadIdx.x;
-    if ((t & ~31) >= OCT_CPL * n_ghost) return;  // whole warp past the end
-    oct_c2f_thread<StC, StF>(C.b[blockIdx.y], F.b[blockIdx.y], t, blockIdx.y, tab, n_ghost, xi_h, xi_dev, *step_dev,
-                             seed, phase);
-}
 
 // fine_to_coarse (src/octree/interface.rs:175-206) + refresh of the
 // coincident node (src/octree/solver.rs:874-876, 936-942) + that node's next
@@ -718,48 +632,36 @@ __global__ void __launch_bounds__(OT) k_oct_c2f(LvlPair<StC> C, LvlPair<StF> F,
 // collisions run after its own model evaluation).  Four lanes per coincident node
 // (eight nodes per warp): lane l takes the stencil nodes l, l + 4 (and 8 for
 // lane 0) in three rounds, and the round sums are added in stencil order.
-// Thread t of block blk's coincident nodes (4 per node); s0 = the coarse
-// step index.
 template <class StF, class StC>
-__device__ __forceinline__ void oct_f2c_thread(const LvlIO<StF>& Lf, const LvlIO<StC>& Lc, int t, int blk,
-                                               const CoinE* __restrict__ tab, int n0, int n1,
-                                               Xi<typename Fmt<StF>::A> xi_h,
-                                               const Xi<typename Fmt<StF>::A>* __restrict__ xi_dev,
-                                               const OctScal<typename Fmt<StF>::A>* __restrict__ stab, int S,
-                                               long long s0, int off, int lvl_c, uint32_t seed, int phase,
-                                               int collide) {
+__global__ void __launch_bounds__(OT) k_oct_f2c(LvlPair<StF> F, LvlPair<StC> C, const CoinE* __restrict__ tab, int n0,
+                                                int n1, Xi<typename Fmt<StF>::A> xi_h,
+                                                const Xi<typename Fmt<StF>::A>* __restrict__ xi_dev,
+                                                const OctScal<typename Fmt<StF>::A>* __restrict__ stab, int S,
+                                                const long long* __restrict__ step_dev, int off, int lvl_c,
+                                                uint32_t seed, int phase, int collide) {
+    pdl_wait();
+    pdl_trigger();
     using A = typename Fmt<StF>::A;
     constexpr bool SH = Fmt<StF>::SHIFT;
-    constexpr int LN = OCT_CPL;
-    const int j = LN == 4 ? t >> 2 : t, l = LN == 4 ? t & 3 : 0;
+    const int t = blockIdx.x * OT + threadIdx.x;
+    const int j = t >> 2, l = t & 3;
+    const int blk = blockIdx.y;
     const int nb = blk == 0 ? n0 : n1;
-    if ((t & ~31) >= LN * nb) return;  // whole warp past the end
+    if ((t & ~31) >= 4 * nb) return;  // whole warp past the end
     const bool act_e = j < nb;
-    if (LN == 1 && !act_e) return;
+    const LvlIO<StF> Lf = F.b[blk];
+    const LvlIO<StC> Lc = C.b[blk];
     CoinE e{0, 0, 0};
     if (act_e) e = tab[(blk == 0 ? 0 : n0) + j];
-    const long long sidx = s0 + off;
-    const LvlScal<A> sc = stab[sidx < S ? sidx : S].l[lvl_c];
+    long long sidx;
+    const LvlScal<A> sc = row_of<A>(stab, S, step_dev, off, &sidx).l[lvl_c];
     const int base = (threadIdx.x & 31) & ~3;
     const A ww[3] = {A(0.25), A(0.5), A(0.25)};
     A c[NC];
 #pragma unroll
     for (int m = 0; m < NC; ++m) c[m] = A(0.0);
-    if constexpr (LN == 1) {
-        // one lane per coincident node: the nine stencil terms summed in
-        // stencil order
 #pragma unroll
-        for (int st = 0; st < 9; ++st) {
-            const int jb = st / 3, ja = st - 3 * jb;
-            const int kf = (e.b + jb - 1) * Lf.nx + (e.a + ja - 1);
-            A term[NC];
-            stencil_term<StF>(Lf, kf, ww[ja] * ww[jb], term);
-#pragma unroll
-            for (int m = 0; m < NC; ++m) c[m] = st == 0 ? term[m] : c[m] + term[m];
-        }
-    }
-#pragma unroll
-    for (int round = 0; round < (LN == 4 ? 3 : 0); ++round) {
+    for (int round = 0; round < 3; ++round) {
         const int st = 4 * round + l;  // this lane's stencil node in this round
         A term[NC];
         if (act_e && st < 9) {
@@ -806,204 +708,6 @@ __device__ __forceinline__ void oct_f2c_thread(const LvlIO<StF>& Lf, const LvlIO
     oct_collide<A, SH>(f, g, m, sc, fy_new);
     Lc.fy[e.kc] = fy_new;
     store_pops<StC>(Lc.pc_out, Lc.n, e.kc, f, g, true, seed, sidx * 16 + phase + 1, (long long)Lc.node_off + e.kc);
-}
-template <class StF, class StC>
-__global__ void __launch_bounds__(OT) k_oct_f2c(LvlPair<StF> F, LvlPair<StC> C, const CoinE* __restrict__ tab, int n0,
-                                                int n1, Xi<typename Fmt<StF>::A> xi_h,
-                                                const Xi<typename Fmt<StF>::A>* __restrict__ xi_dev,
-                                                const OctScal<typename Fmt<StF>::A>* __restrict__ stab, int S,
-                                                const long long* __restrict__ step_dev, int off, int lvl_c,
-                                                uint32_t seed, int phase, int collide) {
-    pdl_wait();
-    pdl_trigger();
-    const int t = blockIdx.x * OT + threadIdx.x;
-    if ((t & ~31) >= OCT_CPL * (blockIdx.y == 0 ? n0 : n1)) return;  // whole warp past the end
-    oct_f2c_thread<StF, StC>(F.b[blockIdx.y], C.b[blockIdx.y], t, blockIdx.y, tab, n0, n1, xi_h, xi_dev, stab, S,
-                             *step_dev, off, lvl_c, seed, phase, collide);
-}
-
-// ---------------------------------------------------------------------------
-// One coarse step in one cooperative launch (k_oct_coarse).  The phases of
-// launch_coarse_step -- L0 step, c2f L0 -> L1, L1 sub-step, [c2f L1 -> L2,
-// two L2 sub-steps, f2c L2 -> L1], L1 sub-step, f2c L1 -> L0 -- run in
-// order, separated by grid-wide barriers, and each phase runs the same
-// per-node code as its own kernel (oct_step_node, oct_c2f_thread,
-// oct_f2c_thread), so the results are those of the ten launches bit for bit.
-// A CTA is GROUPS groups of OT threads; group g of CTA b takes the phase's
-// OT-thread work units g * gridDim.x + b, then every gridDim.x * GROUPS-th
-// (a phase with fewer units than groups spreads them over all SMs).
-// The step counter is read by every CTA before the first barrier and
-// advanced by CTA 0 after it.  Every barrier wait is bounded (OCF_WAIT_NS):
-// a CTA that gives up sets *err, the others see it and leave, and the later
-// launches of the same graph return at once; the host reports the lost
-// steps as CAV_ERR_TIMEOUT.
-// ---------------------------------------------------------------------------
-constexpr unsigned long long OCF_WAIT_NS = 1000000000ull;
-template <class A>
-struct OcfShape {
-    static constexpr int GROUPS = sizeof(A) == 8 ? 2 : 4;  // FP64 keeps up to 255 registers a thread
-    static constexpr int THREADS = OT * GROUPS;
-};
-
-template <class StC, class StF>
-struct CoarseArgs {
-    using A = typename Fmt<StF>::A;
-    LvlPair<StC> l0;             // L0 step
-    LvlPair<StC> c1c;            // c2f L0 -> L1: coarse side
-    LvlPair<StF> c1f;            //               fine side
-    LvlPair<StF> l1a, l1b;       // the two L1 sub-steps
-    LvlPair<StF> c2c, c2f;       // c2f L1 -> L2
-    LvlPair<StF> l2a, l2b;       // the two L2 sub-steps
-    LvlPair<StF> f2f, f2c;       // f2c L2 -> L1: fine, coarse side
-    LvlPair<StF> f1f;            // f2c L1 -> L0: fine side
-    LvlPair<StC> f1c;            //               coarse side
-    const OctScal<A>* tab;
-    const GhostE<A>* gh1;
-    const GhostE<A>* gh2;
-    const CoinE* co1;
-    const CoinE* co2;
-    const Xi<A>* xia_dev;        // nullptr: xa
-    const Xi<A>* xib_dev;        // nullptr: xb
-    Xi<A> xa, xb;
-    long long* step_dev;
-    unsigned* bar;               // arrival word of the grid barrier
-    unsigned* err;               // set when a barrier wait gave up
-    int S, levels, n_ghost, n_ghost2, n_co0, n_co1, n_co2_0, n_co2_1;
-    float inv_nx0, inv_nx1, inv_nx2;
-    uint32_t seed;
-};
-
-__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ unsigned long long oct_global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-// Grid-wide barrier of a cooperative launch.  CTA 0 adds 2^31 - (CTAs - 1)
-// to the arrival word, every other CTA adds 1, so bit 31 of the word flips
-// exactly when the last CTA has arrived and the low bits return to their
-// value (the word never needs a reset).  The writes of the CTA before the
-// barrier are released by thread 0's fence before its arrival; the reads
-// after it are ordered by the acquire loads and the fence after the wait.
-// Bounded: false when this wait gave up (after OCF_WAIT_NS, *err set) or
-// another CTA's did (*err seen).
-__device__ __forceinline__ bool grid_sync_bounded(unsigned* bar, unsigned* err) {
-    __syncthreads();
-    int ok = 1;
-    if (threadIdx.x == 0) {
-        const unsigned nb = gridDim.x;
-        const unsigned add = blockIdx.x == 0 ? 0x80000000u - (nb - 1u) : 1u;
-        __threadfence();
-        const unsigned old = atomicAdd(bar, add);
-        unsigned long long t0 = 0;
-        for (unsigned it = 0;; ++it) {
-            if ((ld_acquire_gpu(bar) ^ old) & 0x80000000u) break;
-            if ((it & 63u) == 63u) {
-                if (ld_acquire_gpu(err)) {
-                    ok = 0;
-                    break;
-                }
-                const unsigned long long t = oct_global_ns();
-                if (t0 == 0) {
-                    t0 = t;
-                } else if (t - t0 > OCF_WAIT_NS) {
-                    atomicOr(err, 1u);
-                    ok = 0;
-                    break;
-                }
-            }
-        }
-        __threadfence();
-    }
-    return __syncthreads_and(ok) != 0;
-}
-
-// Level step over both blocks of a pair (nb = 1: L0) in work units of OT nodes.
-template <class St, bool COARSE>
-__device__ __forceinline__ void ocf_step(const LvlPair<St>& P, int nb, const OctScal<typename Fmt<St>::A>* tab, int S,
-                                         long long s0, int off, int lvl, uint32_t seed, int phase, float inv_nx,
-                                         int u0, int us, int tid) {
-    const int gx = (P.b[0].n + OT - 1) / OT;
-    for (int u = u0; u < nb * gx; u += us) {
-        const int by = u >= gx ? 1 : 0, bx = u - by * gx;
-        const int k = bx * OT + tid;
-        if (k < P.b[by].n) {
-            int x, y;
-            split_k(k, P.b[by].nx, inv_nx, x, y);
-            oct_step_node<St, COARSE>(P.b[by], x, y, tab, S, s0, off, lvl, seed, phase, 1);
-        }
-    }
-}
-
-template <class StC, class StF>
-__global__ void __launch_bounds__(OcfShape<typename Fmt<StF>::A>::THREADS, 1) k_oct_coarse(CoarseArgs<StC, StF> a) {
-    using A = typename Fmt<StF>::A;
-    constexpr int G = OcfShape<A>::GROUPS;
-    if (ld_acquire_gpu(a.err)) return;  // an earlier launch gave up: its steps are lost already
-    const int tid = threadIdx.x % OT;
-    // units spread over the SMs first: group g of CTA b starts at unit g * gridDim.x + b
-    const int u0 = (threadIdx.x / OT) * gridDim.x + blockIdx.x, us = gridDim.x * G;
-    const long long s0 = *(volatile long long*)a.step_dev;
-
-    ocf_step<StC, true>(a.l0, 1, a.tab, a.S, s0, 1, 0, a.seed, 1, a.inv_nx0, u0, us, tid);
-    if (!grid_sync_bounded(a.bar, a.err)) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) *a.step_dev = s0 + 1;
-
-    {  // c2f L0 -> L1 (four threads per ghost)
-        const int gx = (OCT_CPL * a.n_ghost + OT - 1) / OT;
-        for (int u = u0; u < 2 * gx; u += us) {
-            const int by = u >= gx ? 1 : 0;
-            const int t = (u - by * gx) * OT + tid;
-            oct_c2f_thread<StC, StF>(a.c1c.b[by], a.c1f.b[by], t, by, a.gh1, a.n_ghost, a.xa, a.xia_dev, s0, a.seed,
-                                     2);
-        }
-    }
-    if (!grid_sync_bounded(a.bar, a.err)) return;
-    ocf_step<StF, false>(a.l1a, 2, a.tab, a.S, s0, 0, 1, a.seed, 3, a.inv_nx1, u0, us, tid);
-    if (!grid_sync_bounded(a.bar, a.err)) return;
-
-    if (a.levels == 3) {
-        {  // c2f L1 -> L2
-            const int gx = (OCT_CPL * a.n_ghost2 + OT - 1) / OT;
-            for (int u = u0; u < 2 * gx; u += us) {
-                const int by = u >= gx ? 1 : 0;
-                const int t = (u - by * gx) * OT + tid;
-                oct_c2f_thread<StF, StF>(a.c2c.b[by], a.c2f.b[by], t, by, a.gh2, a.n_ghost2, a.xb, a.xib_dev, s0,
-                                         a.seed, 4);
-            }
-        }
-        if (!grid_sync_bounded(a.bar, a.err)) return;
-        ocf_step<StF, false>(a.l2a, 2, a.tab, a.S, s0, 0, 2, a.seed, 5, a.inv_nx2, u0, us, tid);
-        if (!grid_sync_bounded(a.bar, a.err)) return;
-        ocf_step<StF, false>(a.l2b, 2, a.tab, a.S, s0, 1, 2, a.seed, 6, a.inv_nx2, u0, us, tid);
-        if (!grid_sync_bounded(a.bar, a.err)) return;
-        {  // f2c L2 -> L1 (+ refresh and next collision of the coincident nodes)
-            const int gx = (OCT_CPL * (a.n_co2_0 > a.n_co2_1 ? a.n_co2_0 : a.n_co2_1) + OT - 1) / OT;
-            for (int u = u0; u < 2 * gx; u += us) {
-                const int by = u >= gx ? 1 : 0;
-                const int t = (u - by * gx) * OT + tid;
-                oct_f2c_thread<StF, StF>(a.f2f.b[by], a.f2c.b[by], t, by, a.co2, a.n_co2_0, a.n_co2_1, a.xb,
-                                         a.xib_dev, a.tab, a.S, s0, 0, 1, a.seed, 7, 1);
-            }
-        }
-        if (!grid_sync_bounded(a.bar, a.err)) return;
-    }
-
-    ocf_step<StF, false>(a.l1b, 2, a.tab, a.S, s0, 1, 1, a.seed, 9, a.inv_nx1, u0, us, tid);
-    if (!grid_sync_bounded(a.bar, a.err)) return;
-    {  // f2c L1 -> L0
-        const int gx = (OCT_CPL * (a.n_co0 > a.n_co1 ? a.n_co0 : a.n_co1) + OT - 1) / OT;
-        for (int u = u0; u < 2 * gx; u += us) {
-            const int by = u >= gx ? 1 : 0;
-            const int t = (u - by * gx) * OT + tid;
-            oct_f2c_thread<StF, StC>(a.f1f.b[by], a.f1c.b[by], t, by, a.co1, a.n_co0, a.n_co1, a.xa, a.xia_dev,
-                                     a.tab, a.S, s0, 1, 0, a.seed, 13, 1);
-        }
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1385,8 +1089,6 @@ struct Octree {
     virtual void set_dynamic_sgs(bool on, double smag_alpha, double nu_sm_min, double eta_test) = 0;
     virtual void dynamic_stats(double* out14) = 0;
     virtual void get_nut(int lvl, double* nut, double* at) = 0;
-    virtual void set_step_mode(int mode) = 0;
-    virtual int get_step_mode() const = 0;
 
     cav_octree_params p{};
     int levels = 2, nx0 = 0, ny0 = 0, nx1 = 0, ny1 = 0, nx2 = 0, ny2 = 0;
@@ -1514,16 +1216,6 @@ struct OctImpl final : Octree {
     bool pc_valid = false;
     Xi<A> xa{}, xb{};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    // two-stream coarse step: the side stream, its events and the far parts
-    cudaStream_t side = nullptr;
-    cudaEvent_t sev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-    bool split = false;
-    NodeSet far0{}, far1a{}, far1b{}, far2a{};
-    // one-launch coarse step (k_oct_coarse): barrier word and error flag,
-    // resident CTAs, and the step form in use
-    unsigned* ocf_flags = nullptr;
-    int ocf_grid = 0;
-    int step_mode = CAV_OCT_STEP_PER_PHASE;
     // dynamic mixed-scale SGS model (set_dynamic_sgs, src/octree/solver.rs:476-481)
     bool dyn = false;
     double dyn_alpha = 0.5, dyn_min = -0.1, dyn_eta = 2.0;
@@ -1546,9 +1238,6 @@ struct OctImpl final : Octree {
         for (auto& gx : dgraph)
             if (gx) cudaGraphExecDestroy(gx);
         for (void* b : allocs) cudaFree(b);
-        for (auto& e : sev)
-            if (e) cudaEventDestroy(e);
-        if (side) cudaStreamDestroy(side);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -1767,23 +1456,6 @@ struct OctImpl final : Octree {
         iface = dalloc<double>(8);
         dout = dalloc<double>(16);
         rowbuf = dalloc<double>(size_t(5) * std::max(std::max(ny0, ny1), levels == 3 ? ny2 : 0));
-        ocf_flags = dalloc<unsigned>(2);
-        {
-            // one cooperative launch per coarse step: as many CTAs as are
-            // resident together (0: the multi-launch step only)
-            int dev = 0, n_sm = 0, occ = 0, coop = 0;
-            CK(cudaGetDevice(&dev));
-            CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
-            CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_oct_coarse<StC, StF>, OcfShape<A>::THREADS, 0));
-            ocf_grid = coop ? occ * n_sm : 0;
-        }
-        split = plan_split(g1, g2);
-        if (split) {
-            CK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
-            for (auto& e : sev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        }
-        step_mode = CAV_OCT_STEP_PER_PHASE;
         CK(cudaStreamSynchronize(stream));
         init_cavity();
     }
@@ -1926,15 +1598,11 @@ struct OctImpl final : Octree {
     // pdl_wait(), so a launch overlaps only the tail of its predecessor).
     template <typename... KArgs, typename... Args>
     void launch(void (*kern)(KArgs...), dim3 grid, Args... args) {
-        launch_on(stream, kern, grid, args...);
-    }
-    template <typename... KArgs, typename... Args>
-    void launch_on(cudaStream_t st, void (*kern)(KArgs...), dim3 grid, Args... args) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = grid;
         cfg.blockDim = dim3(OT);
         cfg.dynamicSmemBytes = 0;
-        cfg.stream = st;
+        cfg.stream = stream;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
         attr[0].val.programmaticStreamSerializationAllowed = 1;
@@ -1983,202 +1651,47 @@ struct OctImpl final : Octree {
     void c2f_L1() {
         LvlPair<StC> c = pair_cur(L0, L0);
         LvlPair<StF> f = pair_cur(L1[0], L1[1]);
-        launch(k_oct_c2f<StC, StF>, grid_of(OCT_CPL * n_ghost, 2), c, f, (const GhostE<A>*)gh1, n_ghost, xa, xi_a_dev(),
+        launch(k_oct_c2f<StC, StF>, grid_of(4 * n_ghost, 2), c, f, (const GhostE<A>*)gh1, n_ghost, xa, xi_a_dev(),
                (const long long*)step_dev, seed32, 2);
     }
     void c2f_L2() {
         LvlPair<StF> c = pair_cur(L1[0], L1[1]);
         LvlPair<StF> f = pair_cur(L2[0], L2[1]);
-        launch(k_oct_c2f<StF, StF>, grid_of(OCT_CPL * n_ghost2, 2), c, f, (const GhostE<A>*)gh2, n_ghost2, xb, xi_b_dev(),
+        launch(k_oct_c2f<StF, StF>, grid_of(4 * n_ghost2, 2), c, f, (const GhostE<A>*)gh2, n_ghost2, xb, xi_b_dev(),
                (const long long*)step_dev, seed32, 4);
     }
     void f2c_L2(int off) {
         LvlPair<StF> f = pair_cur(L2[0], L2[1]);
         LvlPair<StF> c = pair_cur(L1[0], L1[1]);
-        launch(k_oct_f2c<StF, StF>, grid_of(OCT_CPL * std::max(n_co2_0, n_co2_1), 2), f, c, (const CoinE*)co2, n_co2_0,
+        launch(k_oct_f2c<StF, StF>, grid_of(4 * std::max(n_co2_0, n_co2_1), 2), f, c, (const CoinE*)co2, n_co2_0,
                n_co2_1, xb, xi_b_dev(), (const OctScal<A>*)tab, S, (const long long*)step_dev, off, 1, seed32, 7,
                int(!dyn));
     }
     void f2c_L1(int off) {
         LvlPair<StF> f = pair_cur(L1[0], L1[1]);
         LvlPair<StC> c = pair_cur(L0, L0);
-        launch(k_oct_f2c<StF, StC>, grid_of(OCT_CPL * std::max(n_co0, n_co1), 2), f, c, (const CoinE*)co1, n_co0, n_co1,
+        launch(k_oct_f2c<StF, StC>, grid_of(4 * std::max(n_co0, n_co1), 2), f, c, (const CoinE*)co1, n_co0, n_co1,
                xa, xi_a_dev(), (const OctScal<A>*)tab, S, (const long long*)step_dev, off, 0, seed32, 13, int(!dyn));
     }
-    // Nodes of a part per block (both blocks of a part have the same count).
-    static int part_count(const NodeSet& ns, int nx, int ny) {
-        if (ns.mode == 0) return nx * ny;
-        const int fw = (ns.x1[0] - ns.x0[0] + 1) * (ns.y1 - ns.y0 + 1);
-        return ns.mode == 1 ? fw : nx * ny - fw;
-    }
-    static NodeSet all_nodes() {
-        NodeSet n{};
-        n.mode = 0;
-        return n;
-    }
-    static NodeSet as_mode(NodeSet n, int mode) {
-        n.mode = mode;
-        return n;
-    }
-    // One level step (or one part of it) of pair q on stream st.
-    template <class St, bool COARSE>
-    void step_part(cudaStream_t st, const LvlPair<St>& q, int nb, const NodeSet& ns, int off, int lvl, int phase) {
-        const LvlIO<St>& l = q.b[0];
-        launch_on(st, k_oct_step<St, COARSE>, grid_of(part_count(ns, l.nx, l.ny), nb), q, ns, (const OctScal<A>*)tab,
-                  S, (const long long*)step_dev, off, lvl, seed32, phase, 1.0f / float(l.nx), int(!dyn));
-    }
     void step_L0() {
-        step_part<StC, true>(stream, pair(L0, L0), 1, all_nodes(), 1, 0, 1);
+        LvlPair<StC> q = pair(L0, L0);
+        launch(k_oct_step<StC, true>, grid_of(L0.n, 1), q, (const OctScal<A>*)tab, S, (const long long*)step_dev, 1,
+               0, seed32, 1, 1.0f / float(L0.nx), int(!dyn));
         L0.cur ^= 1;
     }
     void step_L1(int off, int phase) {
-        step_part<StF, false>(stream, pair(L1[0], L1[1]), 2, all_nodes(), off, 1, phase);
+        LvlPair<StF> q = pair(L1[0], L1[1]);
+        launch(k_oct_step<StF, false>, grid_of(L1[0].n, 2), q, (const OctScal<A>*)tab, S,
+               (const long long*)step_dev, off, 1, seed32, phase, 1.0f / float(L1[0].nx), int(!dyn));
         L1[0].cur ^= 1;
         L1[1].cur ^= 1;
     }
     void step_L2(int off, int phase) {
-        step_part<StF, false>(stream, pair(L2[0], L2[1]), 2, all_nodes(), off, 2, phase);
+        LvlPair<StF> q = pair(L2[0], L2[1]);
+        launch(k_oct_step<StF, false>, grid_of(L2[0].n, 2), q, (const OctScal<A>*)tab, S,
+               (const long long*)step_dev, off, 2, seed32, phase, 1.0f / float(L2[0].nx), int(!dyn));
         L2[0].cur ^= 1;
         L2[1].cur ^= 1;
-    }
-
-    // One step_cavity on two streams: the far parts of L0, L1a, L2a and L1b
-    // (nodes that neither read nor write anything a coupling of this coarse
-    // step touches) run on `side` beside the chain of couplings and near
-    // parts on `stream`:
-    //   stream: L0 near -> c2f L0->L1 -> L1a near -> [L1a, L2a far done]
-    //           -> c2f L1->L2 -> L2a near -> L2b -> f2c L2->L1 -> L1b near
-    //           -> [L1b far done] -> f2c L1->L0 -> [L0 far done] -> step + 1
-    //   side:   L2a far, L1a far | after L1a near: L1b far | L0 far
-    // Every node runs the same code as in the one-stream order, so the
-    // state is the same bit for bit.
-    void launch_coarse_split() {
-        const LvlPair<StC> l0 = pair(L0, L0);
-        L0.cur ^= 1;
-        const LvlPair<StC> c1c = pair_cur(L0, L0);
-        const LvlPair<StF> c1f = pair_cur(L1[0], L1[1]);
-        const LvlPair<StF> l1a = pair(L1[0], L1[1]);
-        L1[0].cur ^= 1;
-        L1[1].cur ^= 1;
-        LvlPair<StF> c2c{}, c2f{}, l2a{}, l2b{}, f2f{}, f2c{};
-        if (levels == 3) {
-            c2c = pair_cur(L1[0], L1[1]);
-            c2f = pair_cur(L2[0], L2[1]);
-            l2a = pair(L2[0], L2[1]);
-            L2[0].cur ^= 1;
-            L2[1].cur ^= 1;
-            l2b = pair(L2[0], L2[1]);
-            L2[0].cur ^= 1;
-            L2[1].cur ^= 1;
-            f2f = pair_cur(L2[0], L2[1]);
-            f2c = pair_cur(L1[0], L1[1]);
-        }
-        const LvlPair<StF> l1b = pair(L1[0], L1[1]);
-        L1[0].cur ^= 1;
-        L1[1].cur ^= 1;
-        const LvlPair<StF> f1f = pair_cur(L1[0], L1[1]);
-        const LvlPair<StC> f1c = pair_cur(L0, L0);
-
-        CK(cudaEventRecord(sev[0], stream));
-        CK(cudaStreamWaitEvent(side, sev[0], 0));
-        if (levels == 3) step_part<StF, false>(side, l2a, 2, far2a, 0, 2, 5);
-        step_part<StF, false>(side, l1a, 2, far1a, 0, 1, 3);
-        CK(cudaEventRecord(sev[1], side));
-
-        step_part<StC, true>(stream, l0, 1, as_mode(far0, 2), 1, 0, 1);
-        launch(k_oct_c2f<StC, StF>, grid_of(OCT_CPL * n_ghost, 2), c1c, c1f, (const GhostE<A>*)gh1, n_ghost, xa,
-               xi_a_dev(), (const long long*)step_dev, seed32, 2);
-        step_part<StF, false>(stream, l1a, 2, as_mode(far1a, 2), 0, 1, 3);
-        CK(cudaEventRecord(sev[2], stream));
-
-        CK(cudaStreamWaitEvent(side, sev[2], 0));
-        step_part<StF, false>(side, l1b, 2, far1b, 1, 1, 9);
-        CK(cudaEventRecord(sev[3], side));
-        step_part<StC, true>(side, l0, 1, far0, 1, 0, 1);
-        CK(cudaEventRecord(sev[4], side));
-
-        CK(cudaStreamWaitEvent(stream, sev[1], 0));
-        if (levels == 3) {
-            launch(k_oct_c2f<StF, StF>, grid_of(OCT_CPL * n_ghost2, 2), c2c, c2f, (const GhostE<A>*)gh2, n_ghost2,
-                   xb, xi_b_dev(), (const long long*)step_dev, seed32, 4);
-            step_part<StF, false>(stream, l2a, 2, as_mode(far2a, 2), 0, 2, 5);
-            step_part<StF, false>(stream, l2b, 2, all_nodes(), 1, 2, 6);
-            launch(k_oct_f2c<StF, StF>, grid_of(OCT_CPL * std::max(n_co2_0, n_co2_1), 2), f2f, f2c,
-                   (const CoinE*)co2, n_co2_0, n_co2_1, xb, xi_b_dev(), (const OctScal<A>*)tab, S,
-                   (const long long*)step_dev, 0, 1, seed32, 7, 1);
-        }
-        step_part<StF, false>(stream, l1b, 2, as_mode(far1b, 2), 1, 1, 9);
-        CK(cudaStreamWaitEvent(stream, sev[3], 0));
-        launch(k_oct_f2c<StF, StC>, grid_of(OCT_CPL * std::max(n_co0, n_co1), 2), f1f, f1c, (const CoinE*)co1, n_co0,
-               n_co1, xa, xi_a_dev(), (const OctScal<A>*)tab, S, (const long long*)step_dev, 1, 0, seed32, 13, 1);
-        CK(cudaStreamWaitEvent(stream, sev[4], 0));
-        k_add_step<<<1, 1, 0, stream>>>(step_dev, 1);
-        check_launch();
-    }
-
-    // The far parts of the two-stream step, from the coupling tables (host
-    // copies): L0 columns strictly between the columns the couplings read
-    // (c2f stencils) or write (coincident nodes) of the two blocks; L1a / L2a
-    // interior nodes that pull from no interface ghost; L1b those nodes
-    // minus the columns of L2's couplings and one column beside the
-    // coincident nodes (their post-collision populations are pulled).  Both
-    // blocks get parts of one width.  False when a part would be empty.
-    bool plan_split(const HostGrid* g1, const HostGrid* g2) {
-        auto cols = [](const HostGrid& g, int nxc, int& lo, int& hi, int& clo, int& chi) {
-            lo = 1 << 30;
-            hi = -1;
-            clo = 1 << 30;
-            chi = -1;
-            for (const auto& e : g.ghosts)
-                for (int s = 0; s < 4; ++s) {
-                    lo = std::min(lo, e.kc[s] % nxc);
-                    hi = std::max(hi, e.kc[s] % nxc);
-                }
-            for (const auto& c : g.coin) {
-                clo = std::min(clo, c.kc % nxc);
-                chi = std::max(chi, c.kc % nxc);
-            }
-        };
-        int lo0, hi0, clo0, chi0, lo1, hi1, clo1, chi1;
-        cols(g1[0], nx0, lo0, hi0, clo0, chi0);
-        cols(g1[1], nx0, lo1, hi1, clo1, chi1);
-        far0 = NodeSet{};
-        far0.mode = 1;
-        far0.y0 = 0;
-        far0.y1 = ny0 - 1;
-        far0.x0[0] = far0.x0[1] = std::max(hi0, chi0) + 1;
-        far0.x1[0] = far0.x1[1] = std::min(lo1, clo1) - 1;
-        if (far0.x1[0] < far0.x0[0]) return false;
-        // L1a / L2a: the hot block's interface ghost column is nx - 1, the
-        // cold block's 0; their neighbours nx - 2 and 1 pull from them
-        auto interior = [](int nx, int ny) {
-            NodeSet n{};
-            n.mode = 1;
-            n.y0 = 1;
-            n.y1 = ny - 2;
-            n.x0[0] = 1;
-            n.x1[0] = nx - 3;
-            n.x0[1] = 2;
-            n.x1[1] = nx - 2;
-            return n;
-        };
-        far1a = interior(nx1, ny1);
-        if (far1a.x1[0] < far1a.x0[0] || far1a.y1 < far1a.y0) return false;
-        far1b = far1a;
-        if (levels == 3) {
-            far2a = interior(nx2, ny2);
-            if (far2a.x1[0] < far2a.x0[0] || far2a.y1 < far2a.y0) return false;
-            int lo2h, hi2h, clo2h, chi2h, lo2c, hi2c, clo2c, chi2c;
-            cols(g2[0], nx1, lo2h, hi2h, clo2h, chi2h);
-            cols(g2[1], nx1, lo2c, hi2c, clo2c, chi2c);
-            far1b.x0[0] = std::max(far1b.x0[0], std::max(hi2h + 1, chi2h + 2));
-            far1b.x1[1] = std::min(far1b.x1[1], std::min(lo2c - 1, clo2c - 2));
-            const int w = std::min(far1b.x1[0] - far1b.x0[0], far1b.x1[1] - far1b.x0[1]);
-            if (w < 0) return false;
-            far1b.x1[0] = far1b.x0[0] + w;  // the hot part keeps its low columns, the cold part its high ones
-            far1b.x0[1] = far1b.x1[1] - w;
-        }
-        return true;
     }
 
     // ---- dynamic mixed-scale SGS model ------------------------------------
@@ -2414,116 +1927,9 @@ struct OctImpl final : Octree {
         }
     }
 
-    // One step_cavity as one cooperative launch of k_oct_coarse: the buffer
-    // views of the per-phase launches below, in their order and parities.
-    void launch_coarse_fused() {
-        CoarseArgs<StC, StF> a{};
-        a.l0 = pair(L0, L0);
-        L0.cur ^= 1;
-        a.c1c = pair_cur(L0, L0);
-        a.c1f = pair_cur(L1[0], L1[1]);
-        a.l1a = pair(L1[0], L1[1]);
-        L1[0].cur ^= 1;
-        L1[1].cur ^= 1;
-        if (levels == 3) {
-            a.c2c = pair_cur(L1[0], L1[1]);
-            a.c2f = pair_cur(L2[0], L2[1]);
-            a.l2a = pair(L2[0], L2[1]);
-            L2[0].cur ^= 1;
-            L2[1].cur ^= 1;
-            a.l2b = pair(L2[0], L2[1]);
-            L2[0].cur ^= 1;
-            L2[1].cur ^= 1;
-            a.f2f = pair_cur(L2[0], L2[1]);
-            a.f2c = pair_cur(L1[0], L1[1]);
-        }
-        a.l1b = pair(L1[0], L1[1]);
-        L1[0].cur ^= 1;
-        L1[1].cur ^= 1;
-        a.f1f = pair_cur(L1[0], L1[1]);
-        a.f1c = pair_cur(L0, L0);
-        a.tab = tab;
-        a.gh1 = gh1;
-        a.gh2 = gh2;
-        a.co1 = co1;
-        a.co2 = co2;
-        a.xia_dev = xi_a_dev();
-        a.xib_dev = xi_b_dev();
-        a.xa = xa;
-        a.xb = xb;
-        a.step_dev = step_dev;
-        a.bar = ocf_flags;
-        a.err = ocf_flags + 1;
-        a.S = S;
-        a.levels = levels;
-        a.n_ghost = n_ghost;
-        a.n_ghost2 = n_ghost2;
-        a.n_co0 = n_co0;
-        a.n_co1 = n_co1;
-        a.n_co2_0 = n_co2_0;
-        a.n_co2_1 = n_co2_1;
-        a.inv_nx0 = 1.0f / float(L0.nx);
-        a.inv_nx1 = 1.0f / float(L1[0].nx);
-        a.inv_nx2 = levels == 3 ? 1.0f / float(L2[0].nx) : 0.0f;
-        a.seed = seed32;
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(ocf_grid);
-        cfg.blockDim = dim3(OcfShape<A>::THREADS);
-        cfg.dynamicSmemBytes = 0;
-        cfg.stream = stream;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeCooperative;
-        attr[0].val.cooperative = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        CK(cudaLaunchKernelEx(&cfg, k_oct_coarse<StC, StF>, a));
-        check_launch();
-    }
-
-    // A barrier wait of k_oct_coarse that gave up: reported once (the steps
-    // of that launch and of the launches after it are lost), then the flag
-    // and the barrier word are cleared.
-    void check_ocf() {
-        if (!ocf_flags) return;
-        unsigned h[2] = {0, 0};
-        CK(cudaMemcpyAsync(h, ocf_flags, sizeof(h), cudaMemcpyDeviceToHost, stream));
-        CK(cudaStreamSynchronize(stream));
-        if (h[1]) {
-            CK(cudaMemsetAsync(ocf_flags, 0, 2 * sizeof(unsigned), stream));
-            CK(cudaStreamSynchronize(stream));
-            throw ArgError{CAV_ERR_TIMEOUT, "a grid barrier of the one-launch coarse step did not complete"};
-        }
-    }
-
-    void set_step_mode(int mode) override {
-        if (mode != CAV_OCT_STEP_PER_PHASE && mode != CAV_OCT_STEP_ONE_LAUNCH && mode != CAV_OCT_STEP_TWO_STREAMS)
-            throw ArgError{CAV_ERR_ARG, "unknown octree step mode"};
-        if (mode == CAV_OCT_STEP_ONE_LAUNCH && ocf_grid <= 0)
-            throw ArgError{CAV_ERR_ARG, "this device cannot run the one-launch coarse step (no cooperative launch)"};
-        if (mode == CAV_OCT_STEP_TWO_STREAMS && !split)
-            throw ArgError{CAV_ERR_ARG, "this octree has no far parts for the two-stream coarse step"};
-        if (mode == step_mode) return;
-        CK(cudaStreamSynchronize(stream));
-        for (auto& gx : graph)
-            if (gx) {
-                CK(cudaGraphExecDestroy(gx));
-                gx = nullptr;
-            }
-        step_mode = mode;
-    }
-    int get_step_mode() const override { return step_mode; }
-
     // One step_cavity (src/octree/solver.rs:647-947), all launches on `stream`,
     // with the step index taken from *step_dev (advanced at the end).
     void launch_coarse_step() {
-        if (step_mode == CAV_OCT_STEP_ONE_LAUNCH) {
-            launch_coarse_fused();
-            return;
-        }
-        if (step_mode == CAV_OCT_STEP_TWO_STREAMS) {
-            launch_coarse_split();
-            return;
-        }
         step_L0();
         c2f_L1();
         step_L1(0, 3);
@@ -2557,11 +1963,7 @@ struct OctImpl final : Octree {
         return gx;
     }
 
-    int per_step_launches() const {
-        if (step_mode == CAV_OCT_STEP_ONE_LAUNCH) return 1;
-        if (step_mode == CAV_OCT_STEP_TWO_STREAMS) return levels == 3 ? 14 : 9;
-        return levels == 3 ? 10 : 6;
-    }
+    int per_step_launches() const { return levels == 3 ? 10 : 6; }
 
     // OCT_GRAPH_STEPS dynamic coarse steps in one graph: valid once the
     // viscosity ramp has converged (the model's constants no longer change).
@@ -2628,7 +2030,6 @@ struct OctImpl final : Octree {
 
     void get_level(int lvl, double* r, double* u, double* v, double* t, double* f, double* g) override {
         CK(cudaStreamSynchronize(stream));
-        check_ocf();
         if (lvl == 0) return download_state(L0, r, u, v, t, f, g);
         if (lvl == 1 || lvl == 2) return download_state(L1[lvl - 1], r, u, v, t, f, g);
         if (levels == 3 && (lvl == 3 || lvl == 4)) return download_state(L2[lvl - 3], r, u, v, t, f, g);
@@ -2735,13 +2136,9 @@ struct OctImpl final : Octree {
         check_launch();
         CK(cudaMemcpyAsync(out, dout, sizeof(double) * 10, cudaMemcpyDeviceToHost, stream));
         CK(cudaStreamSynchronize(stream));
-        check_ocf();
     }
 
-    void sync() override {
-        CK(cudaStreamSynchronize(stream));
-        check_ocf();
-    }
+    void sync() override { CK(cudaStreamSynchronize(stream)); }
 };
 
 }  // namespace oct

@@ -302,21 +302,6 @@ int cav_octree_launch_count(cav_octree* h, int64_t* n) {
     });
 }
 
-int cav_octree_set_step_mode(cav_octree* h, int32_t mode) {
-    return oguarded(h, [&](Octree& o) {
-        o.set_step_mode(mode);
-        return CAV_OK;
-    });
-}
-
-int cav_octree_get_step_mode(cav_octree* h, int32_t* mode) {
-    if (!mode) return ofail(h, CAV_ERR_ARG, "null output");
-    return oguarded(h, [&](Octree& o) {
-        *mode = o.get_step_mode();
-        return CAV_OK;
-    });
-}
-
 int cav_octree_set_dynamic_sgs(cav_octree* h, int32_t on, double smag_alpha, double nu_sm_min, double eta_test) {
     return oguarded(h, [&](Octree& o) {
         o.set_dynamic_sgs(on != 0, smag_alpha, nu_sm_min, eta_test);

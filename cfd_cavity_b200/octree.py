@@ -178,20 +178,6 @@ class OctreeSolver:
         self._ck(L.load().cav_octree_launch_count(self._h, ctypes.byref(n)))
         return n.value
 
-    def set_step_mode(self, mode):
-        """How a coarse step is launched: ``CAV_OCT_STEP_PER_PHASE`` (the
-        default: one launch per level step and coupling, one stream),
-        ``CAV_OCT_STEP_ONE_LAUNCH`` (one cooperative launch with grid
-        barriers) or ``CAV_OCT_STEP_TWO_STREAMS`` (the nodes of the level
-        steps that no coupling of the step touches on a second stream beside
-        the chain of couplings); the results are the same bit for bit."""
-        self._ck(L.load().cav_octree_set_step_mode(self._h, int(mode)))
-
-    def step_mode(self):
-        m = ctypes.c_int32()
-        self._ck(L.load().cav_octree_get_step_mode(self._h, ctypes.byref(m)))
-        return m.value
-
     def set_dynamic_sgs(self, on, smag_alpha=0.5, nu_sm_min=-0.1, eta_test=2.0):
         """``set_dynamic_sgs`` (src/octree/solver.rs:476-481): the dynamic
         mixed-scale model on every level (src/octree/smag.rs)."""

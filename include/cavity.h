@@ -421,27 +421,6 @@ int cav_octree_check_guards(cav_octree* h, double max_u_abort);
 int cav_octree_sync(cav_octree* h);
 int cav_octree_get_stream(cav_octree* h, void** stream);
 int cav_octree_launch_count(cav_octree* h, int64_t* n);
-/* How a coarse step is launched (same results bit for bit):
- *   CAV_OCT_STEP_PER_PHASE   the default: one launch per level step and per
- *                            coupling, in the reference's order on one
- *                            stream (10 with levels = 3, 6 with levels = 2);
- *   CAV_OCT_STEP_ONE_LAUNCH  one cooperative launch per coarse step, the
- *                            phases separated by bounded grid barriers (where
- *                            the device supports cooperative launches; a
- *                            barrier that gave up is reported as
- *                            CAV_ERR_TIMEOUT by the next cav_octree_sync,
- *                            cav_octree_diag or cav_octree_get_level, the
- *                            steps since then being lost);
- *   CAV_OCT_STEP_TWO_STREAMS the level steps split into the nodes next to
- *                            a coupling, on the chain of couplings, and the
- *                            rest, on a second stream beside that chain (14
- *                            launches with levels = 3, 9 with levels = 2).
- * The dynamic SGS model always runs per phase. */
-#define CAV_OCT_STEP_PER_PHASE 0
-#define CAV_OCT_STEP_ONE_LAUNCH 1
-#define CAV_OCT_STEP_TWO_STREAMS 2
-int cav_octree_set_step_mode(cav_octree* h, int32_t mode);
-int cav_octree_get_step_mode(cav_octree* h, int32_t* mode);
 /* set_dynamic_sgs (src/octree/solver.rs:476-481): on = 1 runs the dynamic
  * mixed-scale model on every level before each of its collisions
  * (compute_dynamic_sgs_level, src/octree/smag.rs:144-416) and rescales the

@@ -234,67 +234,6 @@ def test_fine_to_coarse_conserves_moments():
     assert worst < 1e-12, worst
 
 
-def assert_same_state(a, b, levels):
-    for lvl in range(n_levels(levels)):
-        ga, gb = a.level(lvl, pops=True), b.level(lvl, pops=True)
-        for k in ("rho", "ux", "uy", "temp", "f", "g"):
-            np.testing.assert_array_equal(ga[k], gb[k], err_msg=f"level {lvl} {k}")
-
-
-@pytest.mark.parametrize("prec", ["f64", "f32", "f32_f16", "f32_f16g"])
-@pytest.mark.parametrize("levels", [2, 3])
-def test_step_modes_bit_identical(prec, levels):
-    """The three launch forms of a coarse step give the same state bit for
-    bit: the two-stream step (the default: far parts of the level steps on a
-    second stream), the one-launch step (k_oct_coarse: one cooperative
-    launch, the phases separated by grid barriers) and the per-phase
-    launches on one stream -- every level's populations and moments after 37
-    coarse steps (two graph replays of 16 and single steps) across the
-    viscosity ramp, with switches of form half way; launch counts per step."""
-    args = (48, 96, 6, 1.0e7, 0.71, 0.03, 7)
-    a = OctreeSolver(*args, levels=levels, precision=prec, nu_start_mult=2.5)
-    b = OctreeSolver(*args, levels=levels, precision=prec, nu_start_mult=2.5)
-    c = OctreeSolver(*args, levels=levels, precision=prec, nu_start_mult=2.5)
-    assert b.step_mode() == L.CAV_OCT_STEP_PER_PHASE
-    a.set_step_mode(L.CAV_OCT_STEP_TWO_STREAMS)
-    assert a.step_mode() == L.CAV_OCT_STEP_TWO_STREAMS
-    c.set_step_mode(L.CAV_OCT_STEP_ONE_LAUNCH)
-    for s in (a, b, c):
-        s.step_cavity(1)
-    per_step = {a: 14 if levels == 3 else 9, b: 10 if levels == 3 else 6, c: 1}
-    for s in (a, b, c):
-        n0 = s.launch_count()
-        s.step_cavity(20)
-        assert s.launch_count() - n0 == 20 * per_step[s]
-    b.set_step_mode(L.CAV_OCT_STEP_TWO_STREAMS)
-    c.set_step_mode(L.CAV_OCT_STEP_PER_PHASE)
-    a.set_step_mode(L.CAV_OCT_STEP_ONE_LAUNCH)
-    for s in (a, b, c):
-        s.step_cavity(17)
-    assert_same_state(a, b, levels)
-    assert_same_state(a, c, levels)
-    assert a.diag() == b.diag() == c.diag()
-    with pytest.raises(L.CavError) as e:
-        a.set_step_mode(7)
-    assert e.value.code == L.CAV_ERR_ARG
-
-
-def test_step_modes_bit_identical_large():
-    """The same identity on the 256 x 1024 base, bl_width 16, 3 levels,
-    binary16 fine levels, fixed-Cs extension (the benchmark's shape: the
-    side stream's far parts overlap the couplings, every group of the
-    cooperative grid takes several work units per phase), 40 coarse steps."""
-    args = (256, 1024, 16, 1.0e10, 0.71, 0.1, 42)
-    runs = []
-    for mode in (L.CAV_OCT_STEP_TWO_STREAMS, L.CAV_OCT_STEP_PER_PHASE, L.CAV_OCT_STEP_ONE_LAUNCH):
-        s = OctreeSolver(*args, levels=3, precision="f32_f16", nu_start_mult=4.0, cs=0.12)
-        s.set_step_mode(mode)
-        s.step_cavity(40)
-        runs.append(s)
-    assert_same_state(runs[0], runs[1], 3)
-    assert_same_state(runs[0], runs[2], 3)
-
-
 @pytest.mark.parametrize("prec,tol_t,tol_nu", [("f32", 1e-4, 5e-4), ("f32_f16", 3e-3, 2e-3),
                                                 ("f32_f16g", 5e-4, 1e-3)])
 def test_reduced_precision_against_fp64(prec, tol_t, tol_nu):
