@@ -28,6 +28,7 @@ PRECISIONS = {"f64": CAV_PREC_F64, "f32": CAV_PREC_F32, "f16": CAV_PREC_F16, "bf
               "f16gsr": CAV_PREC_F16GSR}
 CAV_INIT_LINEAR, CAV_INIT_ZERO = 0, 1
 CAV_STEP_NODE, CAV_STEP_PAIR, CAV_STEP_PAIR_SPLIT = 0, 1, 2
+CAV_OCT_LEVEL_NODE, CAV_OCT_LEVEL_FG = 0, 1
 (CAV_PHASE_COLLIDE, CAV_PHASE_STREAM, CAV_PHASE_BOUNCE_BACK, CAV_PHASE_THERMAL_BC,
  CAV_PHASE_MACRO, CAV_PHASE_NOSLIP, CAV_PHASE_FUSED_IDENTITY, CAV_PHASE_CHANNEL) = range(8)
 
@@ -205,6 +206,8 @@ def load(path: str | None = None):
         "cav_octree_sync": (i32, [vp]),
         "cav_octree_get_stream": (i32, [vp, ctypes.POINTER(vp)]),
         "cav_octree_launch_count": (i32, [vp, ctypes.POINTER(i64)]),
+        "cav_octree_set_level_kernel": (i32, [vp, i32]),
+        "cav_octree_get_level_kernel": (i32, [vp, ctypes.POINTER(i32)]),
         "cav_octree_set_dynamic_sgs": (i32, [vp, i32, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
         "cav_octree_dynamic_stats": (i32, [vp, _dp]),
         "cav_octree_get_nu_t": (i32, [vp, i32, _dp, _dp]),

@@ -116,6 +116,63 @@ __device__ __forceinline__ const OctScal<A>& row_of(const OctScal<A>* tab, int S
 // Collision of one node (collide_node_cavity, src/octree/cavity.rs:70-150,
 // nu_t = 0): TRT + Guo forcing for f, BGK for g.
 // ---------------------------------------------------------------------------
+// The shifted formats' collision in two halves (pairwise (i, opp(i)) TRT on
+// h_i = f_i - w_i, as in the uniform FP32 collision, with the level's fixed
+// relaxation rates; BGK for g): the f half needs T for the Guo force, the g
+// half u, v; u^2 is formed once (oct_u2) and handed to both.  Every operation
+// is an explicitly rounded intrinsic (no contraction left to the compiler),
+// so the two halves give the same bits whether one thread runs them or two.
+__device__ __forceinline__ float oct_u2(float u, float v) { return __fmaf_rn(u, u, __fmul_rn(v, v)); }
+// c_p . u for p = 1..4 (c_x, c_y in {-1, 0, 1}: the products are exact)
+__device__ __forceinline__ float oct_eu(int p, float u, float v) {
+    return __fadd_rn(__fmul_rn(float(CX(p)), u), __fmul_rn(float(CY(p)), v));
+}
+// 4.5 (c_p . u)^2 - 1.5 u^2
+__device__ __forceinline__ float oct_q(float eu, float u2) {
+    return __fmaf_rn(__fmul_rn(4.5f, eu), eu, __fmul_rn(-1.5f, u2));
+}
+__device__ __forceinline__ void oct_collide_f_sh(float (&f)[Q], float r, float drho, float u, float v, float u2,
+                                                 float temp, const LvlScal<float>& c, float& fy_out) {
+    const float fyv = __fmul_rn(__fmul_rn(r, c.beta), temp);
+    fy_out = fyv;
+    const float hp = __fmul_rn(-0.5f, c.om_p), hm = __fmul_rn(-0.5f, c.om_m);
+    const float m3v = __fmul_rn(-3.0f, v);
+    const float feq0 = __fmul_rn(float(WD(0)), __fmaf_rn(-__fmul_rn(1.5f, r), u2, drho));
+    const float d0 = __fsub_rn(f[0], feq0);
+    const float s0 = __fmul_rn(__fmul_rn(__fmul_rn(c.k_p, float(WD(0))), m3v), fyv);
+    f[0] = __fmaf_rn(-c.om_p, d0, __fadd_rn(f[0], s0));
+    const float r3 = __fmul_rn(r, 3.0f);
+#pragma unroll
+    for (int p = 1; p <= 4; ++p) {
+        const float w = float(WD(p)), cy = float(CY(p));
+        const float eu = oct_eu(p, u, v);
+        const float feS = __fmul_rn(w, __fmaf_rn(r, oct_q(eu, u2), drho));
+        const float feA = __fmul_rn(w, __fmul_rn(r3, eu));
+        const float dS = __fmaf_rn(-2.0f, feS, __fadd_rn(f[p], f[p + 4]));
+        const float dD = __fmaf_rn(-2.0f, feA, __fsub_rn(f[p], f[p + 4]));
+        const float sE = __fmaf_rn(__fmul_rn(9.0f, cy), eu, m3v);
+        const float E = __fmaf_rn(hp, dS, __fmul_rn(__fmul_rn(__fmul_rn(c.k_p, w), sE), fyv));
+        const float O = __fmaf_rn(hm, dD, __fmul_rn(__fmul_rn(__fmul_rn(c.k_m, w), __fmul_rn(3.0f, cy)), fyv));
+        f[p] = __fadd_rn(f[p], __fadd_rn(E, O));
+        f[p + 4] = __fadd_rn(f[p + 4], __fsub_rn(E, O));
+    }
+}
+__device__ __forceinline__ void oct_collide_g_sh(float (&g)[Q], float u, float v, float u2, float temp,
+                                                 const LvlScal<float>& c) {
+    const float om_g = c.om_g, one_m = __fsub_rn(1.0f, om_g);
+    const float a0 = __fmul_rn(__fmul_rn(om_g, float(WD(0))), temp);
+    g[0] = __fmaf_rn(one_m, g[0], __fmul_rn(a0, __fmaf_rn(-1.5f, u2, 1.0f)));
+#pragma unroll
+    for (int p = 1; p <= 4; ++p) {
+        const float eu = oct_eu(p, u, v);
+        const float ogw = __fmul_rn(__fmul_rn(om_g, float(WD(p))), temp);
+        const float gS = __fmul_rn(ogw, __fadd_rn(1.0f, oct_q(eu, u2)));
+        const float gA = __fmul_rn(ogw, __fmul_rn(3.0f, eu));
+        g[p] = __fmaf_rn(one_m, g[p], __fadd_rn(gS, gA));
+        g[p + 4] = __fmaf_rn(one_m, g[p + 4], __fsub_rn(gS, gA));
+    }
+}
+
 template <class A, bool SHIFT>
 __device__ __forceinline__ void oct_collide(A (&f)[Q], A (&g)[Q], const Macro<A, SHIFT>& m, const LvlScal<A>& c0,
                                             A& fy_out, const A* nut = nullptr, const A* at = nullptr) {
@@ -181,40 +238,9 @@ __device__ __forceinline__ void oct_collide(A (&f)[Q], A (&g)[Q], const Macro<A,
 #pragma unroll
         for (int i = 0; i < Q; ++i) g[i] = g[i] + (-c.a_g * d_g[i] - 0.0 * d_g[OPP(i)]);
     } else {
-        // Pairwise (i, opp(i)) TRT on h_i = f_i - w_i, as in the uniform FP32
-        // collision, with the level's fixed relaxation rates.
-        const float r = m.rho, u = m.ux, v = m.uy, temp = m.t;
-        const float fyv = r * c.beta * temp;
-        fy_out = fyv;
-        const float u2 = u * u + v * v;
-        const float om_p = c.om_p, om_m = c.om_m, k_p = c.k_p, k_m = c.k_m;
-        const float feq0 = float(WD(0)) * (m.drho - 1.5f * r * u2);
-        const float d0 = f[0] - feq0;
-        f[0] = f[0] - om_p * d0 + k_p * float(WD(0)) * (-3.0f * v) * fyv;
-#pragma unroll
-        for (int p = 1; p <= 4; ++p) {
-            const float cx = CX(p), cy = CY(p);
-            const float eu = cx * u + cy * v;
-            const float feS = float(WD(p)) * (m.drho + r * (4.5f * eu * eu - 1.5f * u2));
-            const float feA = float(WD(p)) * (r * 3.0f * eu);
-            const float dS = (f[p] + f[p + 4]) - 2.0f * feS;
-            const float dD = (f[p] - f[p + 4]) - 2.0f * feA;
-            const float E = -0.5f * om_p * dS + k_p * float(WD(p)) * (-3.0f * v + 9.0f * eu * cy) * fyv;
-            const float O = -0.5f * om_m * dD + k_m * float(WD(p)) * (3.0f * cy) * fyv;
-            f[p] = f[p] + (E + O);
-            f[p + 4] = f[p + 4] + (E - O);
-        }
-        const float om_g = c.om_g, one_m = 1.0f - om_g;
-        g[0] = one_m * g[0] + om_g * float(WD(0)) * temp * (1.0f - 1.5f * u2);
-#pragma unroll
-        for (int p = 1; p <= 4; ++p) {
-            const float cx = CX(p), cy = CY(p);
-            const float eu = cx * u + cy * v;
-            const float gS = om_g * float(WD(p)) * temp * (1.0f + (4.5f * eu * eu - 1.5f * u2));
-            const float gA = om_g * float(WD(p)) * temp * (3.0f * eu);
-            g[p] = one_m * g[p] + (gS + gA);
-            g[p + 4] = one_m * g[p + 4] + (gS - gA);
-        }
+        const float u2 = oct_u2(m.ux, m.uy);
+        oct_collide_f_sh(f, m.rho, m.drho, m.ux, m.uy, u2, m.t, c, fy_out);
+        oct_collide_g_sh(g, m.ux, m.uy, u2, m.t, c);
     }
 }
 
@@ -294,6 +320,64 @@ __device__ __forceinline__ void store_pops(St* __restrict__ dst, int n, int k, t
         dst[q * n + k] = v;
         if (BACK) x = Fmt<St>::load(v, q);
     }
+}
+
+// The planes of one half of store_pops (G: the g planes Q..2Q-1 from x,
+// else the f planes 0..Q-1), each with the bits store_pops gives it: the
+// node's draws are generated in full and this half's share of each pair used.
+// A binary16 / bfloat16 pair that store_pops rounds by one cvt.rs is rounded
+// here with the other half zero (the two halves are rounded independently).
+template <class St, bool G>
+__device__ __forceinline__ void store_half(St* __restrict__ dst, int n, int k, const typename Fmt<St>::A (&x)[Q],
+                                           bool sr, uint32_t seed, long long key, long long node) {
+    constexpr int Q0 = G ? Q : 0;
+    if constexpr (Fmt<St>::HW_SR_F) {
+        if (sr) {
+            NodeRng rng(seed, key, node);
+            const float sf = p2(Fmt<St>::EF), sg = p2(Fmt<St>::EG);
+#pragma unroll
+            for (int q = 0; q < NPLANES; q += 2) {
+                const uint32_t r = rng.next();
+                const bool ha = q < Q || Fmt<St>::HW_SR_G, hb = q + 1 < Q || Fmt<St>::HW_SR_G;
+                if (q >= Q0 && q < Q0 + Q) {  // plane q (the pair's first) is this half's
+                    const float xa = x[q - Q0];
+                    St va;
+                    if (ha && hb)
+                        va.bits = (unsigned short)(Fmt<St>::enc2_sr(xa * (q < Q ? sf : sg), 0.0f, r) >> 16);
+                    else if (ha)
+                        va.bits = (unsigned short)(Fmt<St>::enc2_sr(xa * sf, 0.0f, r) >> 16);
+                    else
+                        va = Fmt<St>::store_sr(xa, q, r & 0xffff0000u);
+                    dst[q * n + k] = va;
+                }
+                if (q + 1 >= Q0 && q + 1 < Q0 + Q) {  // plane q + 1 is this half's
+                    const float xb = x[q + 1 - Q0];
+                    St vb;
+                    if (ha && hb)
+                        vb.bits = (unsigned short)(Fmt<St>::enc2_sr(0.0f, xb * (q + 1 < Q ? sf : sg), r) & 0xffffu);
+                    else
+                        vb = Fmt<St>::store_sr(xb, q + 1, r << 16);
+                    dst[(q + 1) * n + k] = vb;
+                }
+            }
+            return;
+        }
+    } else if constexpr (Fmt<St>::SR) {
+        if (sr) {
+            NodeRng rng(seed, key, node);
+            uint32_t r = 0;
+#pragma unroll
+            for (int q = 0; q < NPLANES; ++q) {
+                if ((q & 1) == 0) r = rng.next();
+                if (q < Q0 || q >= Q0 + Q) continue;
+                const uint32_t bits = (q & 1) == 0 ? (r & 0xffff0000u) : (r << 16);
+                dst[q * n + k] = Fmt<St>::store_sr(x[q - Q0], q, bits);
+            }
+            return;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < Q; ++i) dst[(Q0 + i) * n + k] = Fmt<St>::store(x[i], Q0 + i, RN_BITS);
 }
 
 template <class St>
@@ -448,6 +532,87 @@ __global__ void __launch_bounds__(OT) k_oct_step(LvlPair<St> P, const OctScal<ty
     oct_collide<A, SH>(f, g, m, sc, fy_new);
     L.fy[k] = fy_new;
     store_pops<St>(L.pc_out, L.n, k, f, g, true, seed, s * 16 + phase, (long long)L.node_off + k);
+}
+
+// One (sub-)step of a fine level (L1 / L2) with each node's f and g halves
+// on two threads, for the shifted formats without the fixed-Cs extension:
+// OCT_FG nodes per CTA; the first OCT_FG threads take the f halves (pull of
+// f, rho and u with the Guo half force and no-slip, the f REF planes and the
+// moments, the TRT update with the Guo force, the f PC planes, fy), the
+// others the g halves (pull of g at its boundary-condition source, T, the g
+// REF planes, the BGK update, the g PC planes); they exchange u, v, u^2 and
+// T through shared memory at one barrier.  Same bits as k_oct_step.
+constexpr int OCT_FG = 64;
+template <class St>
+__global__ void __launch_bounds__(2 * OCT_FG) k_oct_step_fg(LvlPair<St> P, const OctScal<float>* __restrict__ tab,
+                                                           int S, const long long* __restrict__ step_dev, int off,
+                                                           int lvl, uint32_t seed, int phase, float inv_nx) {
+    static_assert(Fmt<St>::SHIFT, "the split step runs the shifted formats");
+    pdl_wait();
+    pdl_trigger();
+    __shared__ float xu[OCT_FG], xv[OCT_FG], xq[OCT_FG], xt[OCT_FG];
+    const LvlIO<St> L = P.b[blockIdx.y];
+    const bool g_half = threadIdx.x >= OCT_FG;
+    const int j = g_half ? threadIdx.x - OCT_FG : threadIdx.x;
+    const int k = blockIdx.x * OCT_FG + j;
+    const bool act = k < L.n;
+    long long s;
+    const LvlScal<float> sc = row_of<float>(tab, S, step_dev, off, &s).l[lvl];
+    int x = 0, y = 0;
+    if (act) split_k(k, L.nx, inv_nx, x, y);
+    const bool ghost = x == 0 || x == L.nx - 1 || y == 0 || y == L.ny - 1;
+    const long long key = s * 16 + phase, node = (long long)L.node_off + k;
+    if (!g_half) {
+        float f[Q];
+        float r = 0.0f, drho = 0.0f, u = 0.0f, v = 0.0f, u2 = 0.0f;
+        if (act) {
+            const Src own = src_of<false>(L, x, y);
+            if (ghost) {
+#pragma unroll
+                for (int i = 0; i < Q; ++i) f[i] = Fmt<St>::load(L.ref_in[i * L.n + k], i);
+            } else {
+#pragma unroll
+                for (int i = 0; i < Q; ++i) f[i] = pull_one<St>(L, own, i, i);
+            }
+            const bool wall = (L.hot && x == 1) || (L.cold && x == L.nx - 2) || y == 1 || y == L.ny - 2;
+            const Macro<float, true> m = macro_f<float, true>(f, L.fy[k], wall);
+            store_half<St, false>(L.ref_out, L.n, k, f, false, 0, 0, 0);
+            L.mac[k] = m.drho;
+            L.mac[L.n + k] = m.ux;
+            L.mac[2 * L.n + k] = m.uy;
+            r = m.rho;
+            drho = m.drho;
+            u = m.ux;
+            v = m.uy;
+            u2 = oct_u2(u, v);
+        }
+        xu[j] = u;
+        xv[j] = v;
+        xq[j] = u2;
+        named_bar_sync(1, 2 * OCT_FG);
+        if (act && !ghost) {
+            float fy_new;
+            oct_collide_f_sh(f, r, drho, u, v, u2, xt[j], sc, fy_new);
+            L.fy[k] = fy_new;
+            store_half<St, false>(L.pc_out, L.n, k, f, true, seed, key, node);
+        }
+    } else {
+        float g[Q];
+        float t = 0.0f;
+        if (act) {
+            const Src own = src_of<false>(L, x, y);
+            bc_g<St, false>(L, x, y, own, g);
+            t = sum_g<float>(g);
+            store_half<St, true>(L.ref_out, L.n, k, g, false, 0, 0, 0);
+            L.mac[3 * L.n + k] = t;
+        }
+        xt[j] = t;
+        named_bar_sync(1, 2 * OCT_FG);
+        if (act && !ghost) {
+            oct_collide_g_sh(g, xu[j], xv[j], xq[j], t, sc);
+            store_half<St, true>(L.pc_out, L.n, k, g, true, seed, key, node);
+        }
+    }
 }
 
 // Collision of the REF state into PC: the first collision after the state
@@ -1089,6 +1254,8 @@ struct Octree {
     virtual void set_dynamic_sgs(bool on, double smag_alpha, double nu_sm_min, double eta_test) = 0;
     virtual void dynamic_stats(double* out14) = 0;
     virtual void get_nut(int lvl, double* nut, double* at) = 0;
+    virtual void set_level_kernel(int kind) = 0;
+    virtual int get_level_kernel() const = 0;
 
     cav_octree_params p{};
     int levels = 2, nx0 = 0, ny0 = 0, nx1 = 0, ny1 = 0, nx2 = 0, ny2 = 0;
@@ -1216,6 +1383,7 @@ struct OctImpl final : Octree {
     bool pc_valid = false;
     Xi<A> xa{}, xb{};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int level_kernel = CAV_OCT_LEVEL_FG;  // fine-level step form (step_fine)
     // dynamic mixed-scale SGS model (set_dynamic_sgs, src/octree/solver.rs:476-481)
     bool dyn = false;
     double dyn_alpha = 0.5, dyn_min = -0.1, dyn_eta = 2.0;
@@ -1679,20 +1847,43 @@ struct OctImpl final : Octree {
                0, seed32, 1, 1.0f / float(L0.nx), int(!dyn));
         L0.cur ^= 1;
     }
-    void step_L1(int off, int phase) {
-        LvlPair<StF> q = pair(L1[0], L1[1]);
-        launch(k_oct_step<StF, false>, grid_of(L1[0].n, 2), q, (const OctScal<A>*)tab, S,
-               (const long long*)step_dev, off, 1, seed32, phase, 1.0f / float(L1[0].nx), int(!dyn));
-        L1[0].cur ^= 1;
-        L1[1].cur ^= 1;
+    // A fine level's (sub-)step: the f and g halves of a node on two threads
+    // where that form exists (shifted formats, no fixed-Cs extension, not the
+    // dynamic model's step, which collides separately), else one thread.
+    bool split_fg() const { return level_kernel == CAV_OCT_LEVEL_FG && Fmt<StF>::SHIFT && !dyn && p.cs == 0.0; }
+    void step_fine(Lvl<StF>* Lv, int lvl, int off, int phase) {
+        LvlPair<StF> q = pair(Lv[0], Lv[1]);
+        if constexpr (Fmt<StF>::SHIFT) {
+            if (split_fg()) {
+                launch(k_oct_step_fg<StF>, dim3((Lv[0].n + OCT_FG - 1) / OCT_FG, 2), q, (const OctScal<float>*)tab, S,
+                       (const long long*)step_dev, off, lvl, seed32, phase, 1.0f / float(Lv[0].nx));
+                Lv[0].cur ^= 1;
+                Lv[1].cur ^= 1;
+                return;
+            }
+        }
+        launch(k_oct_step<StF, false>, grid_of(Lv[0].n, 2), q, (const OctScal<A>*)tab, S, (const long long*)step_dev,
+               off, lvl, seed32, phase, 1.0f / float(Lv[0].nx), int(!dyn));
+        Lv[0].cur ^= 1;
+        Lv[1].cur ^= 1;
     }
-    void step_L2(int off, int phase) {
-        LvlPair<StF> q = pair(L2[0], L2[1]);
-        launch(k_oct_step<StF, false>, grid_of(L2[0].n, 2), q, (const OctScal<A>*)tab, S,
-               (const long long*)step_dev, off, 2, seed32, phase, 1.0f / float(L2[0].nx), int(!dyn));
-        L2[0].cur ^= 1;
-        L2[1].cur ^= 1;
+    void step_L1(int off, int phase) { step_fine(L1, 1, off, phase); }
+    void step_L2(int off, int phase) { step_fine(L2, 2, off, phase); }
+
+    void set_level_kernel(int kind) override {
+        if (kind != CAV_OCT_LEVEL_NODE && kind != CAV_OCT_LEVEL_FG)
+            throw ArgError{CAV_ERR_ARG, "unknown octree level kernel"};
+        if (kind == level_kernel) return;
+        CK(cudaStreamSynchronize(stream));
+        for (auto* gs : {graph, dgraph})
+            for (int i = 0; i < 2; ++i)
+                if (gs[i]) {
+                    CK(cudaGraphExecDestroy(gs[i]));
+                    gs[i] = nullptr;
+                }
+        level_kernel = kind;
     }
+    int get_level_kernel() const override { return level_kernel; }
 
     // ---- dynamic mixed-scale SGS model ------------------------------------
     void set_dynamic_sgs(bool on, double smag_alpha, double nu_sm_min, double eta_test) override {

@@ -302,6 +302,21 @@ int cav_octree_launch_count(cav_octree* h, int64_t* n) {
     });
 }
 
+int cav_octree_set_level_kernel(cav_octree* h, int32_t kind) {
+    return oguarded(h, [&](Octree& o) {
+        o.set_level_kernel(kind);
+        return CAV_OK;
+    });
+}
+
+int cav_octree_get_level_kernel(cav_octree* h, int32_t* kind) {
+    if (!kind) return ofail(h, CAV_ERR_ARG, "null output");
+    return oguarded(h, [&](Octree& o) {
+        *kind = o.get_level_kernel();
+        return CAV_OK;
+    });
+}
+
 int cav_octree_set_dynamic_sgs(cav_octree* h, int32_t on, double smag_alpha, double nu_sm_min, double eta_test) {
     return oguarded(h, [&](Octree& o) {
         o.set_dynamic_sgs(on != 0, smag_alpha, nu_sm_min, eta_test);

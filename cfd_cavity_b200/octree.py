@@ -178,6 +178,17 @@ class OctreeSolver:
         self._ck(L.load().cav_octree_launch_count(self._h, ctypes.byref(n)))
         return n.value
 
+    def set_level_kernel(self, kind):
+        """The fine levels' step kernel: ``CAV_OCT_LEVEL_NODE`` (one thread
+        per node) or ``CAV_OCT_LEVEL_FG`` (a node's f and g halves on two
+        threads, the default where it applies); same results bit for bit."""
+        self._ck(L.load().cav_octree_set_level_kernel(self._h, int(kind)))
+
+    def level_kernel(self):
+        k = ctypes.c_int32()
+        self._ck(L.load().cav_octree_get_level_kernel(self._h, ctypes.byref(k)))
+        return k.value
+
     def set_dynamic_sgs(self, on, smag_alpha=0.5, nu_sm_min=-0.1, eta_test=2.0):
         """``set_dynamic_sgs`` (src/octree/solver.rs:476-481): the dynamic
         mixed-scale model on every level (src/octree/smag.rs)."""

@@ -421,6 +421,17 @@ int cav_octree_check_guards(cav_octree* h, double max_u_abort);
 int cav_octree_sync(cav_octree* h);
 int cav_octree_get_stream(cav_octree* h, void** stream);
 int cav_octree_launch_count(cav_octree* h, int64_t* n);
+/* The fine levels' (L1, L2) step kernel, same results bit for bit:
+ *   CAV_OCT_LEVEL_NODE one thread per node;
+ *   CAV_OCT_LEVEL_FG   the default: a node's f and g halves on two threads
+ *                      exchanging u, v, u^2 and T through shared memory
+ *                      (shifted formats without the fixed-Cs extension and
+ *                      outside the dynamic model; the rest run one thread
+ *                      per node). */
+#define CAV_OCT_LEVEL_NODE 0
+#define CAV_OCT_LEVEL_FG 1
+int cav_octree_set_level_kernel(cav_octree* h, int32_t kind);
+int cav_octree_get_level_kernel(cav_octree* h, int32_t* kind);
 /* set_dynamic_sgs (src/octree/solver.rs:476-481): on = 1 runs the dynamic
  * mixed-scale model on every level before each of its collisions
  * (compute_dynamic_sgs_level, src/octree/smag.rs:144-416) and rescales the

@@ -234,6 +234,37 @@ def test_fine_to_coarse_conserves_moments():
     assert worst < 1e-12, worst
 
 
+@pytest.mark.parametrize("prec", ["f32", "f32_f16", "f32_f16g"])
+@pytest.mark.parametrize("levels", [2, 3])
+def test_fg_level_kernel_bit_identical(prec, levels):
+    """The fine levels' step with a node's f and g halves on two threads
+    (the default) and with one thread per node give the same state bit for
+    bit: every level's populations and moments after 37 coarse steps (graph
+    replays and single steps) across the viscosity ramp, with a switch of
+    form half way (binary16 pairs rounded by one cvt.rs against each half
+    rounded alone, the fixed-point g planes, FP32)."""
+    args = (48, 96, 6, 1.0e7, 0.71, 0.03, 7)
+    a = OctreeSolver(*args, levels=levels, precision=prec, nu_start_mult=2.5)
+    b = OctreeSolver(*args, levels=levels, precision=prec, nu_start_mult=2.5)
+    assert a.level_kernel() == L.CAV_OCT_LEVEL_FG
+    b.set_level_kernel(L.CAV_OCT_LEVEL_NODE)
+    assert b.level_kernel() == L.CAV_OCT_LEVEL_NODE
+    a.step_cavity(20)
+    b.step_cavity(20)
+    b.set_level_kernel(L.CAV_OCT_LEVEL_FG)
+    a.set_level_kernel(L.CAV_OCT_LEVEL_NODE)
+    a.step_cavity(17)
+    b.step_cavity(17)
+    for lvl in range(n_levels(levels)):
+        ga, gb = a.level(lvl, pops=True), b.level(lvl, pops=True)
+        for k in ("rho", "ux", "uy", "temp", "f", "g"):
+            np.testing.assert_array_equal(ga[k], gb[k], err_msg=f"level {lvl} {k}")
+    assert a.diag() == b.diag()
+    with pytest.raises(L.CavError) as e:
+        a.set_level_kernel(5)
+    assert e.value.code == L.CAV_ERR_ARG
+
+
 @pytest.mark.parametrize("prec,tol_t,tol_nu", [("f32", 1e-4, 5e-4), ("f32_f16", 3e-3, 2e-3),
                                                 ("f32_f16g", 5e-4, 1e-3)])
 def test_reduced_precision_against_fp64(prec, tol_t, tol_nu):
