@@ -794,9 +794,10 @@ __global__ void __launch_bounds__(OT) k_oct_c2f(LvlPair<StC> C, LvlPair<StF> F,
 // fine_to_coarse (src/octree/interface.rs:175-206) + refresh of the
 // coincident node (src/octree/solver.rs:874-876, 936-942) + that node's next
 // collision into the coarser level's PC (not with the dynamic model, whose
-// collisions run after its own model evaluation).  Four lanes per coincident node
-// (eight nodes per warp): lane l takes the stencil nodes l, l + 4 (and 8 for
-// lane 0) in three rounds, and the round sums are added in stencil order.
+// collisions run after its own model evaluation).  Three lanes per
+// coincident node (F2C_NPW nodes per warp): lane l takes the stencil nodes l,
+// l + 3 and l + 6 in three rounds, and the terms are added in stencil order.
+constexpr int F2C_NPW = 10;
 template <class StF, class StC>
 __global__ void __launch_bounds__(OT) k_oct_f2c(LvlPair<StF> F, LvlPair<StC> C, const CoinE* __restrict__ tab, int n0,
                                                 int n1, Xi<typename Fmt<StF>::A> xi_h,
@@ -808,28 +809,30 @@ __global__ void __launch_bounds__(OT) k_oct_f2c(LvlPair<StF> F, LvlPair<StC> C, 
     pdl_trigger();
     using A = typename Fmt<StF>::A;
     constexpr bool SH = Fmt<StF>::SHIFT;
+    // F2C_NPW coincident nodes per warp, three lanes each (lanes 30, 31 idle)
     const int t = blockIdx.x * OT + threadIdx.x;
-    const int j = t >> 2, l = t & 3;
+    const int wi = t >> 5, lane = t & 31;
+    const int j = wi * F2C_NPW + lane / 3, l = lane - 3 * (lane / 3);
     const int blk = blockIdx.y;
     const int nb = blk == 0 ? n0 : n1;
-    if ((t & ~31) >= 4 * nb) return;  // whole warp past the end
-    const bool act_e = j < nb;
+    if (wi * F2C_NPW >= nb) return;  // whole warp past the end
+    const bool act_e = lane < 3 * F2C_NPW && j < nb;
     const LvlIO<StF> Lf = F.b[blk];
     const LvlIO<StC> Lc = C.b[blk];
     CoinE e{0, 0, 0};
     if (act_e) e = tab[(blk == 0 ? 0 : n0) + j];
     long long sidx;
     const LvlScal<A> sc = row_of<A>(stab, S, step_dev, off, &sidx).l[lvl_c];
-    const int base = (threadIdx.x & 31) & ~3;
+    const int base = lane < 3 * F2C_NPW ? lane - l : 3 * (F2C_NPW - 1);
     const A ww[3] = {A(0.25), A(0.5), A(0.25)};
     A c[NC];
 #pragma unroll
     for (int m = 0; m < NC; ++m) c[m] = A(0.0);
 #pragma unroll
     for (int round = 0; round < 3; ++round) {
-        const int st = 4 * round + l;  // this lane's stencil node in this round
+        const int st = 3 * round + l;  // this lane's stencil node in this round
         A term[NC];
-        if (act_e && st < 9) {
+        if (act_e) {
             const int jb = st / 3, ja = st - 3 * jb;
             const int kf = (e.b + jb - 1) * Lf.nx + (e.a + ja - 1);
             stencil_term<StF>(Lf, kf, ww[ja] * ww[jb], term);
@@ -837,12 +840,10 @@ __global__ void __launch_bounds__(OT) k_oct_f2c(LvlPair<StF> F, LvlPair<StC> C, 
 #pragma unroll
             for (int m = 0; m < NC; ++m) term[m] = A(0.0);
         }
-        const int nl = round < 2 ? 4 : 1;  // stencil nodes 0..3, 4..7, 8
 #pragma unroll
         for (int m = 0; m < NC; ++m)
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-                if (q < nl) {
+            for (int q = 0; q < 3; ++q) {
                     const A v = __shfl_sync(0xffffffffu, term[m], base + q);
                     c[m] = (round == 0 && q == 0) ? v : c[m] + v;
                 }
@@ -1761,6 +1762,8 @@ struct OctImpl final : Octree {
         return q;
     }
     static dim3 grid_of(int n, int nb) { return dim3((n + OT - 1) / OT, nb); }
+    // fine_to_coarse: a warp per F2C_NPW coincident nodes, both blocks
+    static dim3 f2c_grid(int n) { return grid_of(32 * ((n + F2C_NPW - 1) / F2C_NPW), 2); }
 
     // Launch with programmatic dependent launch (the kernels start with
     // pdl_wait(), so a launch overlaps only the tail of its predecessor).
@@ -1831,14 +1834,14 @@ struct OctImpl final : Octree {
     void f2c_L2(int off) {
         LvlPair<StF> f = pair_cur(L2[0], L2[1]);
         LvlPair<StF> c = pair_cur(L1[0], L1[1]);
-        launch(k_oct_f2c<StF, StF>, grid_of(4 * std::max(n_co2_0, n_co2_1), 2), f, c, (const CoinE*)co2, n_co2_0,
+        launch(k_oct_f2c<StF, StF>, f2c_grid(std::max(n_co2_0, n_co2_1)), f, c, (const CoinE*)co2, n_co2_0,
                n_co2_1, xb, xi_b_dev(), (const OctScal<A>*)tab, S, (const long long*)step_dev, off, 1, seed32, 7,
                int(!dyn));
     }
     void f2c_L1(int off) {
         LvlPair<StF> f = pair_cur(L1[0], L1[1]);
         LvlPair<StC> c = pair_cur(L0, L0);
-        launch(k_oct_f2c<StF, StC>, grid_of(4 * std::max(n_co0, n_co1), 2), f, c, (const CoinE*)co1, n_co0, n_co1,
+        launch(k_oct_f2c<StF, StC>, f2c_grid(std::max(n_co0, n_co1)), f, c, (const CoinE*)co1, n_co0, n_co1,
                xa, xi_a_dev(), (const OctScal<A>*)tab, S, (const long long*)step_dev, off, 0, seed32, 13, int(!dyn));
     }
     void step_L0() {
