@@ -32,28 +32,13 @@ constexpr int TX_BX = TX_W + 2 * TILE_HX;  // box width, halo included (80)
 constexpr int TX_WORDS = TX_BX / 2;        // 32-bit words per staged row (40)
 constexpr int TX_HY = 1;                   // staged y halo
 
-// Interior rows pulled without the y bounce-back selects (a warp-uniform
-// branch on the row).
-#ifndef TILEX_INTERIOR_PULL
-#define TILEX_INTERIOR_PULL 1
-#endif
-
-// Resident CTAs per SM the 4-row tiles' register budget is sized for.
-#ifndef TILEX_R4_CTAS
-#define TILEX_R4_CTAS 5
-#endif
-
-// Warps per CTA of the 8-row tiles (each warp TY / WARPS rows).
-#ifndef TILEX_R8_WARPS
-#define TILEX_R8_WARPS 4
-#endif
-
 template <int TY_>
 struct TileXShape {
     static constexpr int TY = TY_;
-    static constexpr int WARPS = TY_ == 8 ? TILEX_R8_WARPS : 4;
-    // resident CTAs per SM the register budget is sized for
-    static constexpr int MIN_CTAS = WARPS == 8 ? 3 : (TY_ == 4 ? TILEX_R4_CTAS : 4);
+    static constexpr int WARPS = 4;  // each warp TY / WARPS rows
+    // resident CTAs per SM the register budget is sized for (4-row tiles: 96
+    // registers, 5 CTAs)
+    static constexpr int MIN_CTAS = TY_ == 4 ? 5 : 4;
     static constexpr int THREADS = 32 * WARPS;
     static constexpr int BY = TY + 2 * TX_HY;
     static constexpr int POP_BYTES = NPLANES * BY * TX_BX * 2;  // the populations of the tile and its halo
@@ -224,7 +209,7 @@ __global__ void __launch_bounds__(TileXShape<TY>::THREADS, TileXShape<TY>::MIN_C
                     const float th = ix == 0 ? meta.c.t_hot[gy] : 0.0f;
                     xpair_core<St, WRITE_NUT, false, false>(
                         [=](uint32_t(&w)[Q]) {
-                            if (TILEX_INTERIOR_PULL && iy > 0 && iy < G.ny - 1)
+                            if (iy > 0 && iy < G.ny - 1)
                                 pull_f_tx<TS::BY, true>(S, G, ix, iy, trow, wc, w);
                             else
                                 pull_f_tx<TS::BY, false>(S, G, ix, iy, trow, wc, w);

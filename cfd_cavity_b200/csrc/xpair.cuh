@@ -28,20 +28,6 @@ namespace cav {
 #ifndef XPAIR_MAXNREG
 #define XPAIR_MAXNREG 96
 #endif
-#ifndef XPAIR_EARLY_G
-#define XPAIR_EARLY_G 0
-#endif
-#ifndef XPAIR_REDECODE_F
-#define XPAIR_REDECODE_F 0
-#endif
-
-// The value itself, opaque to the compiler: a decode of it is not merged
-// with an earlier decode of the same word (so the decoded values need not
-// stay live in between).
-__device__ __forceinline__ uint32_t opaque_u32(uint32_t x) {
-    asm volatile("mov.b32 %0, %1;" : "=r"(x) : "r"(x));
-    return x;
-}
 
 template <class St>
 struct PairEnc;
@@ -172,9 +158,6 @@ __device__ __forceinline__ void xpair_core(PF&& pull_f, PG&& pull_g, TAt&& t_at,
     float2 f[Q];
     uint32_t wg[Q], wf[Q];
     pull_f(wf);
-#if XPAIR_EARLY_G
-    pull_g(wg);
-#endif
 #pragma unroll
     for (int i = 0; i < Q; ++i) f[i] = E::dec(wf[i], i);
     const bool wy = iy == 0 || iy == G.ny - 1;
@@ -186,9 +169,7 @@ __device__ __forceinline__ void xpair_core(PF&& pull_f, PG&& pull_g, TAt&& t_at,
     const CollCoef<float2> kc = collide_f_coef_lane<float2, EF>(f, m, c, nullptr);
     float2 g[Q];
     {
-#if !XPAIR_EARLY_G
         pull_g(wg);
-#endif
         const bool h0 = ix == 0, c0 = ix == G.nx - 1, c1 = ix + 1 == G.nx - 1;
         const float tw0 = (h0 ? t_hot_row : c.t_cold) * p2(EG), tw1 = c.t_cold * p2(EG);
         const float2 tw = make_float2(tw0, tw1);
@@ -234,12 +215,6 @@ __device__ __forceinline__ void xpair_core(PF&& pull_f, PG&& pull_g, TAt&& t_at,
         for (int q = 0; q < Q; ++q) d[(Q + q) * P2 + k2] = E::enc(g[q], Q + q, 0u);
     }
     if (!NO_COLLIDE) {
-#if XPAIR_REDECODE_F
-        // f again from its words (the decoded values were not kept alive
-        // across the g half)
-#pragma unroll
-        for (int i = 0; i < Q; ++i) f[i] = E::dec(opaque_u32(wf[i]), i);
-#endif
         const CollF<float2> o = collide_f_parts_lane<float2, EF>(f, m, kc);
         const float2 fyv = collide_f_post_lane<float2, EF, EG>(f, o, m, c, m.t);
         *reinterpret_cast<float2*>(fy_out + k0) = fyv;
