@@ -46,8 +46,8 @@ BYTES_PER_NODE = {"f64": 304, "f32": 152, "f16": 80, "bf16": 80, "f16g": 80, "f1
                   "bf16sr": 80, "f16gsr": 80}
 PRECISION = "f16sr"
 L2_FLUSH_BYTES = 256 << 20
-# B200 HBM3e nominal bandwidth (the north star's "~8 TB/s peak"), reported
-# beside the measured copy peak
+# B200 HBM3e nominal bandwidth (~8 TB/s), reported beside the measured copy
+# peak
 SPEC_HBM_GBS = 8000.0
 
 
@@ -173,7 +173,7 @@ def cpu_baseline(seconds=12.0, jobs=None):
 
 
 def batched_sweep(precisions, dev, steps=300):
-    """The 64-cavity sweep (configs[2]: Ra log-uniform in [1e6, 1e8], grids
+    """The 64-cavity sweep (Ra log-uniform in [1e6, 1e8], grids
     {64x256, 96x384, 128x512}, Cs in [0.08, 0.12]) as one batched launch per
     step: MLUPS and HBM roofline fraction per storage format, after the
     autotuner picks the tile height and CTAs per SM."""
@@ -210,7 +210,7 @@ def batched_sweep(precisions, dev, steps=300):
 
 
 def c2_nusselt_error(dev, precisions=("f32", "f16sr", "f16", "f16gsr", "bf16sr")):
-    """The accuracy half of the headline: configs[1] (128x512, Ra = 1e8,
+    """The accuracy half of the headline: the 128x512 cavity (Ra = 1e8,
     theta = 0 + 1e-4 noise) for 200 000 steps, the per-step hot / cold wall
     Nu (post.rs:68-111) averaged over steps 150 001-200 000 on the device,
     against the same average of the FP64 oracle (the committed fixture
@@ -238,7 +238,7 @@ def c2_nusselt_error(dev, precisions=("f32", "f16sr", "f16", "f16gsr", "bf16sr")
 
 
 def adjoint_c4(dev):
-    """96x384, Ra=1e7, FP32; J = mean hot-wall Nu over steps
+    """The adjoint workload: 96x384, Ra=1e7, FP32; J = mean hot-wall Nu over steps
     40 001-60 000 of 60 000, gradient w.r.t. the 384-value hot-wall profile
     (seeded +-0.01 around 0.5) and Cs, checkpoints every 500 steps.  Ratio =
     (forward with checkpoints + recomputation + adjoint sweep) / forward."""
@@ -259,7 +259,7 @@ def adjoint_c4(dev):
 
 
 def octree_c5(dev, chain=(30_000, 30_000, 140_000), window=40_000, sample_every=1000):
-    """block-refined cavity, 256x1024 base, L1 bands of bl_width 16
+    """The block-refined cavity: 256x1024 base, L1 bands of bl_width 16
     (Lx/16) on both vertical walls, levels 3 (L2 strips), Ra = 1e10, FP32
     arithmetic with 16-bit fine-level storage.
 
@@ -611,8 +611,8 @@ def main():
         extras["fp32_single_cavity_mlups"] = single_mlups("f32", NX, NY, RA, args.chunk * 3)
         extras["f16_single_cavity_mlups"] = single_mlups("f16", NX, NY, RA, args.chunk * 3)
         # like-for-like with the reference's FP64 arithmetic: the FP64 GPU
-        # path (bit-identical to the FP64 oracle) on configs[0] (64x256,
-        # Ra = 1e6) and on this workload
+        # path (bit-identical to the FP64 oracle) on the 64x256, Ra = 1e6
+        # cavity and on this workload
         extras["fp64_single_cavity"] = {
             "c1_64x256_ra1e6_mlups": single_mlups("f64", 64, 256, 1e6, 2000),
             "c2_128x512_ra1e8_mlups": single_mlups("f64", NX, NY, RA, 2000),

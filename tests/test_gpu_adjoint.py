@@ -104,7 +104,7 @@ def test_adjoint_c4_fp32_gradient_matches_fp64_adjoint_in_every_component():
     components: the 384 hot-wall theta values and Cs.  Tolerances: 1e-3
     relative on the gradient's norm and on dJ/dCs; per theta component
     1e-3 of its own size plus 1e-4 of the gradient's RMS (components that
-    are almost zero, the wall rows, are judged on the RMS scale)."""
+    are almost zero, the wall rows, are compared on the RMS scale)."""
     c = C4
     th = profile(c["ny"])
     out = {}
